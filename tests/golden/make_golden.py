@@ -1,0 +1,289 @@
+"""Generates the golden fixtures in this folder from the reference programs.
+
+Runs ATUS-2's own ``rt_solver``, ``bragg`` and ``sobmin`` (built unmodified
+from the ATUS-2 sources by ``make -C oracle ref``) single-threaded on small
+seeded inputs, and stores inputs and outputs as ``<case>.npz``.  The CPU tests
+replay every case on the oracle restatement and require bit-identical results;
+the GPU tests use the same inputs.
+
+Usage (needs the reference sources, i.e. only where oracle/_ref can be built):
+
+    python tests/golden/make_golden.py            # all cases
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+import re
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+from atus2_b200 import binfmt  # noqa: E402
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF = os.path.join(ROOT, "oracle", "_ref")
+
+
+def grid(header):
+    dim = int(header["nDims"])
+    axes = [binfmt.x_coords(header, a) for a in range(dim)]
+    return np.meshgrid(*axes, indexing="ij")
+
+
+def libm(f, arr):
+    """Element-wise libm call (the reference's expression parser calls libm)."""
+    flat = np.asarray(arr, dtype=np.float64).ravel()
+    return np.array([f(float(v)) for v in flat]).reshape(np.shape(arr))
+
+
+# ------------------------------------------------------------------- cases
+def rt_case(name, dim, n, lo, hi, g, alpha, V_expr, V_fn, seq, psi_fn, algo_dt):
+    return dict(name=name, program="rt_solver", dim=dim, ncomp=1, n=n, lo=lo, hi=hi,
+                gs=[g], Alpha_1=alpha, V_expr=V_expr, V_fn=V_fn, sequence=seq,
+                psi_fn=psi_fn, algo_dt=algo_dt)
+
+
+def psi_gauss_1d(X, rng):
+    (x,) = X
+    p = libm(math.exp, (-0.5 * (x - 1.5)) * (x - 1.5)) * np.exp(2j * x)
+    return p + 1e-6 * (rng.standard_normal(x.shape) + 1j * rng.standard_normal(x.shape))
+
+
+def psi_gauss_2d(X, rng):
+    x, y = X
+    p = libm(math.exp, -((x + 2.0) * (x + 2.0) + y * y) / 8.0) * np.exp(3j * x)
+    return p + 1e-6 * (rng.standard_normal(x.shape) + 1j * rng.standard_normal(x.shape))
+
+
+def psi_gauss_3d(X, rng):
+    x, y, z = X
+    p = libm(math.exp, -0.5 * (x * x + y * y + z * z)) * np.exp(1j * (x + 0.5 * y))
+    return p + 1e-6 * (rng.standard_normal(x.shape) + 1j * rng.standard_normal(x.shape))
+
+
+def psi_tf_3d(X, rng):
+    x, y, z = X
+    return np.sqrt(np.maximum(0.0, 2.0 - 0.5 * (x * x + y * y + z * z))).astype(np.complex128)
+
+
+CASES = [
+    rt_case("rt1d", 1, [128], [-16.0], [16.0], 10.0, [0.5], "0.5*x*x",
+            lambda X: (0.5 * X[0]) * X[0],
+            [dict(name="freeprop", dt=0.001, Nk=40, duration=0.08)], psi_gauss_1d, 1.0),
+    rt_case("rt1d_tables_at_ctor", 1, [128], [-16.0], [16.0], 10.0, [0.5], "0.5*x*x",
+            lambda X: (0.5 * X[0]) * X[0],
+            [dict(name="freeprop", dt=0.001, Nk=40, duration=0.08)], psi_gauss_1d, 0.001),
+    rt_case("rt2d_slit", 2, [64, 32], [-16.0, -8.0], [16.0, 8.0], 1.0, [0.5, 0.5],
+            "200*rect(x,-0.5,0.5)*(1-rect(y,-4.5,-3.5)-rect(y,3.5,4.5))",
+            None,
+            [dict(name="freeprop", dt=0.0005, Nk=30, duration=0.03)], psi_gauss_2d, 1.0),
+    rt_case("rt3d", 3, [16, 8, 16], [-4.0, -4.0, -4.0], [4.0, 4.0, 4.0], 5.0, [0.5, 0.5, 0.5],
+            "0.5*(x*x+y*y+z*z)", lambda X: 0.5 * ((X[0] * X[0] + X[1] * X[1]) + X[2] * X[2]),
+            [dict(name="freeprop", dt=0.001, Nk=20, duration=0.04)], psi_gauss_3d, 1.0),
+]
+
+BRAGG_CASES = [
+    dict(name="bragg1d", dim=1, n=[256], lo=[-32.0], hi=[32.0], laser_k=2.0, laser_domh=8.0, Amp=4.0,
+         tc=0.03, two_sigma2=2 * 0.01 ** 2, g=[100.0, 100.0, 100.0, 100.0], Delta_L=[0.0, 0.0], Beta=[0.0]),
+    dict(name="bragg2d", dim=2, n=[64, 32], lo=[-16.0, -8.0], hi=[16.0, 8.0], laser_k=2.0, laser_domh=8.0,
+         Amp=4.0, tc=0.03, two_sigma2=2 * 0.01 ** 2, g=[100.0, 100.0, 100.0, 100.0], Delta_L=[0.0, 0.5],
+         Beta=[0.1, 0.0]),
+    dict(name="bragg3d", dim=3, n=[16, 8, 16], lo=[-8.0, -4.0, -8.0], hi=[8.0, 4.0, 8.0], laser_k=1.5,
+         laser_domh=4.0, Amp=4.0, tc=0.03, two_sigma2=2 * 0.01 ** 2, g=[100.0, 100.0, 100.0, 100.0],
+         Delta_L=[0.0, 0.0], Beta=[0.0, 0.0, 0.0]),
+]
+
+SOB_CASES = [
+    dict(name="sob1d", dim=1, n=[64], lo=[-8.0], hi=[8.0], g=50.0, Nparticles=1.0, alpha=0.5, stepsize=0.01,
+         epsilon=1e-7, V_expr="0.5*x*x", guess_expr="exp(-0.5*x*x)"),
+    dict(name="sob2d", dim=2, n=[32, 32], lo=[-6.0, -6.0], hi=[6.0, 6.0], g=20.0, Nparticles=1.0, alpha=0.5,
+         stepsize=0.01, epsilon=1e-6, V_expr="0.5*(x*x+4*y*y)", guess_expr="exp(-0.5*(x*x+y*y))"),
+    dict(name="sob3d", dim=3, n=[16, 16, 8], lo=[-6.0, -6.0, -6.0], hi=[6.0, 6.0, 6.0], g=10.0,
+         Nparticles=1.0, alpha=0.5, stepsize=0.01, epsilon=1e-5, V_expr="0.5*(x*x+y*y+z*z)",
+         guess_expr="exp(-0.5*(x*x+y*y+z*z))"),
+]
+
+
+# --------------------------------------------------------------- helpers
+def xml_vec(v):
+    return ",".join(repr(float(a)) for a in v)
+
+
+def run(prog, cwd):
+    env = dict(os.environ, MY_NO_OF_THREADS="1", OMP_NUM_THREADS="1")
+    r = subprocess.run([os.path.join(REF, prog), "run.xml"], cwd=cwd, capture_output=True, text=True,
+                       env=env, timeout=600)
+    if r.returncode != 0:
+        raise RuntimeError(f"{prog} failed: {r.stdout[-2000:]} {r.stderr[-2000:]}")
+    return r.stdout
+
+
+def seq_xml(seq, extra=""):
+    return "".join(
+        f'<{s["name"]} dt="{s["dt"]!r}" Nk="{s["Nk"]}" output_freq="each" pn_freq="each"{extra if s.get("rabi") else ""}>'
+        f'{s["duration"]!r}</{s["name"]}>' for s in seq)
+
+
+def collect_outputs(cwd, ncomp, seq):
+    """Every block's Save_Phi output, in order of time."""
+    files = {}
+    for fn in os.listdir(cwd):
+        m = re.match(r"^(-?\d+\.\d{3})_(\d)\.bin$", fn)
+        if m and fn != "inp_1.bin":
+            files.setdefault(m.group(1), {})[int(m.group(2))] = fn
+    out_t, out_psi = [], []
+    for key in sorted(files, key=float):
+        comps = files[key]
+        recs = [binfmt.read_bin(os.path.join(cwd, comps[c + 1])) for c in range(ncomp)]
+        out_t.append(float(recs[0].header["t"]))
+        out_psi.append(np.stack([r.data for r in recs]))
+    return np.array(out_t), np.stack(out_psi)
+
+
+def make_rt(case, tmp):
+    rng = np.random.default_rng(0)
+    h = binfmt.make_header(case["dim"], case["n"], case["lo"], case["hi"], dt=0.001)
+    X = grid(h)
+    psi0 = case["psi_fn"](X, rng)
+    binfmt.write_bin(os.path.join(tmp, "inp_1.bin"), h, psi0)
+    xml = f"""<SIMULATION>
+  <DIM>{case['dim']}</DIM>
+  <FILENAME>inp_1.bin</FILENAME>
+  <POTENTIAL_{case['dim']}D>{case['V_expr']}</POTENTIAL_{case['dim']}D>
+  <CONSTANTS><unused>0</unused></CONSTANTS>
+  <VCONSTANTS><Alpha_1>{xml_vec(case['Alpha_1'])}</Alpha_1><GS_1>{xml_vec(case['gs'])}</GS_1></VCONSTANTS>
+  <ALGORITHM><DT>{case['algo_dt']!r}</DT></ALGORITHM>
+  <SEQUENCE>{seq_xml(case['sequence'])}</SEQUENCE>
+</SIMULATION>"""
+    open(os.path.join(tmp, "run.xml"), "w").write(xml)
+    run("rt_solver", tmp)
+    t, psi = collect_outputs(tmp, 1, case["sequence"])
+    if case["dim"] == 2 and case["V_fn"] is None:
+        V = potential_2d_from_txt(os.path.join(tmp, "potential.txt"), h)
+    else:
+        V = case["V_fn"](X)
+    params = dict(program="rt_solver", dim=case["dim"], ncomp=1, header_dt=0.001, algo_dt=case["algo_dt"],
+                  Alpha_1=case["Alpha_1"], gs=case["gs"], sequence=case["sequence"])
+    return dict(header=h.tobytes(), psi0=psi0[None], V=V, t=t, psi=psi, params=json.dumps(params), xml=xml)
+
+
+def potential_2d_from_txt(path, h):
+    """rt_solver writes the 2D potential to potential.txt (rt_solver.cpp:117-130)
+    with 6 significant digits; the slit potential only takes the values 0 and
+    200, which that format holds exactly."""
+    vals = []
+    for line in open(path):
+        parts = line.split()
+        if len(parts) == 3:
+            vals.append(float(parts[2]))
+    nx, ny = int(h["nDimX"]), int(h["nDimY"])
+    V = np.array(vals).reshape(nx, ny)
+    assert set(np.unique(V)).issubset({0.0, 200.0})
+    return V
+
+
+def make_bragg(case, tmp):
+    rng = np.random.default_rng(1)
+    dim = case["dim"]
+    h = binfmt.make_header(dim, case["n"], case["lo"], case["hi"], dt=0.001)
+    X = grid(h)
+    r2 = sum(x * x for x in X)
+    psi1 = np.sqrt(np.maximum(0.0, 1.0 - 0.1 * r2)) * (1 + 0.01 * rng.standard_normal(r2.shape))
+    psi1 = psi1.astype(np.complex128)
+    psi2 = np.zeros_like(psi1)
+    binfmt.write_bin(os.path.join(tmp, "inp_1.bin"), h, psi1)
+    binfmt.write_bin(os.path.join(tmp, "inp_2.bin"), h, psi2)
+    seq = [dict(name="bragg_ad", dt=0.001, Nk=20, duration=0.06, rabi=True),
+           dict(name="freeprop", dt=0.001, Nk=20, duration=0.04, rabi=True)]
+    xml = f"""<SIMULATION>
+  <DIM>{dim}</DIM>
+  <FILENAME>inp_1.bin</FILENAME>
+  <FILENAME_2>inp_2.bin</FILENAME_2>
+  <AMP_T>exp(-(t-{case['tc']!r})*(t-{case['tc']!r})/{case['two_sigma2']!r})</AMP_T>
+  <CONSTANTS>
+    <laser_k>{case['laser_k']!r}</laser_k><laser_dk>0</laser_dk><laser_domh>{case['laser_domh']!r}</laser_domh>
+    <rabi_threshold>1.0</rabi_threshold><chirp>0</chirp>
+  </CONSTANTS>
+  <VCONSTANTS>
+    <Amp_1>{case['Amp']!r},{case['Amp']!r}</Amp_1>
+    <Alpha_1>{xml_vec([0.5] * dim)}</Alpha_1>
+    <Delta_L>{xml_vec(case['Delta_L'])}</Delta_L>
+    <GS_1>{xml_vec(case['g'][:2])}</GS_1>
+    <GS_2>{xml_vec(case['g'][2:])}</GS_2>
+    <Beta>{xml_vec(case['Beta'])}</Beta>
+  </VCONSTANTS>
+  <ALGORITHM><DT>1</DT></ALGORITHM>
+  <SEQUENCE>{seq_xml(seq, ' rabi_output_freq="each"')}</SEQUENCE>
+</SIMULATION>"""
+    open(os.path.join(tmp, "run.xml"), "w").write(xml)
+    run("bragg", tmp)
+    t, psi = collect_outputs(tmp, 2, seq)
+    rabi = []
+    for s in (1, 2):
+        rows = [ln.split() for ln in open(os.path.join(tmp, f"Rabi_{s}_0.txt")) if not ln.startswith("#")]
+        rabi += [[float(v) for v in r[1:]] for r in rows if r]
+    k0 = np.zeros((3, dim))
+    k0[1, 0] = 2 * case["laser_k"]
+    k0[2, 0] = -2 * case["laser_k"]
+    params = dict(program="bragg", dim=dim, ncomp=2, header_dt=0.001, algo_dt=1.0, Alpha_1=[0.5] * dim,
+                  gs=case["g"], sequence=seq, AMP_T=dict(tc=case["tc"], two_sigma2=case["two_sigma2"]),
+                  laser_k=case["laser_k"], laser_domh=case["laser_domh"], laser_dk=0.0, chirp=0.0,
+                  Amp_1=[case["Amp"], case["Amp"]], Delta_L=case["Delta_L"], Beta=case["Beta"],
+                  rabi_threshold=1.0, rabi_k0=k0.tolist())
+    return dict(header=h.tobytes(), psi0=np.stack([psi1, psi2]), t=t, psi=psi, rabi=np.array(rabi),
+                params=json.dumps(params), xml=xml)
+
+
+def make_sob(case, tmp):
+    dim = case["dim"]
+    ax = "XYZ"[:dim]
+    algo = "".join(f"<N{a}>{n}</N{a}>" for a, n in zip(ax, case["n"]))
+    algo += "".join(f"<{a}MIN>{lo!r}</{a}MIN><{a}MAX>{hi!r}</{a}MAX>" for a, lo, hi in zip(ax, case["lo"], case["hi"]))
+    xml = f"""<SIMULATION>
+  <DIM>{dim}</DIM>
+  <FILENAME>final.bin</FILENAME>
+  <GUESS_{dim}D>{case['guess_expr']}</GUESS_{dim}D>
+  <POTENTIAL_{dim}D>{case['V_expr']}</POTENTIAL_{dim}D>
+  <CONSTANTS><epsilon>{case['epsilon']!r}</epsilon><stepsize>{case['stepsize']!r}</stepsize></CONSTANTS>
+  <VCONSTANTS><Alpha_1>{case['alpha']!r}</Alpha_1><GS_1>{case['g']!r}</GS_1><N>{case['Nparticles']!r}</N></VCONSTANTS>
+  <ALGORITHM>{algo}</ALGORITHM>
+</SIMULATION>"""
+    open(os.path.join(tmp, "run.xml"), "w").write(xml)
+    out = run("sobmin", tmp)
+    res = [float(m) for m in re.findall(r"^res (\S+)$", out, re.M)]
+    final = binfmt.read_bin(os.path.join(tmp, "final.bin"))
+    params = dict(program="sobmin", dim=dim, n=case["n"], lo=case["lo"], hi=case["hi"], g=case["g"],
+                  Nparticles=case["Nparticles"], alpha=case["alpha"], stepsize=case["stepsize"],
+                  epsilon=case["epsilon"], V_expr=case["V_expr"], guess_expr=case["guess_expr"])
+    return dict(header=final.header.tobytes(), psi=final.data, res=np.array(res), iterations=len(res),
+                params=json.dumps(params), xml=xml)
+
+
+def main():
+    if not os.path.exists(os.path.join(REF, "rt_solver")):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+    for case in CASES:
+        with tempfile.TemporaryDirectory() as tmp:
+            d = make_rt(case, tmp)
+        np.savez_compressed(os.path.join(HERE, case["name"] + ".npz"), **d)
+        print("wrote", case["name"], d["psi"].shape)
+    for case in BRAGG_CASES:
+        with tempfile.TemporaryDirectory() as tmp:
+            d = make_bragg(case, tmp)
+        np.savez_compressed(os.path.join(HERE, case["name"] + ".npz"), **d)
+        print("wrote", case["name"], d["psi"].shape, d["rabi"].shape)
+    for case in SOB_CASES:
+        with tempfile.TemporaryDirectory() as tmp:
+            d = make_sob(case, tmp)
+        np.savez_compressed(os.path.join(HERE, case["name"] + ".npz"), **d)
+        print("wrote", case["name"], "iterations", d["iterations"])
+
+
+if __name__ == "__main__":
+    main()
