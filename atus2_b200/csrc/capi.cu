@@ -1,0 +1,851 @@
+// capi.cu -- host side of libatus_gpu.so: context, planning of the fused
+// passes, and the extern "C" entry points declared in include/atus_gpu.h.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/atus_gpu.h"
+#include "ctx.h"
+#include "launch.h"
+#include "kernels_host.cuh"
+
+using namespace atus;
+
+static int ilog2(int64_t v) {
+  int l = 0;
+  while ((int64_t(1) << l) < v) l++;
+  return l;
+}
+
+// ------------------------------------------------------------------ tables
+// exp(-2 pi i m / TWN) in long double, rounded once; quarter turns exact.
+template <typename R> static std::vector<cplx<R>> twiddles() {
+  std::vector<cplx<R>> t(TWN);
+  const long double two_pi = 6.283185307179586476925286766559005768L;
+  for (int m = 0; m < TWN; m++) {
+    long double c, s;
+    if (m == 0) { c = 1; s = 0; }
+    else if (4 * m == TWN) { c = 0; s = 1; }
+    else if (2 * m == TWN) { c = -1; s = 0; }
+    else if (4 * m == 3 * TWN) { c = 0; s = -1; }
+    else {
+      const long double th = two_pi * (long double)m / (long double)TWN;
+      c = cosl(th);
+      s = sinl(th);
+    }
+    t[m].x = (R)c;
+    t[m].y = (R)(-s);
+  }
+  return t;
+}
+
+// Scale factors of cft_Nd::scale (cft_1d.cpp:191-201, cft_2d.cpp:449-459,
+// cft_3d.cpp:627-637): forward uses dx.., backward dk..
+static double scale_fak(int dim, const double *s) {
+  if (dim == 1) return s[0] / sqrt(2.0 * M_PI);
+  if (dim == 2) return 0.5 * s[0] * s[1] / M_PI;
+  return s[0] * s[1] * s[2] / pow(2 * M_PI, 1.5);
+}
+
+static int64_t wrapped(int64_t i, int64_t n) { return ((i + n / 2) % n) - n / 2; }
+
+template <typename R> static int build_kinetic(atus_ctx *ctx) {
+  using C = cplx<R>;
+  const double s = scale_fak(ctx->dim, ctx->d) * scale_fak(ctx->dim, ctx->dk);
+  for (int hf = 0; hf < 2; hf++) {
+    for (int c = 0; c < ctx->ncomp; c++) {
+      for (int ax = 0; ax < 3; ax++) {
+        const int64_t n = ctx->n[ax];
+        std::vector<C> tab(n);
+        for (int64_t i = 0; i < n; i++) {
+          long double ph = 0.0L;
+          if (ax < ctx->dim) {
+            const long double k = (long double)ctx->dk[ax] * (long double)wrapped(i, n);
+            ph = -(long double)ctx->dt * (long double)ctx->alpha[c][ax] * k * k;
+            if (hf == 0) ph *= 0.5L;
+          }
+          long double cr = cosl(ph), ci = sinl(ph);
+          if (ax == 0) { cr *= s; ci *= s; }
+          tab[i].x = (R)cr;
+          tab[i].y = (R)ci;
+        }
+        if (!ctx->kt[hf][c][ax]) CK(cudaMalloc(&ctx->kt[hf][c][ax], sizeof(C) * n));
+        CK(cudaMemcpyAsync(ctx->kt[hf][c][ax], tab.data(), sizeof(C) * n, cudaMemcpyHostToDevice, ctx->stream));
+      }
+    }
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  return ATUS_OK;
+}
+
+// ------------------------------------------------------------------ launch helpers
+static NLArgs nl_args(const atus_ctx *ctx, int kind, double t1, double F) {
+  NLArgs a;
+  memset(&a, 0, sizeof(a));
+  a.kind = kind;
+  a.ncomp = ctx->ncomp;
+  a.mdt = -ctx->dt;
+  a.dt = ctx->dt;
+  for (int i = 0; i < MAXC * MAXC; i++) a.gs[i] = ctx->gs[i];
+  for (int c = 0; c < MAXC; c++) a.V[c] = (c < ctx->ncomp) ? ctx->V[c] : nullptr;
+  a.L.beta0 = ctx->laser.beta[0];
+  for (int c = 0; c < MAXC; c++) a.L.DeltaL[c] = ctx->laser.DeltaL[c];
+  a.L.Amp0 = ctx->laser.Amp[0];
+  a.L.laser_k0 = ctx->laser.laser_k[0];
+  a.L.laser_dk0 = ctx->laser.laser_dk[0];
+  a.L.laser_domh0 = ctx->laser.laser_domh[0];
+  a.L.phase0 = ctx->laser.phase[0];
+  a.L.chirp_rate0 = ctx->laser.chirp_rate[0];
+  a.L.chirp = ctx->laser.chirp;
+  a.t1 = t1;
+  a.F = F;
+  a.dx0 = ctx->d[0];
+  a.shift0 = (int)(ctx->n[0] / 2);
+  return a;
+}
+
+static int tc_for(int ncomp) { return ncomp <= 1 ? 1 : (ncomp <= 2 ? 2 : 4); }
+
+// One pass along `axis` over `fields` (nullptr: the context's fields).
+static int run_pass(atus_ctx *ctx, int axis, int t1, int op, int t2, const NLArgs *nl, int half,
+                    void *const *fields = nullptr, int nfields = -1) {
+  PassArgs a;
+  memset(&a, 0, sizeof(a));
+  const int nf = nfields < 0 ? ctx->ncomp : nfields;
+  for (int c = 0; c < MAXC; c++) a.psi[c] = (c < nf) ? (fields ? fields[c] : ctx->psi[c]) : nullptr;
+  a.t1 = t1;
+  a.op = op;
+  a.t2 = t2;
+  a.per_comp = (op != OP_NL) ? 1 : 0;
+  a.nc = (op == OP_NL) ? nf : 1;
+  if (op == OP_KIN)
+    for (int c = 0; c < MAXC; c++)
+      for (int ax = 0; ax < 3; ax++) a.kt[c][ax] = (c < ctx->ncomp) ? ctx->kt[half ? 0 : 1][c][ax] : nullptr;
+  if (nl) a.nl = *nl;
+  // per-component passes launch ncomp CTAs in y; override when the field set differs
+  if (a.per_comp && nf != ctx->ncomp) {
+    int saved = ctx->ncomp;
+    ctx->ncomp = nf;
+    int r = (ctx->prec == ATUS_PREC_FP64) ? launch_pass_d1(ctx, a, axis) : launch_pass_f1(ctx, a, axis);
+    ctx->ncomp = saved;
+    return r;
+  }
+  const int tc = a.per_comp ? 1 : tc_for(nf);
+  if (ctx->prec == ATUS_PREC_FP64) {
+    if (tc == 1) return launch_pass_d1(ctx, a, axis);
+    if (tc == 2) return launch_pass_d2(ctx, a, axis);
+    return launch_pass_d4(ctx, a, axis);
+  }
+  if (tc == 1) return launch_pass_f1(ctx, a, axis);
+  if (tc == 2) return launch_pass_f2(ctx, a, axis);
+  return launch_pass_f4(ctx, a, axis);
+}
+
+#define RUN(x)                  \
+  do {                          \
+    int _r = (x);               \
+    if (_r != ATUS_OK) return _r; \
+  } while (0)
+
+// Forward (dir -1) or inverse (+1) transform of the axes other than 0.
+static int transform_inner(atus_ctx *ctx, int dir, void *const *f = nullptr, int nf = -1) {
+  if (ctx->dim == 2) return run_pass(ctx, 1, dir, OP_NONE, T_NONE, nullptr, 0, f, nf);
+  if (ctx->dim == 3) {
+    if (dir == T_FWD) {
+      RUN(run_pass(ctx, 2, T_FWD, OP_NONE, T_NONE, nullptr, 0, f, nf));
+      return run_pass(ctx, 1, T_FWD, OP_NONE, T_NONE, nullptr, 0, f, nf);
+    }
+    RUN(run_pass(ctx, 1, T_INV, OP_NONE, T_NONE, nullptr, 0, f, nf));
+    return run_pass(ctx, 2, T_INV, OP_NONE, T_NONE, nullptr, 0, f, nf);
+  }
+  return ATUS_OK;
+}
+
+// k-space kinetic pass along axis 0: FFT_x, phase, IFFT_x.
+static int kinetic_pass(atus_ctx *ctx, int half) {
+  return run_pass(ctx, 0, T_FWD, OP_KIN, T_INV, nullptr, half);
+}
+
+// Real-space potential pass: 2D one pass over rows; 3D inverse y, rows, forward y.
+static int potential_pass(atus_ctx *ctx, const NLArgs &nl) {
+  const int last = ctx->dim - 1;
+  if (ctx->dim == 3) RUN(run_pass(ctx, 1, T_INV, OP_NONE, T_NONE, nullptr, 0));
+  RUN(run_pass(ctx, last, T_INV, OP_NL, T_FWD, &nl, 0));
+  if (ctx->dim == 3) RUN(run_pass(ctx, 1, T_FWD, OP_NONE, T_NONE, nullptr, 0));
+  return ATUS_OK;
+}
+
+// ------------------------------------------------------------------ reductions
+static int reduce(atus_ctx *ctx, RedArgs &a, double *out) {
+  a.g = geo(ctx);
+  a.dim = ctx->dim;
+  for (int ax = 0; ax < 3; ax++) {
+    a.d[ax] = ctx->d[ax];
+    a.dk[ax] = ctx->dk[ax];
+    a.n[ax] = (int)ctx->n[ax];
+    a.shift[ax] = (int)(ctx->n[ax] / 2);
+  }
+  if (ctx->prec == ATUS_PREC_FP64 || a.mode == RED_MOM || a.mode == RED_RABI)
+    reduce_kernel<double><<<RED_BLOCKS, RED_THREADS, 0, ctx->stream>>>(a, ctx->red_partial);
+  else
+    reduce_kernel<float><<<RED_BLOCKS, RED_THREADS, 0, ctx->stream>>>(a, ctx->red_partial);
+  LAUNCHED(ctx);
+  reduce_final<<<1, 32, 0, ctx->stream>>>(ctx->red_partial, RED_BLOCKS, a.nq, ctx->red_out);
+  LAUNCHED(ctx);
+  CK(cudaMemcpyAsync(ctx->h_red, ctx->red_out, sizeof(double) * a.nq, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (int i = 0; i < a.nq; i++) out[i] = ctx->h_red[i];
+  return ATUS_OK;
+}
+
+static int grid_blocks(int64_t n, int threads) {
+  int64_t b = (n + threads - 1) / threads;
+  return (int)(b < 148 * 16 ? b : 148 * 16);
+}
+
+// Copy component comp into the FP64 scratch buffer (complex128).
+static int to_scratch(atus_ctx *ctx, int comp) {
+  if (ctx->prec == ATUS_PREC_FP64) {
+    CK(cudaMemcpyAsync(ctx->scratch, ctx->psi[comp], 16 * ctx->npts, cudaMemcpyDeviceToDevice, ctx->stream));
+  } else {
+    convert_out_kernel<float><<<grid_blocks(ctx->npts, 256), 256, 0, ctx->stream>>>((double2 *)ctx->scratch,
+                                                                                     ctx->psi[comp], ctx->npts);
+    LAUNCHED(ctx);
+  }
+  return ATUS_OK;
+}
+
+// Forward transform (with the reference's forward scale, applied by the caller)
+// of the FP64 scratch buffer over all axes.
+static int scratch_forward(atus_ctx *ctx) {
+  const int saved = ctx->prec;
+  ctx->prec = ATUS_PREC_FP64;
+  void *f[1] = {ctx->scratch};
+  int r = ATUS_OK;
+  for (int ax = ctx->dim - 1; ax >= 0 && r == ATUS_OK; ax--) r = run_pass(ctx, ax, T_FWD, OP_NONE, T_NONE, nullptr, 0, f, 1);
+  ctx->prec = saved;
+  return r;
+}
+
+// ------------------------------------------------------------------ API
+extern "C" {
+
+int atus_create(const atus_grid *grid, int ncomp, int precision, atus_ctx **out) {
+  if (!grid || !out) return ATUS_E_ARG;
+  *out = nullptr;
+  if (grid->dim < 1 || grid->dim > 3 || ncomp < 1 || ncomp > MAXC) return ATUS_E_ARG;
+  if (precision != ATUS_PREC_FP64 && precision != ATUS_PREC_MIXED) return ATUS_E_ARG;
+  atus_ctx *ctx = new atus_ctx();
+  ctx->dim = grid->dim;
+  ctx->ncomp = ncomp;
+  ctx->prec = precision;
+  ctx->csize = precision == ATUS_PREC_FP64 ? 16 : 8;
+  ctx->npts = 1;
+  for (int a = 0; a < 3; a++) {
+    ctx->n[a] = (a < grid->dim) ? grid->n[a] : 1;
+    ctx->d[a] = (a < grid->dim) ? grid->d[a] : 0.0;
+    ctx->dk[a] = (a < grid->dim) ? grid->dk[a] : 0.0;
+    if (ctx->n[a] < 1 || (ctx->n[a] & (ctx->n[a] - 1)) != 0 || ctx->n[a] > TWN) {
+      delete ctx;
+      return ATUS_E_UNSUPPORTED;
+    }
+    if (a < grid->dim && ctx->n[a] < 2) {
+      delete ctx;
+      return ATUS_E_UNSUPPORTED;
+    }
+    ctx->lg[a] = ilog2(ctx->n[a]);
+    ctx->npts *= ctx->n[a];
+  }
+  if (grid->dim == 1) { ctx->ar = ctx->d[0]; ctx->ar_k = ctx->dk[0]; }
+  else if (grid->dim == 2) { ctx->ar = ctx->d[0] * ctx->d[1]; ctx->ar_k = ctx->dk[0] * ctx->dk[1]; }
+  else { ctx->ar = ctx->d[0] * ctx->d[1] * ctx->d[2]; ctx->ar_k = ctx->dk[0] * ctx->dk[1] * ctx->dk[2]; }
+  ctx->t = grid->t;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) { delete ctx; return ATUS_E_CUDA; }
+  if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return ATUS_E_CUDA; }
+  ctx->stream = ctx->own_stream;
+  bool ok = true;
+  for (int c = 0; c < ncomp && ok; c++) {
+    ok = cudaMalloc(&ctx->psi[c], ctx->csize * ctx->npts) == cudaSuccess;
+    if (ok) ok = cudaMemset(ctx->psi[c], 0, ctx->csize * ctx->npts) == cudaSuccess;
+  }
+  if (ok) ok = cudaMalloc(&ctx->scratch, 16 * ctx->npts) == cudaSuccess;
+  if (ok) ok = cudaMalloc(&ctx->red_partial, sizeof(double) * RED_BLOCKS * RED_MAXQ) == cudaSuccess;
+  if (ok) ok = cudaMalloc(&ctx->red_out, sizeof(double) * RED_MAXQ) == cudaSuccess;
+  if (ok) ok = cudaMallocHost(&ctx->h_red, sizeof(double) * RED_MAXQ) == cudaSuccess;
+  if (ok) {
+    ok = cudaMalloc(&ctx->tw64, 16 * TWN) == cudaSuccess;
+    if (ok) {
+      auto t = twiddles<double>();
+      ok = cudaMemcpy(ctx->tw64, t.data(), 16 * TWN, cudaMemcpyHostToDevice) == cudaSuccess;
+    }
+    ctx->tw = ctx->tw64;
+    if (ok && precision == ATUS_PREC_MIXED) {
+      ok = cudaMalloc(&ctx->tw, 8 * TWN) == cudaSuccess;
+      if (ok) {
+        auto t = twiddles<float>();
+        ok = cudaMemcpy(ctx->tw, t.data(), 8 * TWN, cudaMemcpyHostToDevice) == cudaSuccess;
+      }
+    }
+  }
+  if (!ok) {
+    atus_destroy(ctx);
+    return ATUS_E_NOMEM;
+  }
+  // CRT_Base's constructor builds the tables once (alpha still zero).
+  int r = precision == ATUS_PREC_FP64 ? build_kinetic<double>(ctx) : build_kinetic<float>(ctx);
+  if (r != ATUS_OK) {
+    atus_destroy(ctx);
+    return r;
+  }
+  *out = ctx;
+  return ATUS_OK;
+}
+
+void atus_destroy(atus_ctx *ctx) {
+  if (!ctx) return;
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (int c = 0; c < MAXC; c++) {
+    cudaFree(ctx->psi[c]);
+    cudaFree(ctx->V[c]);
+    cudaFree(ctx->sob_lap[c]);
+    cudaFree(ctx->sob_psi[c]);
+    cudaFree(ctx->sob_grad[c]);
+    for (int hf = 0; hf < 2; hf++)
+      for (int ax = 0; ax < 3; ax++) cudaFree(ctx->kt[hf][c][ax]);
+  }
+  cudaFree(ctx->scratch);
+  if (ctx->tw != ctx->tw64) cudaFree(ctx->tw);
+  cudaFree(ctx->tw64);
+  cudaFree(ctx->red_partial);
+  cudaFree(ctx->red_out);
+  if (ctx->h_red) cudaFreeHost(ctx->h_red);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  delete ctx;
+}
+
+const char *atus_last_error(const atus_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int atus_set_stream(atus_ctx *ctx, void *stream) {
+  if (!ctx) return ATUS_E_ARG;
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+  return ATUS_OK;
+}
+
+int atus_synchronize(atus_ctx *ctx) {
+  if (!ctx) return ATUS_E_ARG;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return ATUS_OK;
+}
+
+int atus_launch_count(const atus_ctx *ctx, int64_t *out) {
+  if (!ctx || !out) return ATUS_E_ARG;
+  *out = ctx->launches;
+  return ATUS_OK;
+}
+
+int atus_set_alpha(atus_ctx *ctx, int comp, const double *alpha) {
+  if (!ctx || !alpha || comp < 0 || comp >= ctx->ncomp) return ATUS_E_ARG;
+  for (int a = 0; a < 3; a++) ctx->alpha[comp][a] = (a < ctx->dim) ? alpha[a] : 0.0;
+  return ATUS_OK;
+}
+
+int atus_set_dt(atus_ctx *ctx, double dt) {
+  if (!ctx) return ATUS_E_ARG;
+  ctx->dt = dt;
+  return ctx->prec == ATUS_PREC_FP64 ? build_kinetic<double>(ctx) : build_kinetic<float>(ctx);
+}
+
+int atus_get_dt(const atus_ctx *ctx, double *dt) {
+  if (!ctx || !dt) return ATUS_E_ARG;
+  *dt = ctx->dt;
+  return ATUS_OK;
+}
+
+int atus_set_time(atus_ctx *ctx, double t) {
+  if (!ctx) return ATUS_E_ARG;
+  ctx->t = t;
+  return ATUS_OK;
+}
+
+int atus_get_time(const atus_ctx *ctx, double *t) {
+  if (!ctx || !t) return ATUS_E_ARG;
+  *t = ctx->t;
+  return ATUS_OK;
+}
+
+int atus_set_gs(atus_ctx *ctx, const double *gs) {
+  if (!ctx || !gs) return ATUS_E_ARG;
+  for (int i = 0; i < MAXC * MAXC; i++) ctx->gs[i] = 0;
+  for (int i = 0; i < ctx->ncomp; i++)
+    for (int j = 0; j < ctx->ncomp; j++) ctx->gs[i * MAXC + j] = gs[j + ctx->ncomp * i];
+  return ATUS_OK;
+}
+
+int atus_set_potential(atus_ctx *ctx, int comp, const double *V) {
+  if (!ctx || comp < 0 || comp >= ctx->ncomp) return ATUS_E_ARG;
+  if (!V) {
+    CK(cudaStreamSynchronize(ctx->stream));
+    cudaFree(ctx->V[comp]);
+    ctx->V[comp] = nullptr;
+    return ATUS_OK;
+  }
+  if (!ctx->V[comp] && cudaMalloc(&ctx->V[comp], sizeof(double) * ctx->npts) != cudaSuccess)
+    return fail(ctx, ATUS_E_NOMEM, "potential allocation");
+  CK(cudaMemcpyAsync(ctx->V[comp], V, sizeof(double) * ctx->npts, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return ATUS_OK;
+}
+
+int atus_set_laser(atus_ctx *ctx, const atus_laser *laser) {
+  if (!ctx || !laser) return ATUS_E_ARG;
+  ctx->laser = *laser;
+  return ATUS_OK;
+}
+
+int atus_upload_psi(atus_ctx *ctx, int comp, const double *psi) {
+  if (!ctx || !psi || comp < 0 || comp >= ctx->ncomp) return ATUS_E_ARG;
+  if (ctx->prec == ATUS_PREC_FP64) {
+    CK(cudaMemcpyAsync(ctx->psi[comp], psi, 16 * ctx->npts, cudaMemcpyHostToDevice, ctx->stream));
+  } else {
+    CK(cudaMemcpyAsync(ctx->scratch, psi, 16 * ctx->npts, cudaMemcpyHostToDevice, ctx->stream));
+    convert_in_kernel<float><<<grid_blocks(ctx->npts, 256), 256, 0, ctx->stream>>>(ctx->psi[comp],
+                                                                                    (const double2 *)ctx->scratch, ctx->npts);
+    LAUNCHED(ctx);
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  return ATUS_OK;
+}
+
+int atus_download_psi(atus_ctx *ctx, int comp, double *psi) {
+  if (!ctx || !psi || comp < 0 || comp >= ctx->ncomp) return ATUS_E_ARG;
+  if (ctx->prec == ATUS_PREC_FP64) {
+    CK(cudaMemcpyAsync(psi, ctx->psi[comp], 16 * ctx->npts, cudaMemcpyDeviceToHost, ctx->stream));
+  } else {
+    RUN(to_scratch(ctx, comp));
+    CK(cudaMemcpyAsync(psi, ctx->scratch, 16 * ctx->npts, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  return ATUS_OK;
+}
+
+int atus_device_psi(atus_ctx *ctx, int comp, void **dptr) {
+  if (!ctx || !dptr || comp < 0 || comp >= ctx->ncomp) return ATUS_E_ARG;
+  *dptr = ctx->psi[comp];
+  return ATUS_OK;
+}
+
+int atus_ft_step(atus_ctx *ctx, int half) {
+  if (!ctx) return ATUS_E_ARG;
+  RUN(transform_inner(ctx, T_FWD));
+  RUN(kinetic_pass(ctx, half));
+  RUN(transform_inner(ctx, T_INV));
+  ctx->t += half ? 0.5 * ctx->dt : ctx->dt;
+  return ATUS_OK;
+}
+
+static int check_kind(atus_ctx *ctx, int kind) {
+  if (kind != K_NL && kind != K_NL_IF && kind != K_BRAGG) return fail(ctx, ATUS_E_ARG, "unknown step kind");
+  if (kind == K_BRAGG && ctx->ncomp != 2) return fail(ctx, ATUS_E_ARG, "bragg_ad needs two components");
+  return ATUS_OK;
+}
+
+int atus_nl_step(atus_ctx *ctx, int kind, double F) {
+  if (!ctx) return ATUS_E_ARG;
+  RUN(check_kind(ctx, kind));
+  NLKArgs a;
+  memset(&a, 0, sizeof(a));
+  for (int c = 0; c < MAXC; c++) a.psi[c] = ctx->psi[c];
+  a.nl = nl_args(ctx, kind, ctx->t + 0.5 * ctx->dt, F);
+  a.g = geo(ctx);
+  if (ctx->prec == ATUS_PREC_FP64)
+    nl_kernel<double><<<grid_blocks(ctx->npts, 256), 256, 0, ctx->stream>>>(a);
+  else
+    nl_kernel<float><<<grid_blocks(ctx->npts, 256), 256, 0, ctx->stream>>>(a);
+  LAUNCHED(ctx);
+  return ATUS_OK;
+}
+
+int atus_strang_block(atus_ctx *ctx, int nk, int kind, const double *F) {
+  if (!ctx || nk < 1) return ATUS_E_ARG;
+  RUN(check_kind(ctx, kind));
+  const double dt = ctx->dt;
+  if (ctx->dim == 1) {
+    Block1DArgs a;
+    memset(&a, 0, sizeof(a));
+    for (int c = 0; c < MAXC; c++) {
+      a.psi[c] = ctx->psi[c];
+      a.kh[c] = (c < ctx->ncomp) ? ctx->kt[0][c][0] : nullptr;
+      a.kf[c] = (c < ctx->ncomp) ? ctx->kt[1][c][0] : nullptr;
+    }
+    a.tw = ctx->tw;
+    a.nl = nl_args(ctx, kind, 0.0, 1.0);
+    a.nk = nk;
+    a.t0 = ctx->t;
+    double *dF = nullptr;
+    if (F) {
+      CK(cudaMalloc(&dF, sizeof(double) * nk));
+      CK(cudaMemcpyAsync(dF, F, sizeof(double) * nk, cudaMemcpyHostToDevice, ctx->stream));
+    }
+    a.F = dF;
+    const int tc = tc_for(ctx->ncomp);
+    int r;
+    if (tc > 2) return fail(ctx, ATUS_E_UNSUPPORTED, "1D blocks take at most two components");
+    if (ctx->prec == ATUS_PREC_FP64)
+      r = tc == 1 ? launch_block1d_d1(ctx, a) : launch_block1d_d2(ctx, a);
+    else
+      r = tc == 1 ? launch_block1d_f1(ctx, a) : launch_block1d_f2(ctx, a);
+    if (dF) {
+      cudaStreamSynchronize(ctx->stream);
+      cudaFree(dF);
+    }
+    if (r != ATUS_OK) return r;
+    // replay the header-time additions of the reference
+    double t = ctx->t + 0.5 * dt;
+    for (int j = 0; j < nk; j++) t += (j == nk - 1) ? 0.5 * dt : dt;
+    ctx->t = t;
+    return ATUS_OK;
+  }
+  // 2D / 3D: [inner forward] kinetic(half) { potential, kinetic } ... [inner inverse]
+  RUN(transform_inner(ctx, T_FWD));
+  RUN(kinetic_pass(ctx, 1));
+  ctx->t += 0.5 * dt;
+  for (int j = 0; j < nk; j++) {
+    const NLArgs nl = nl_args(ctx, kind, ctx->t + 0.5 * dt, F ? F[j] : 1.0);
+    RUN(potential_pass(ctx, nl));
+    const bool last = (j == nk - 1);
+    RUN(kinetic_pass(ctx, last ? 1 : 0));
+    ctx->t += last ? 0.5 * dt : dt;
+  }
+  RUN(transform_inner(ctx, T_INV));
+  return ATUS_OK;
+}
+
+int atus_profile_passes(atus_ctx *ctx, int kind, int reps, double *ms, double *lps, double *bytes, int *npass) {
+  if (!ctx || !ms || !lps || !bytes || !npass || reps < 1) return ATUS_E_ARG;
+  RUN(check_kind(ctx, kind));
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  const NLArgs nl = nl_args(ctx, kind, ctx->t + 0.5 * ctx->dt, 1.0);
+  const double fb = 2.0 * (double)ctx->csize * (double)ctx->ncomp * (double)ctx->npts;  // read + write all fields
+  const double vb = (kind == K_NL) ? 8.0 * ctx->npts * [&] {
+    int k = 0;
+    for (int c = 0; c < ctx->ncomp; c++) k += ctx->V[c] != nullptr;
+    return k;
+  }() : 0.0;
+  int np = 0;
+  auto timed = [&](auto &&launch, double per_step, double b) -> int {
+    RUN(launch());  // warm-up launch
+    CK(cudaEventRecord(e0, ctx->stream));
+    for (int r = 0; r < reps; r++) RUN(launch());
+    CK(cudaEventRecord(e1, ctx->stream));
+    CK(cudaEventSynchronize(e1));
+    float t = 0;
+    CK(cudaEventElapsedTime(&t, e0, e1));
+    ms[np] = (double)t / reps;
+    lps[np] = per_step;
+    bytes[np] = b;
+    np++;
+    return ATUS_OK;
+  };
+  int r = ATUS_OK;
+  if (ctx->dim == 1) {
+    const int nk = 16;
+    auto blk = [&]() { return atus_strang_block(ctx, nk, kind, nullptr); };
+    r = timed(blk, 1.0 / nk, fb);
+  } else {
+    auto kin = [&]() { return kinetic_pass(ctx, 0); };
+    r = timed(kin, 1.0, fb);
+    const int last = ctx->dim - 1;
+    if (r == ATUS_OK && ctx->dim == 3) {
+      auto yinv = [&]() { return run_pass(ctx, 1, T_INV, OP_NONE, T_NONE, nullptr, 0); };
+      r = timed(yinv, 1.0, fb);
+    }
+    if (r == ATUS_OK) {
+      auto pot = [&]() { return run_pass(ctx, last, T_INV, OP_NL, T_FWD, &nl, 0); };
+      r = timed(pot, 1.0, fb + vb);
+    }
+    if (r == ATUS_OK && ctx->dim == 3) {
+      auto yfwd = [&]() { return run_pass(ctx, 1, T_FWD, OP_NONE, T_NONE, nullptr, 0); };
+      r = timed(yfwd, 1.0, fb);
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *npass = np;
+  return r;
+}
+
+int atus_particle_number(atus_ctx *ctx, int comp, double *out) {
+  if (!ctx || !out || comp < 0 || comp >= ctx->ncomp) return ATUS_E_ARG;
+  RedArgs a;
+  memset(&a, 0, sizeof(a));
+  a.mode = RED_NORM;
+  a.nq = 1;
+  a.a = ctx->psi[comp];
+  double s;
+  RUN(reduce(ctx, a, &s));
+  *out = ctx->ar * s;
+  return ATUS_OK;
+}
+
+int atus_expval_position(atus_ctx *ctx, int comp, double *out) {
+  if (!ctx || !out || comp < 0 || comp >= ctx->ncomp) return ATUS_E_ARG;
+  RedArgs a;
+  memset(&a, 0, sizeof(a));
+  a.mode = RED_POS;
+  a.nq = ctx->dim;
+  a.a = ctx->psi[comp];
+  double s[3];
+  RUN(reduce(ctx, a, s));
+  for (int i = 0; i < ctx->dim; i++) out[i] = ctx->ar * s[i];
+  return ATUS_OK;
+}
+
+int atus_expval_momentum(atus_ctx *ctx, int comp, double *out) {
+  if (!ctx || !out || comp < 0 || comp >= ctx->ncomp) return ATUS_E_ARG;
+  RUN(to_scratch(ctx, comp));
+  RUN(scratch_forward(ctx));
+  RedArgs a;
+  memset(&a, 0, sizeof(a));
+  a.mode = RED_MOM;
+  a.nq = ctx->dim;
+  a.a = ctx->scratch;
+  double s[3];
+  RUN(reduce(ctx, a, s));
+  const double f = scale_fak(ctx->dim, ctx->d);
+  for (int i = 0; i < ctx->dim; i++) out[i] = ctx->ar_k * (f * f * s[i]);
+  return ATUS_OK;
+}
+
+int atus_setup_momentum(atus_ctx *ctx, int comp, const double *p) {
+  if (!ctx || !p || comp < 0 || comp >= ctx->ncomp) return ATUS_E_ARG;
+  double pp[3] = {0, 0, 0};
+  for (int i = 0; i < ctx->dim; i++) pp[i] = p[i];
+  const Geo g = geo(ctx);
+  const int b = grid_blocks(ctx->npts, 256);
+  if (ctx->prec == ATUS_PREC_FP64)
+    momentum_kernel<double><<<b, 256, 0, ctx->stream>>>(ctx->psi[comp], g, pp[0], pp[1], pp[2], ctx->d[0], ctx->d[1],
+                                                         ctx->d[2], (int)(ctx->n[0] / 2), (int)(ctx->n[1] / 2),
+                                                         (int)(ctx->n[2] / 2));
+  else
+    momentum_kernel<float><<<b, 256, 0, ctx->stream>>>(ctx->psi[comp], g, pp[0], pp[1], pp[2], ctx->d[0], ctx->d[1],
+                                                        ctx->d[2], (int)(ctx->n[0] / 2), (int)(ctx->n[1] / 2),
+                                                        (int)(ctx->n[2] / 2));
+  LAUNCHED(ctx);
+  return ATUS_OK;
+}
+
+int atus_rabi_integrals(atus_ctx *ctx, const double *k0, int n, double thr, double *out) {
+  if (!ctx || !out || n < 0 || n > RED_MAXQ || (n > 0 && !k0)) return ATUS_E_ARG;
+  if (n == 0) return ATUS_OK;
+  RUN(to_scratch(ctx, 0));
+  RUN(scratch_forward(ctx));
+  RedArgs a;
+  memset(&a, 0, sizeof(a));
+  a.mode = RED_RABI;
+  a.nq = n;
+  a.a = ctx->scratch;
+  a.thr = thr;
+  for (int m = 0; m < n; m++)
+    for (int ax = 0; ax < 3; ax++) a.k0[m][ax] = (ax < ctx->dim) ? k0[m * ctx->dim + ax] : 0.0;
+  double s[RED_MAXQ];
+  RUN(reduce(ctx, a, s));
+  const double f = scale_fak(ctx->dim, ctx->d);
+  for (int m = 0; m < n; m++) out[m] = ctx->ar_k * (f * f * s[m]);
+  return ATUS_OK;
+}
+
+// ------------------------------------------------------------------ Sobolev gradient
+// Real k-space filter of an FP64 buffer over all axes: forward transforms,
+// filter inside the axis-0 pass, inverse transforms.
+static int sob_filter(atus_ctx *ctx, void *buf, int mode, double alpha) {
+  const int saved = ctx->prec;
+  ctx->prec = ATUS_PREC_FP64;
+  void *f[1] = {buf};
+  int r = ATUS_OK;
+  for (int ax = ctx->dim - 1; ax >= 1 && r == ATUS_OK; ax--) r = run_pass(ctx, ax, T_FWD, OP_NONE, T_NONE, nullptr, 0, f, 1);
+  if (r == ATUS_OK) {
+    PassArgs a;
+    memset(&a, 0, sizeof(a));
+    a.psi[0] = buf;
+    a.t1 = T_FWD;
+    a.op = OP_FILT;
+    a.t2 = T_INV;
+    a.per_comp = 1;
+    a.nc = 1;
+    a.filt_mode = mode;
+    a.filt_alpha = alpha;
+    a.filt_scale = scale_fak(ctx->dim, ctx->d) * scale_fak(ctx->dim, ctx->dk);
+    const int saved_nc = ctx->ncomp;
+    ctx->ncomp = 1;
+    r = launch_pass_d1(ctx, a, 0);
+    ctx->ncomp = saved_nc;
+  }
+  for (int ax = 1; ax < ctx->dim && r == ATUS_OK; ax++) r = run_pass(ctx, ax, T_INV, OP_NONE, T_NONE, nullptr, 0, f, 1);
+  ctx->prec = saved;
+  return r;
+}
+
+static int sob_norms(atus_ctx *ctx, double *N) {
+  for (int i = 0; i < ctx->ncomp; i++) RUN(atus_particle_number(ctx, i, &N[i]));
+  return ATUS_OK;
+}
+
+static int sob_renorm(atus_ctx *ctx) {
+  double N[MAXC];
+  RUN(sob_norms(ctx, N));
+  for (int i = 0; i < ctx->ncomp; i++) {
+    scale_kernel<<<grid_blocks(ctx->npts, 256), 256, 0, ctx->stream>>>((double2 *)ctx->psi[i], 1.0 / sqrt(N[i]), ctx->npts);
+    LAUNCHED(ctx);
+  }
+  return ATUS_OK;
+}
+
+static int sob_laplace(atus_ctx *ctx) {
+  for (int i = 0; i < ctx->ncomp; i++) {
+    CK(cudaMemcpyAsync(ctx->sob_lap[i], ctx->psi[i], 16 * ctx->npts, cudaMemcpyDeviceToDevice, ctx->stream));
+    RUN(sob_filter(ctx, ctx->sob_lap[i], FILT_LAPLACE, ctx->sob_alpha[i]));
+  }
+  return ATUS_OK;
+}
+
+static int sob_iterate_once(atus_ctx *ctx, double *res_out, double *N_out) {
+  const int n = ctx->ncomp;
+  const int blocks = grid_blocks(ctx->npts, 256);
+  for (int i = 0; i < n; i++) {  // Compute_Sobolev_Psi
+    CK(cudaMemcpyAsync(ctx->sob_psi[i], ctx->psi[i], 16 * ctx->npts, cudaMemcpyDeviceToDevice, ctx->stream));
+    RUN(sob_filter(ctx, ctx->sob_psi[i], FILT_SOBOLEV, ctx->sob_alpha[i]));
+  }
+  RUN(sob_laplace(ctx));  // Compute_Laplace
+  for (int i = 0; i < n; i++) {  // Compute_Sobolev_Gradient
+    SobArgs a;
+    memset(&a, 0, sizeof(a));
+    for (int j = 0; j < MAXC; j++) a.psi[j] = (const double2 *)ctx->psi[j];
+    a.lap = (const double2 *)ctx->sob_lap[i];
+    a.V = ctx->V[i];
+    a.grad = (double2 *)ctx->sob_grad[i];
+    a.comp = i;
+    a.ncomp = n;
+    for (int k = 0; k < MAXC * MAXC; k++) a.gs[k] = ctx->gs[k];
+    a.npts = ctx->npts;
+    sob_assemble_kernel<<<blocks, 256, 0, ctx->stream>>>(a);
+    LAUNCHED(ctx);
+    RUN(sob_filter(ctx, ctx->sob_grad[i], FILT_SOBOLEV, ctx->sob_alpha[i]));
+  }
+  for (int i = 0; i < n; i++) {  // Project_Sobolev_Gradient
+    RedArgs r;
+    memset(&r, 0, sizeof(r));
+    r.mode = RED_DOT2;
+    r.nq = 2;
+    r.a = ctx->psi[i];
+    r.b = ctx->sob_grad[i];
+    r.c = ctx->sob_psi[i];
+    double q[2];
+    RUN(reduce(ctx, r, q));
+    const double fak = q[0] / q[1];
+    axpy_kernel<<<blocks, 256, 0, ctx->stream>>>((double2 *)ctx->sob_grad[i], (const double2 *)ctx->sob_psi[i], fak,
+                                                 ctx->npts);
+    LAUNCHED(ctx);
+  }
+  double res_tot = 0;  // Compute_res
+  for (int i = 0; i < n; i++) {
+    RedArgs r;
+    memset(&r, 0, sizeof(r));
+    r.mode = RED_NORM;
+    r.nq = 1;
+    r.a = ctx->sob_grad[i];
+    double q;
+    RUN(reduce(ctx, r, &q));
+    q *= ctx->ar;
+    res_tot += q * q;
+  }
+  res_tot = sqrt(res_tot);
+  double N[MAXC];
+  RUN(sob_norms(ctx, N));
+  bool renorm = false;
+  for (int i = 0; i < n; i++) {
+    if (N_out) N_out[i] = N[i];
+    if (fabs(N[i] - 1) > 1e-5) renorm = true;
+  }
+  if (renorm) RUN(sob_renorm(ctx));
+  for (int i = 0; i < n; i++) {
+    axpy_kernel<<<blocks, 256, 0, ctx->stream>>>((double2 *)ctx->psi[i], (const double2 *)ctx->sob_grad[i],
+                                                 ctx->stepsize, ctx->npts);
+    LAUNCHED(ctx);
+  }
+  if (res_out) *res_out = res_tot;
+  return ATUS_OK;
+}
+
+int atus_sob_init(atus_ctx *ctx, const double *alpha, double stepsize) {
+  if (!ctx || !alpha) return ATUS_E_ARG;
+  if (ctx->prec != ATUS_PREC_FP64) return fail(ctx, ATUS_E_UNSUPPORTED, "the Sobolev descent runs in FP64");
+  for (int i = 0; i < ctx->ncomp; i++) {
+    ctx->sob_alpha[i] = alpha[i];
+    if (!ctx->sob_lap[i]) {
+      if (cudaMalloc(&ctx->sob_lap[i], 16 * ctx->npts) != cudaSuccess ||
+          cudaMalloc(&ctx->sob_psi[i], 16 * ctx->npts) != cudaSuccess ||
+          cudaMalloc(&ctx->sob_grad[i], 16 * ctx->npts) != cudaSuccess)
+        return fail(ctx, ATUS_E_NOMEM, "Sobolev buffers");
+    }
+  }
+  ctx->stepsize = stepsize;
+  ctx->sob_ready = true;
+  return ATUS_OK;
+}
+
+int atus_sob_renormalize(atus_ctx *ctx) {
+  if (!ctx || !ctx->sob_ready) return ctx ? fail(ctx, ATUS_E_STATE, "atus_sob_init first") : ATUS_E_ARG;
+  return sob_renorm(ctx);
+}
+
+int atus_sob_iterate(atus_ctx *ctx, int n_iter, double *res, double *N) {
+  if (!ctx || !ctx->sob_ready) return ctx ? fail(ctx, ATUS_E_STATE, "atus_sob_init first") : ATUS_E_ARG;
+  for (int k = 0; k < n_iter; k++) RUN(sob_iterate_once(ctx, res, N));
+  return ATUS_OK;
+}
+
+int atus_sob_run(atus_ctx *ctx, double epsilon, int max_iter, int *iters, double *res) {
+  if (!ctx || !ctx->sob_ready) return ctx ? fail(ctx, ATUS_E_STATE, "atus_sob_init first") : ATUS_E_ARG;
+  RUN(sob_renorm(ctx));
+  int it = 0;
+  double r = 0;
+  do {
+    RUN(sob_iterate_once(ctx, &r, nullptr));
+    it++;
+  } while (r > epsilon && it < max_iter);
+  if (iters) *iters = it;
+  if (res) *res = r;
+  return ATUS_OK;
+}
+
+int atus_sob_mu(atus_ctx *ctx, double *mu) {
+  if (!ctx || !mu || !ctx->sob_ready) return ctx ? fail(ctx, ATUS_E_STATE, "atus_sob_init first") : ATUS_E_ARG;
+  RUN(sob_laplace(ctx));
+  for (int i = 0; i < ctx->ncomp; i++) {
+    RedArgs r;
+    memset(&r, 0, sizeof(r));
+    r.mode = RED_MU;
+    r.nq = 1;
+    r.a = ctx->psi[i];
+    r.b = ctx->sob_lap[i];
+    r.V = ctx->V[i];
+    for (int j = 0; j < MAXC; j++) r.psi_all[j] = ctx->psi[j];
+    r.ncomp = ctx->ncomp;
+    r.comp = i;
+    for (int k = 0; k < MAXC * MAXC; k++) r.gs[k] = ctx->gs[k];
+    double q;
+    RUN(reduce(ctx, r, &q));
+    mu[i] = ctx->ar * q;
+  }
+  return ATUS_OK;
+}
+
+}  // extern "C"

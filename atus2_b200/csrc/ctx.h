@@ -1,0 +1,68 @@
+// ctx.h -- the engine context shared by the host translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "../../include/atus_gpu.h"
+#include "kernels.cuh"
+
+using namespace atus;
+
+struct atus_ctx {
+  int dim = 0, ncomp = 0, prec = 0;
+  int64_t n[3] = {1, 1, 1};
+  int lg[3] = {0, 0, 0};
+  int64_t npts = 0;
+  double d[3] = {0, 0, 0}, dk[3] = {0, 0, 0};
+  double ar = 0, ar_k = 0, t = 0, dt = 0.001;
+  double alpha[MAXC][3] = {};
+  double gs[MAXC * MAXC] = {};  // padded [i*MAXC + j]
+  atus_laser laser = {};
+  size_t csize = 16;            // bytes per complex value
+  void *psi[MAXC] = {};
+  double *V[MAXC] = {};
+  void *scratch = nullptr;      // N complex128 (FP64 staging / spectra)
+  void *tw = nullptr;           // twiddles in the field precision
+  void *tw64 = nullptr;         // FP64 twiddles (spectra of the FP64 scratch buffer)
+  void *kt[2][MAXC][3] = {};    // [half=0/full=1][comp][axis]
+  double *red_partial = nullptr, *red_out = nullptr, *h_red = nullptr;
+  cudaStream_t own_stream = nullptr, stream = nullptr;
+  int64_t launches = 0;
+  std::string err;
+  // Sobolev state
+  bool sob_ready = false;
+  void *sob_lap[MAXC] = {}, *sob_psi[MAXC] = {}, *sob_grad[MAXC] = {};
+  double sob_alpha[MAXC] = {};
+  double stepsize = 0;
+};
+
+// ------------------------------------------------------------------ errors
+static inline int fail(atus_ctx *c, int code, const std::string &msg) {
+  if (c) c->err = msg;
+  return code;
+}
+static inline int cuda_check(atus_ctx *c, cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return ATUS_OK;
+  return fail(c, ATUS_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define CK(call)                                           \
+  do {                                                     \
+    int _r = cuda_check(ctx, (call), #call);               \
+    if (_r != ATUS_OK) return _r;                          \
+  } while (0)
+#define LAUNCHED(ctx)                                                     \
+  do {                                                                    \
+    (ctx)->launches++;                                                    \
+    int _r = cuda_check((ctx), cudaGetLastError(), "kernel launch");      \
+    if (_r != ATUS_OK) return _r;                                         \
+  } while (0)
+
+
+static inline Geo geo(const atus_ctx *ctx) {
+  Geo g;
+  for (int a = 0; a < 3; a++) g.lg[a] = ctx->lg[a];
+  g.npts = ctx->npts;
+  return g;
+}
+

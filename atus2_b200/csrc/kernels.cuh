@@ -1,0 +1,635 @@
+// kernels.cuh -- split-step kernels of the ATUS-2 engine (sm_100a).
+//
+// Fields live in HBM as one contiguous array per component, row-major with x
+// slowest (the .bin layout): complex128 in FP64 mode, complex64 in mixed mode.
+//
+// pass_kernel  one HBM read and one HBM write of a tile of pencils along one
+//              axis: [transform] -> point-wise operator -> [transform].  Used
+//              as  FFT_a -> kinetic phase -> IFFT_a   (k-space half-step) and
+//              IFFT_a -> potential/Bragg step -> FFT_a (real-space half-step),
+//              so each Strang step of a 2D grid is two passes over the fields.
+// block1d_kernel  1D grids: a whole Strang block (Nk steps) with the field
+//              resident in shared memory.
+// nl_kernel    the potential step alone (Do_NL_Step / Do_Bragg_ad).
+// reduce_*     deterministic two-level FP64 reductions.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "fft_device.cuh"
+
+namespace atus {
+
+constexpr int MAXC = 4;
+constexpr int TWN = 8192;  // twiddle table length (largest supported pencil)
+
+// Per-CTA tile budget in complex elements and threads per CTA.
+template <typename R> struct Tile;
+template <> struct Tile<double> { static constexpr int E = 4096; static constexpr int NT = 256; };
+template <> struct Tile<float> { static constexpr int E = 8192; static constexpr int NT = 512; };
+
+enum { T_NONE = 0, T_FWD = -1, T_INV = 1 };
+enum { OP_NONE = 0, OP_KIN = 1, OP_NL = 2, OP_FILT = 3 };
+enum { FILT_SOBOLEV = 0, FILT_LAPLACE = 1 };
+enum { K_NL = 0, K_NL_IF = 1, K_BRAGG = 2 };
+
+struct LaserD {
+  double beta0, DeltaL[MAXC], Amp0, laser_k0, laser_dk0, laser_domh0, phase0, chirp_rate0, chirp;
+};
+
+// Potential-step parameters (by value).
+struct NLArgs {
+  int kind;                 // K_NL / K_NL_IF / K_BRAGG
+  int ncomp;
+  double mdt;               // -dt
+  double dt;
+  double gs[MAXC * MAXC];   // gs[i * MAXC + j] = g_ij (GS_(i+1) entry j)
+  const double *V[MAXC];    // nullptr: no potential
+  LaserD L;
+  double t1;                // header t + dt/2
+  double F;                 // pulse amplitude
+  double dx0;               // grid step of axis 0
+  int shift0;               // n0 / 2
+};
+
+struct Geo {
+  int lg[3];                // log2 of n0, n1, n2 (unused axes: 0)
+  int64_t npts;
+};
+
+struct PassArgs {
+  void *psi[MAXC];
+  int nc;                   // components in the tile (NL) or 1 (per-component passes)
+  int per_comp;             // 1: blockIdx.y selects the component
+  int64_t sa;               // pencil stride in elements
+  int64_t inner_tiles;      // strided: tiles per outer block; contiguous: unused
+  int64_t npencils;         // contiguous: number of pencils
+  int t1, op, t2;
+  const void *kt[MAXC][3];  // kinetic phase tables per component and axis
+  const void *tw;           // twiddles exp(-2 pi i m / TWN)
+  Geo g;
+  NLArgs nl;
+  int x_along;              // 1 when the pencil runs along axis 0 (x varies inside a pencil)
+  // OP_FILT: real k-space filter of CSOB_Base (include/CSOB_Base.h:228-248):
+  // 1/(1 + alpha k^2) or -alpha k^2, times the transform scale.
+  int filt_mode;
+  double filt_alpha, filt_scale;
+  double dk[3];
+  int n[3];
+};
+
+__device__ __forceinline__ void idx3(const Geo &g, int64_t l, int &ix, int &iy, int &iz) {
+  ix = (int)(l >> (g.lg[1] + g.lg[2]));
+  iy = (int)((l >> g.lg[2]) & ((1 << g.lg[1]) - 1));
+  iz = (int)(l & ((1 << g.lg[2]) - 1));
+}
+
+// ------------------------------------------------------------ phase helpers
+// a - 2 pi rint(a / 2 pi), Cody-Waite with 2 pi = P1 + P2 (+P3), P1 with 32
+// significant bits so q*P1 is exact for |q| < 2^20.
+__device__ __forceinline__ double reduce_2pi(double a) {
+  const double P1 = 6.2831853069365025, P2 = 2.430840202602477e-10, P3 = 1.40862394607328e-26;
+  const double q = rint(a * 0.15915494309189535);
+  double r = fma(-q, P1, a);
+  r = fma(-q, P2, r);
+  return fma(-q, P3, r);
+}
+
+// e^{i phi} with an FP64 argument.
+template <typename R> __device__ __forceinline__ cplx<R> expi(double phi);
+template <> __device__ __forceinline__ double2 expi<double>(double phi) {
+  double s, c;
+  sincos(phi, &s, &c);
+  return make_double2(c, s);
+}
+template <> __device__ __forceinline__ float2 expi<float>(double phi) {
+  float s, c;
+  sincosf((float)reduce_2pi(phi), &s, &c);
+  return make_float2(c, s);
+}
+
+// ------------------------------------------------------------ potential step
+// Point-wise potential step on the ncomp values v[] at grid index l.
+// FP64: the reference's formulas (include/CRT_Base.h:410-439,
+// CRT_Base_IF.h:392-418, bragg.cpp:210-302).  Mixed: FP64 phase arguments,
+// FP32 field arithmetic, and the eigenvalue-free form of the 2x2 exponential.
+template <typename R>
+__device__ __forceinline__ void nl_point(const NLArgs &a, cplx<R> *v, int64_t l, double x0, double Omega,
+                                         double eta_c, double eta_s) {
+  using C = cplx<R>;
+  const int n = a.ncomp;
+  double rho[MAXC];
+  #pragma unroll
+  for (int j = 0; j < MAXC; j++)
+    if (j < n) rho[j] = (double)v[j].x * (double)v[j].x + (double)v[j].y * (double)v[j].y;
+  if (a.kind != K_BRAGG) {
+    #pragma unroll
+    for (int i = 0; i < MAXC; i++) {
+      if (i >= n) break;
+      double phi;
+      if (a.kind == K_NL) {
+        phi = a.V[i] ? a.V[i][l] : 0.0;
+        #pragma unroll
+        for (int j = 0; j < MAXC; j++)
+          if (j < n) phi += a.gs[i * MAXC + j] * rho[j];
+      } else {
+        phi = 0.0;
+        #pragma unroll
+        for (int j = 0; j < MAXC; j++)
+          if (j < n) phi += a.gs[i * MAXC + j] * rho[j];
+        phi += a.L.beta0 * x0 - a.L.DeltaL[i];
+      }
+      phi *= a.mdt;
+      const C e = expi<R>(phi);
+      v[i] = cmul(v[i], e);
+    }
+    return;
+  }
+  // Bragg 2x2 (components 0 and 1)
+  const double V11 = a.gs[0] * rho[0] + a.gs[1] * rho[1] + a.L.beta0 * x0;
+  const double V22 = a.gs[MAXC] * rho[0] + a.gs[MAXC + 1] * rho[1] - a.L.DeltaL[1] + a.L.beta0 * x0;
+  const double dt = a.dt;
+  if constexpr (sizeof(R) == 8) {
+    double re1, im1;
+    if (Omega == 0.0) {
+      sincos(-dt * V11, &im1, &re1);
+      v[0] = cmul(v[0], make_double2(re1, im1));
+      sincos(-dt * V22, &im1, &re1);
+      v[1] = cmul(v[1], make_double2(re1, im1));
+      return;
+    }
+    double tmp1 = sqrt((V11 - V22) * (V11 - V22) + 4.0 * Omega * Omega);
+    const double Ep = 0.5 * (V11 + V22 + tmp1);
+    const double Em = 0.5 * (V11 + V22 - tmp1);
+    double2 gp, gm;
+    sincos(-dt * Ep, &im1, &re1);
+    tmp1 = 1.0 / fabs((V11 - Ep) * (V11 - Ep) + Omega * Omega);
+    gp = make_double2(tmp1 * re1, tmp1 * im1);
+    sincos(-dt * Em, &im1, &re1);
+    tmp1 = 1.0 / fabs((V11 - Em) * (V11 - Em) + Omega * Omega);
+    gm = make_double2(tmp1 * re1, tmp1 * im1);
+    const double O2 = Omega * Omega;
+    const double2 O11 = make_double2(O2 * (gp.x + gm.x), O2 * (gp.y + gm.y));
+    const double a1 = V11 - Ep, a2 = V11 - Em;
+    const double2 O22 = make_double2(a1 * a1 * gp.x + a2 * a2 * gm.x, a1 * a1 * gp.y + a2 * a2 * gm.y);
+    const double2 Os = make_double2(-Omega * (a1 * gp.x + a2 * gm.x), -Omega * (a1 * gp.y + a2 * gm.y));
+    const double2 eta = make_double2(eta_c, eta_s);
+    const double2 O12 = cmul(Os, eta);   // eta * O12
+    const double2 O21 = cmulc(Os, eta);  // conj(eta) * O21
+    const double2 p1 = v[0], p2 = v[1];
+    v[0] = cadd(cmul(O11, p1), cmul(O12, p2));
+    v[1] = cadd(cmul(O21, p1), cmul(O22, p2));
+  } else {
+    // U = e^{-i dt m} [cos(r dt) I - i sin(r dt)/r [[d, W], [W, -d]]], m = (V11+V22)/2,
+    // d = (V11-V22)/2, W = Omega, r = sqrt(d^2 + W^2); off-diagonals times eta / conj(eta).
+    const double m = 0.5 * (V11 + V22), d = 0.5 * (V11 - V22);
+    const double r = sqrt(d * d + Omega * Omega);
+    float sm, cm, sr, cr;
+    sincosf((float)reduce_2pi(-dt * m), &sm, &cm);
+    sincosf((float)reduce_2pi(dt * r), &sr, &cr);
+    const float sr_over_r = (r > 0.0) ? (float)((double)sr / r) : (float)dt;
+    const float fd = sr_over_r * (float)d, fw = sr_over_r * (float)Omega;
+    // U11 = e(cr - i fd), U22 = e(cr + i fd), Uoff = e(-i fw)
+    const float2 e = make_float2(cm, sm);
+    const float2 U11 = cmul(e, make_float2(cr, -fd));
+    const float2 U22 = cmul(e, make_float2(cr, fd));
+    const float2 Uo = cmul(e, make_float2(0.f, -fw));
+    const float2 et = make_float2((float)eta_c, (float)eta_s);
+    const float2 U12 = cmul(Uo, et), U21 = cmulc(Uo, et);
+    const float2 p1 = v[0], p2 = v[1];
+    v[0] = cadd(cmul(U11, p1), cmul(U12, p2));
+    v[1] = cadd(cmul(U21, p1), cmul(U22, p2));
+  }
+}
+
+// Omega(x0) and eta(x0) of the Bragg step (bragg.cpp:224, 243).
+__device__ __forceinline__ void bragg_coupling(const NLArgs &a, double x0, double &Omega, double &ec, double &es) {
+  const double t1 = a.t1;
+  Omega = a.F * a.L.Amp0 *
+          cos(a.L.laser_k0 * x0 - (a.L.laser_domh0 + a.L.chirp * t1 + a.L.chirp_rate0 * t1) * t1 + a.L.phase0 / 2);
+  sincos(-0.5 * (a.L.laser_dk0 * x0), &es, &ec);
+}
+
+// ------------------------------------------------------------ kinetic step
+template <typename C>
+__device__ __forceinline__ C kin_phase(const C *kx, const C *ky, const C *kz, int ix, int iy, int iz) {
+  return cmul(cmul(__ldg(&kx[ix]), __ldg(&ky[iy])), __ldg(&kz[iz]));
+}
+
+// ------------------------------------------------------------ pass kernel
+template <typename R, int N, int TC>
+struct PassCfg {
+  static constexpr int NT = Tile<R>::NT;
+  static constexpr int B0 = Tile<R>::E / (N * TC);
+  static constexpr int B1 = B0 > 0 ? B0 : 1;
+  static constexpr int B = B1 < 256 ? B1 : 256;  // pencils per tile
+  static constexpr int NP = Pad<N>::NP;
+  static constexpr size_t smem = sizeof(cplx<R>) * (size_t)TC * B * NP;
+};
+
+template <typename R, int N, int TC>
+__global__ void __launch_bounds__(Tile<R>::NT) pass_kernel(PassArgs a) {
+  using C = cplx<R>;
+  using Cfg = PassCfg<R, N, TC>;
+  constexpr int B = Cfg::B, NT = Cfg::NT, NP = Cfg::NP;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *s = reinterpret_cast<C *>(smem_raw);
+  __shared__ double s_om[B], s_ec[B], s_es[B];
+
+  const int comp0 = a.per_comp ? blockIdx.y : 0;
+  const int nc = a.per_comp ? 1 : a.nc;
+  // tile -> pencil bases
+  int64_t base0;
+  int64_t pstride;  // distance between pencils of the tile
+  int nb;
+  if (a.sa > 1) {
+    const int64_t o = blockIdx.x / a.inner_tiles;
+    const int64_t r0 = (blockIdx.x % a.inner_tiles) * B;
+    base0 = o * (int64_t)N * a.sa + r0;
+    pstride = 1;
+    nb = (int)((a.sa - r0) < B ? (a.sa - r0) : B);
+  } else {
+    const int64_t p0 = (int64_t)blockIdx.x * B;
+    base0 = p0 * N;
+    pstride = N;
+    nb = (int)((a.npencils - p0) < B ? (a.npencils - p0) : B);
+  }
+  C *fld[TC];
+  {
+    void *P[MAXC];
+    #pragma unroll
+    for (int c = 0; c < MAXC; c++) P[c] = a.psi[c];
+    #pragma unroll
+    for (int c = 0; c < TC; c++) fld[c] = (C *)P[(comp0 + c) < MAXC ? (comp0 + c) : 0];
+  }
+  // load
+  #pragma unroll
+  for (int c = 0; c < TC; c++) {
+    for (int r = threadIdx.x; r < B * N; r += NT) {
+      int b, i;
+      if (a.sa > 1) { b = r % B; i = r / B; } else { i = r % N; b = r / N; }
+      C val = mk<R>(0, 0);
+      if (c < nc && b < nb) val = fld[c][base0 + b * pstride + (int64_t)i * a.sa];
+      s[c * B * NP + Pad<N>::idx(b, i)] = val;
+    }
+  }
+  __syncthreads();
+  const C *tw = (const C *)a.tw;
+  if (a.t1 == T_FWD) fft_tile<R, N, TC * B, NT, -1, TWN>(s, tw);
+  else if (a.t1 == T_INV) fft_tile<R, N, TC * B, NT, +1, TWN>(s, tw);
+
+  if (a.op == OP_KIN) {
+    const C *kx, *ky, *kz;
+    {
+      const void *T[MAXC][3];
+      #pragma unroll
+      for (int c = 0; c < MAXC; c++)
+        #pragma unroll
+        for (int ax = 0; ax < 3; ax++) T[c][ax] = a.kt[c][ax];
+      kx = (const C *)T[comp0][0]; ky = (const C *)T[comp0][1]; kz = (const C *)T[comp0][2];
+    }
+    for (int e = threadIdx.x; e < B * N; e += NT) {
+      const int b = e / N, i = e % N;
+      if (b < nb) {
+        const int64_t l = base0 + b * pstride + (int64_t)i * a.sa;
+        int ix, iy, iz;
+        idx3(a.g, l, ix, iy, iz);
+        const C k = kin_phase(kx, ky, kz, ix, iy, iz);
+        const int si = Pad<N>::idx(b, i);
+        s[si] = cmul(s[si], k);
+      }
+    }
+    __syncthreads();
+  } else if (a.op == OP_FILT) {
+    for (int e = threadIdx.x; e < B * N; e += NT) {
+      const int b = e / N, i = e % N;
+      if (b < nb) {
+        const int64_t l = base0 + b * pstride + (int64_t)i * a.sa;
+        int ijk[3];
+        idx3(a.g, l, ijk[0], ijk[1], ijk[2]);
+        double phi = 0;
+        #pragma unroll
+        for (int ax = 0; ax < 3; ax++) {
+          const int t = (ijk[ax] + a.n[ax] / 2) % a.n[ax];
+          const double k = a.dk[ax] * (double)(t - a.n[ax] / 2);
+          phi += (k * a.filt_alpha) * k;
+        }
+        const double f = (a.filt_mode == FILT_SOBOLEV ? 1.0 / (1.0 + phi) : -phi) * a.filt_scale;
+        const int si = Pad<N>::idx(b, i);
+        C v = s[si];
+        v.x = (R)((double)v.x * f);
+        v.y = (R)((double)v.y * f);
+        s[si] = v;
+      }
+    }
+    __syncthreads();
+  } else if (a.op == OP_NL) {
+    const bool bragg = (a.nl.kind == K_BRAGG);
+    if (bragg && !a.x_along) {
+      for (int b = threadIdx.x; b < B; b += NT) {
+        double om = 0, ec = 1, es = 0;
+        if (b < nb) {
+          int ix, iy, iz;
+          idx3(a.g, base0 + b * pstride, ix, iy, iz);
+          bragg_coupling(a.nl, (double)(ix - a.nl.shift0) * a.nl.dx0, om, ec, es);
+        }
+        s_om[b] = om; s_ec[b] = ec; s_es[b] = es;
+      }
+      __syncthreads();
+    }
+    for (int e = threadIdx.x; e < B * N; e += NT) {
+      const int b = e / N, i = e % N;
+      if (b < nb) {
+        const int64_t l = base0 + b * pstride + (int64_t)i * a.sa;
+        int ix, iy, iz;
+        idx3(a.g, l, ix, iy, iz);
+        const double x0 = (double)(ix - a.nl.shift0) * a.nl.dx0;
+        double om = 0, ec = 1, es = 0;
+        if (bragg) {
+          if (a.x_along) bragg_coupling(a.nl, x0, om, ec, es);
+          else { om = s_om[b]; ec = s_ec[b]; es = s_es[b]; }
+        }
+        C v[MAXC];
+        #pragma unroll
+        for (int c = 0; c < TC; c++) v[c] = s[c * B * NP + Pad<N>::idx(b, i)];
+        nl_point<R>(a.nl, v, l, x0, om, ec, es);
+        #pragma unroll
+        for (int c = 0; c < TC; c++) s[c * B * NP + Pad<N>::idx(b, i)] = v[c];
+      }
+    }
+    __syncthreads();
+  }
+
+  if (a.t2 == T_FWD) fft_tile<R, N, TC * B, NT, -1, TWN>(s, tw);
+  else if (a.t2 == T_INV) fft_tile<R, N, TC * B, NT, +1, TWN>(s, tw);
+
+  #pragma unroll
+  for (int c = 0; c < TC; c++) {
+    if (c < nc) {
+      for (int r = threadIdx.x; r < B * N; r += NT) {
+        int b, i;
+        if (a.sa > 1) { b = r % B; i = r / B; } else { i = r % N; b = r / N; }
+        if (b < nb) fld[c][base0 + b * pstride + (int64_t)i * a.sa] = s[c * B * NP + Pad<N>::idx(b, i)];
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------ 1D Strang block
+struct Block1DArgs {
+  void *psi[MAXC];
+  const void *kh[MAXC], *kf[MAXC];  // half / full kinetic tables (scale folded in)
+  const void *tw;
+  NLArgs nl;
+  int nk;
+  double t0;                        // header time at block start
+  const double *F;                  // per potential step, or nullptr
+};
+
+template <typename R, int N, int TC>
+__device__ __forceinline__ void kin_1d(cplx<R> *s, const cplx<R> *const (&tab)[TC], int nc) {
+  using C = cplx<R>;
+  constexpr int NT = Tile<R>::NT, NP = Pad<N>::NP;
+  #pragma unroll
+  for (int c = 0; c < TC; c++) {
+    if (c < nc) {
+      for (int i = threadIdx.x; i < N; i += NT) {
+        C &x = s[c * NP + Pad<N>::idx(0, i)];
+        x = cmul(x, __ldg(&tab[c][i]));
+      }
+    }
+  }
+  __syncthreads();
+}
+
+template <typename R, int N, int TC>
+__global__ void __launch_bounds__(Tile<R>::NT) block1d_kernel(Block1DArgs a) {
+  using C = cplx<R>;
+  constexpr int NT = Tile<R>::NT, NP = Pad<N>::NP;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *s = reinterpret_cast<C *>(smem_raw);
+  const int nc = a.nl.ncomp;
+  const C *tw = (const C *)a.tw;
+  C *fld[TC];
+  const C *kh[TC], *kf[TC];
+  #pragma unroll
+  for (int c = 0; c < TC; c++) {
+    fld[c] = (C *)a.psi[c];
+    kh[c] = (const C *)a.kh[c];
+    kf[c] = (const C *)a.kf[c];
+  }
+  #pragma unroll
+  for (int c = 0; c < TC; c++)
+    for (int i = threadIdx.x; i < N; i += NT) s[c * NP + Pad<N>::idx(0, i)] = (c < nc) ? fld[c][i] : mk<R>(0, 0);
+  __syncthreads();
+  double t = a.t0;
+  const double dt = a.nl.dt;
+  // half kinetic step
+  fft_tile<R, N, TC, NT, -1, TWN>(s, tw);
+  kin_1d<R, N, TC>(s, kh, nc);
+  fft_tile<R, N, TC, NT, +1, TWN>(s, tw);
+  t += 0.5 * dt;
+  NLArgs nl = a.nl;
+  for (int j = 0; j < a.nk; j++) {
+    nl.t1 = t + 0.5 * dt;
+    nl.F = a.F ? a.F[j] : 1.0;
+    for (int i = threadIdx.x; i < N; i += NT) {
+      const double x0 = (double)(i - nl.shift0) * nl.dx0;
+      double om = 0, ec = 1, es = 0;
+      if (nl.kind == K_BRAGG) bragg_coupling(nl, x0, om, ec, es);
+      C v[MAXC];
+      #pragma unroll
+      for (int c = 0; c < TC; c++) v[c] = s[c * NP + Pad<N>::idx(0, i)];
+      nl_point<R>(nl, v, i, x0, om, ec, es);
+      #pragma unroll
+      for (int c = 0; c < TC; c++) s[c * NP + Pad<N>::idx(0, i)] = v[c];
+    }
+    __syncthreads();
+    const bool last = (j == a.nk - 1);
+    fft_tile<R, N, TC, NT, -1, TWN>(s, tw);
+    if (last) kin_1d<R, N, TC>(s, kh, nc);
+    else kin_1d<R, N, TC>(s, kf, nc);
+    fft_tile<R, N, TC, NT, +1, TWN>(s, tw);
+    t += last ? 0.5 * dt : dt;
+  }
+  #pragma unroll
+  for (int c = 0; c < TC; c++)
+    if (c < nc)
+      for (int i = threadIdx.x; i < N; i += NT) fld[c][i] = s[c * NP + Pad<N>::idx(0, i)];
+}
+
+// ------------------------------------------------------------ point-wise kernels
+struct NLKArgs {
+  void *psi[MAXC];
+  NLArgs nl;
+  Geo g;
+};
+
+template <typename R>
+__global__ void nl_kernel(NLKArgs a) {
+  using C = cplx<R>;
+  const int n = a.nl.ncomp;
+  for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < a.g.npts;
+       l += (int64_t)gridDim.x * blockDim.x) {
+    int ix, iy, iz;
+    idx3(a.g, l, ix, iy, iz);
+    const double x0 = (double)(ix - a.nl.shift0) * a.nl.dx0;
+    double om = 0, ec = 1, es = 0;
+    if (a.nl.kind == K_BRAGG) bragg_coupling(a.nl, x0, om, ec, es);
+    C v[MAXC];
+    #pragma unroll
+    for (int c = 0; c < MAXC; c++)
+      if (c < n) v[c] = ((C *)a.psi[c])[l];
+    nl_point<R>(a.nl, v, l, x0, om, ec, es);
+    #pragma unroll
+    for (int c = 0; c < MAXC; c++)
+      if (c < n) ((C *)a.psi[c])[l] = v[c];
+  }
+}
+
+// psi *= e^{i p.x}  (Setup_Momentum)
+template <typename R>
+__global__ void momentum_kernel(void *psi, Geo g, double p0, double p1, double p2, double dx0, double dx1,
+                                double dx2, int s0, int s1, int s2) {
+  using C = cplx<R>;
+  for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < g.npts; l += (int64_t)gridDim.x * blockDim.x) {
+    int ix, iy, iz;
+    idx3(g, l, ix, iy, iz);
+    const double dot = p0 * ((double)(ix - s0) * dx0) + p1 * ((double)(iy - s1) * dx1) + p2 * ((double)(iz - s2) * dx2);
+    C *P = (C *)psi;
+    P[l] = cmul(P[l], expi<R>(dot));
+  }
+}
+
+// FP64 <-> field precision conversions (mixed mode upload / download).
+template <typename R>
+__global__ void convert_in_kernel(void *dst, const double2 *src, int64_t n) {
+  for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < n; l += (int64_t)gridDim.x * blockDim.x)
+    ((cplx<R> *)dst)[l] = mk<R>((R)src[l].x, (R)src[l].y);
+}
+template <typename R>
+__global__ void convert_out_kernel(double2 *dst, const void *src, int64_t n) {
+  for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < n; l += (int64_t)gridDim.x * blockDim.x) {
+    const cplx<R> v = ((const cplx<R> *)src)[l];
+    dst[l] = make_double2((double)v.x, (double)v.y);
+  }
+}
+
+// ------------------------------------------------------------ Sobolev helpers
+// G = -Lap psi_i + (V_i + sum_j g_ij |psi_j|^2) psi_i   (CSOB_Base.h:317-326)
+struct SobArgs {
+  const double2 *psi[MAXC];
+  const double2 *lap;
+  const double *V;
+  double2 *grad;
+  int comp, ncomp;
+  double gs[MAXC * MAXC];
+  int64_t npts;
+};
+
+// ------------------------------------------------------------ reductions
+// Quantities per mode (all FP64 accumulations, fixed order per thread, fixed
+// tree per block, partials summed in block order by reduce_final).
+enum { RED_NORM = 0, RED_POS = 1, RED_MOM = 2, RED_RABI = 3, RED_DOT2 = 4, RED_MU = 5 };
+constexpr int RED_MAXQ = 8;
+constexpr int RED_BLOCKS = 592;  // 4 x 148 SMs
+constexpr int RED_THREADS = 256;
+
+struct RedArgs {
+  int mode;
+  int nq;
+  const void *a, *b, *c;   // field operands
+  const double *V;
+  Geo g;
+  int dim;
+  double d[3], dk[3];
+  int n[3], shift[3];
+  double k0[8][3];         // Rabi centres
+  double thr;
+  // mu
+  const void *psi_all[MAXC];
+  int ncomp, comp;
+  double gs[MAXC * MAXC];
+};
+
+template <typename R>
+__device__ __forceinline__ void red_point(const RedArgs &a, int64_t l, double *q) {
+  using C = cplx<R>;
+  const C v = ((const C *)a.a)[l];
+  const double den = (double)v.x * (double)v.x + (double)v.y * (double)v.y;
+  if (a.mode == RED_NORM) { q[0] += den; return; }
+  int ijk[3];
+  idx3(a.g, l, ijk[0], ijk[1], ijk[2]);
+  if (a.mode == RED_POS) {
+    for (int ax = 0; ax < a.dim; ax++) q[ax] += ((double)(ijk[ax] - a.shift[ax]) * a.d[ax]) * den;
+    return;
+  }
+  double k[3];
+  for (int ax = 0; ax < a.dim; ax++) {
+    const int t = (ijk[ax] + a.shift[ax]) % a.n[ax];
+    k[ax] = a.dk[ax] * (double)(t - a.shift[ax]);
+  }
+  if (a.mode == RED_MOM) {
+    for (int ax = 0; ax < a.dim; ax++) q[ax] += k[ax] * den;
+    return;
+  }
+  if (a.mode == RED_RABI) {
+    int j = 0;
+    for (int m = 0; m < a.nq; m++) {
+      double dd = 0;
+      for (int ax = 0; ax < a.dim; ax++) {
+        const double d = a.k0[m][ax] - k[ax];
+        dd += d * d;
+      }
+      if (sqrt(dd) < a.thr) { q[j] += den; continue; }
+      j++;
+    }
+    return;
+  }
+  if (a.mode == RED_DOT2) {  // Re<a,b>, Re<a,c>
+    const C b = ((const C *)a.b)[l];
+    q[0] += (double)v.x * (double)b.x + (double)v.y * (double)b.y;
+    if (a.c) {
+      const C c = ((const C *)a.c)[l];
+      q[1] += (double)v.x * (double)c.x + (double)v.y * (double)c.y;
+    }
+    return;
+  }
+  if (a.mode == RED_MU) {  // a = psi_i, b = Lap psi_i
+    const C lp = ((const C *)a.b)[l];
+    double nl = 0;
+    #pragma unroll
+    for (int j = 0; j < MAXC; j++) {
+      if (j < a.ncomp) {
+        const C pj = ((const C *)a.psi_all[j])[l];
+        nl += a.gs[a.comp * MAXC + j] * ((double)pj.x * (double)pj.x + (double)pj.y * (double)pj.y);
+      }
+    }
+    const double pot = a.V ? a.V[l] : 0.0;
+    q[0] += -((double)v.x * (double)lp.x + (double)v.y * (double)lp.y) + (pot + nl) * den;
+  }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(RED_THREADS) reduce_kernel(RedArgs a, double *partial) {
+  double q[RED_MAXQ];
+  #pragma unroll
+  for (int i = 0; i < RED_MAXQ; i++) q[i] = 0;
+  for (int64_t l = blockIdx.x * (int64_t)RED_THREADS + threadIdx.x; l < a.g.npts; l += (int64_t)gridDim.x * RED_THREADS)
+    red_point<R>(a, l, q);
+  __shared__ double sh[RED_THREADS];
+  for (int i = 0; i < a.nq; i++) {
+    sh[threadIdx.x] = q[i];
+    __syncthreads();
+    for (int s = RED_THREADS / 2; s > 0; s >>= 1) {
+      if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x * RED_MAXQ + i] = sh[0];
+    __syncthreads();
+  }
+}
+
+
+}  // namespace atus

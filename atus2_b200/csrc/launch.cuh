@@ -1,0 +1,96 @@
+// launch.cuh -- launchers of the templated kernels.  Each instantiation file
+// (inst_*.cu) includes this and exports one precision / component-count
+// combination, so the kernels compile in parallel.
+#pragma once
+#include "ctx.h"
+
+template <typename R, int N, int TC>
+static inline int launch_pass_t(atus_ctx *ctx, PassArgs &a, int axis) {
+  using Cfg = PassCfg<R, N, TC>;
+  constexpr size_t smem = Cfg::smem;
+  if (smem + 3 * sizeof(double) * Cfg::B > 227 * 1024) return fail(ctx, ATUS_E_UNSUPPORTED, "pencil too long for this component count");
+  static bool attr_set = false;
+  if (!attr_set) {
+    CK(cudaFuncSetAttribute(pass_kernel<R, N, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_set = true;
+  }
+  int64_t sa = 1;
+  for (int b = axis + 1; b < 3; b++) sa *= ctx->n[b];
+  a.sa = sa;
+  int64_t ntiles;
+  if (sa > 1) {
+    a.inner_tiles = (sa + Cfg::B - 1) / Cfg::B;
+    ntiles = (ctx->npts / (N * sa)) * a.inner_tiles;
+    a.npencils = 0;
+  } else {
+    a.inner_tiles = 1;
+    a.npencils = ctx->npts / N;
+    ntiles = (a.npencils + Cfg::B - 1) / Cfg::B;
+  }
+  a.x_along = (axis == 0);
+  a.g = geo(ctx);
+  a.tw = (sizeof(R) == 8) ? ctx->tw64 : ctx->tw;
+  for (int ax = 0; ax < 3; ax++) {
+    a.dk[ax] = ctx->dk[ax];
+    a.n[ax] = (int)ctx->n[ax];
+  }
+  dim3 grid((unsigned)ntiles, a.per_comp ? ctx->ncomp : 1);
+  pass_kernel<R, N, TC><<<grid, Cfg::NT, smem, ctx->stream>>>(a);
+  LAUNCHED(ctx);
+  return ATUS_OK;
+}
+
+template <typename R, int TC>
+static inline int launch_pass_n(atus_ctx *ctx, PassArgs &a, int axis) {
+  switch (ctx->n[axis]) {
+    case 2: return launch_pass_t<R, 2, TC>(ctx, a, axis);
+    case 4: return launch_pass_t<R, 4, TC>(ctx, a, axis);
+    case 8: return launch_pass_t<R, 8, TC>(ctx, a, axis);
+    case 16: return launch_pass_t<R, 16, TC>(ctx, a, axis);
+    case 32: return launch_pass_t<R, 32, TC>(ctx, a, axis);
+    case 64: return launch_pass_t<R, 64, TC>(ctx, a, axis);
+    case 128: return launch_pass_t<R, 128, TC>(ctx, a, axis);
+    case 256: return launch_pass_t<R, 256, TC>(ctx, a, axis);
+    case 512: return launch_pass_t<R, 512, TC>(ctx, a, axis);
+    case 1024: return launch_pass_t<R, 1024, TC>(ctx, a, axis);
+    case 2048: return launch_pass_t<R, 2048, TC>(ctx, a, axis);
+    case 4096: return launch_pass_t<R, 4096, TC>(ctx, a, axis);
+    case 8192: return launch_pass_t<R, 8192, TC>(ctx, a, axis);
+    default: return fail(ctx, ATUS_E_UNSUPPORTED, "axis length must be a power of two in [2, 8192]");
+  }
+}
+
+template <typename R, int N, int TC>
+static inline int launch_block1d_t(atus_ctx *ctx, Block1DArgs &a) {
+  constexpr size_t smem = sizeof(cplx<R>) * TC * Pad<N>::NP;
+  if (smem > 227 * 1024) return fail(ctx, ATUS_E_UNSUPPORTED, "1D grid too long for the resident kernel");
+  static bool attr_set = false;
+  if (!attr_set) {
+    CK(cudaFuncSetAttribute(block1d_kernel<R, N, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_set = true;
+  }
+  block1d_kernel<R, N, TC><<<1, Tile<R>::NT, smem, ctx->stream>>>(a);
+  LAUNCHED(ctx);
+  return ATUS_OK;
+}
+
+template <typename R, int TC>
+static inline int launch_block1d_n(atus_ctx *ctx, Block1DArgs &a) {
+  switch (ctx->n[0]) {
+    case 2: return launch_block1d_t<R, 2, TC>(ctx, a);
+    case 4: return launch_block1d_t<R, 4, TC>(ctx, a);
+    case 8: return launch_block1d_t<R, 8, TC>(ctx, a);
+    case 16: return launch_block1d_t<R, 16, TC>(ctx, a);
+    case 32: return launch_block1d_t<R, 32, TC>(ctx, a);
+    case 64: return launch_block1d_t<R, 64, TC>(ctx, a);
+    case 128: return launch_block1d_t<R, 128, TC>(ctx, a);
+    case 256: return launch_block1d_t<R, 256, TC>(ctx, a);
+    case 512: return launch_block1d_t<R, 512, TC>(ctx, a);
+    case 1024: return launch_block1d_t<R, 1024, TC>(ctx, a);
+    case 2048: return launch_block1d_t<R, 2048, TC>(ctx, a);
+    case 4096: return launch_block1d_t<R, 4096, TC>(ctx, a);
+    case 8192: return launch_block1d_t<R, 8192, TC>(ctx, a);
+    default: return fail(ctx, ATUS_E_UNSUPPORTED, "axis length must be a power of two in [2, 8192]");
+  }
+}
+

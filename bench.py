@@ -1,0 +1,444 @@
+#!/usr/bin/env python
+"""Benchmark of the split-step Gross-Pitaevskii path on B200.
+
+Workload (the 3D two-component Bragg configuration): 256^3 grid on
+[-32,32)^3, two components, g11 = g12 = g21 = g22 = 100, alpha = 1/2,
+coupling Omega(t) cos(2 k_L x - delta t)/2 with k_L = 4 (laser_k = 8),
+delta = 16 (laser_domh), Gaussian pulse of peak 8 (Amp = 4) and sigma_t = 0.5
+centred at t = 2.5, state 1 a Thomas-Fermi profile (omega = 1) normalised on
+the grid, state 2 empty, dt = 1e-3.  The timed window sits on the pulse
+(header time starts at 2.4).  Synthetic inputs, seeded.
+
+A step is one Strang step of the bragg_ad sequence over the whole grid; the
+metric is grid-point steps per second (grid points x steps / time).  value:
+fields resident in HBM, K steps as one run_sequence block (the fused GPU
+path), timed with CUDA events on the launching stream.  e2e: the same metric
+through the C ABI with host buffers -- every step of the e2e loop is one
+output block of 100 Strang steps framed by the host->device upload and the
+device->host download of both components (pinned host memory).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl atus|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N = 256
+L = 64.0
+G = 100.0
+DT = 1e-3
+T0 = 2.4
+PULSE_TC, PULSE_SIGMA = 2.5, 0.5
+E2E_NK = 100
+METRIC = "grid-pt-steps/s (3D 256^3 two-component Bragg split-step, FP64)"
+UNIT = "grid-pt-steps/s"
+
+
+def pulse(t: float) -> float:
+    return math.exp((-(t - PULSE_TC)) * (t - PULSE_TC) / (2 * PULSE_SIGMA * PULSE_SIGMA))
+
+
+def pulse_train(t0: float, nk: int):
+    """Pulse amplitudes of the nk potential steps of a block starting at t0,
+    with the reference's header-time additions (include/CRT_Base.h:361,391)."""
+    t = t0 + 0.5 * DT
+    out = []
+    for _ in range(nk):
+        out.append(pulse(t + 0.5 * DT))
+        t += DT
+    return np.array(out)
+
+
+def header(n=N):
+    from atus2_b200 import binfmt
+
+    return binfmt.make_header(3, [n, n, n], [-L / 2] * 3, [L / 2] * 3, t=T0, dt=DT)
+
+
+def initial_state(h):
+    from atus2_b200 import binfmt
+
+    n = int(h["nDimX"])
+    x = binfmt.x_coords(h, 0)
+    r2 = x[:, None, None] ** 2 + x[None, :, None] ** 2 + x[None, None, :] ** 2
+    mu = 10.0
+    psi1 = np.sqrt(np.maximum(0.0, (mu - 0.5 * r2) / G)).astype(np.complex128)
+    psi1 /= math.sqrt(float(h["dx"] * h["dy"] * h["dz"]) * float(np.sum(np.abs(psi1) ** 2)))
+    psi2 = np.zeros((n, n, n), dtype=np.complex128)
+    return psi1, psi2
+
+
+def laser_kw():
+    return dict(Amp=[4.0, 4.0], laser_k=[8.0, 0.0], laser_domh=[16.0, 0.0])
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"), p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ helpers
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws <= 1:
+        return 0, 1, 0, None
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    rank = int(os.environ["RANK"])
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    backend = "nccl" if torch.cuda.is_available() else "gloo"
+    if backend == "nccl":
+        torch.cuda.set_device(local)
+    dist.init_process_group(backend, timeout=timedelta(seconds=300))
+    return rank, ws, local, dist
+
+
+def max_over_ranks(dist, v: float) -> float:
+    if dist is None:
+        return v
+    import torch
+
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+# ------------------------------------------------------------------ atus arm
+def run_gpu(prec, steps, warmup, stream):
+    """Returns (solver, ms for `steps` Strang steps, launches) on a resident state."""
+    import torch
+
+    from atus2_b200 import STEP_BRAGG_AD, Laser, Solver
+
+    h = header()
+    psi1, psi2 = initial_state(h)
+    s = Solver(h, 2, prec)
+    s.set_stream(stream.cuda_stream)
+    s.set_psi(0, psi1)
+    s.set_psi(1, psi2)
+    for c in range(2):
+        s.set_alpha(c, [0.5, 0.5, 0.5])
+    s.set_gs([G] * 4)
+    s.set_dt(DT)
+    s.set_laser(Laser.make(**laser_kw()))
+    for _ in range(warmup):
+        s.block(1, STEP_BRAGG_AD, None, pulse_train(s.t, 1))
+    F = pulse_train(s.t, steps)
+    torch.cuda.synchronize()
+    n0 = s.launches
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    s.block(steps, STEP_BRAGG_AD, None, F)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return s, e0.elapsed_time(e1), s.launches - n0, h
+
+
+def run_e2e(steps, stream):
+    import torch
+
+    from atus2_b200 import PREC_FP64, STEP_BRAGG_AD, Laser, Solver
+
+    h = header()
+    psi1, psi2 = initial_state(h)
+    npts = N ** 3
+    host = [torch.empty(2 * npts, dtype=torch.float64, pin_memory=True) for _ in range(2)]
+    host[0].numpy()[:] = psi1.view(np.float64).ravel()
+    host[1].numpy()[:] = psi2.view(np.float64).ravel()
+    s = Solver(h, 2, PREC_FP64)
+    s.set_stream(stream.cuda_stream)
+    for c in range(2):
+        s.set_alpha(c, [0.5, 0.5, 0.5])
+    s.set_gs([G] * 4)
+    s.set_dt(DT)
+    s.set_laser(Laser.make(**laser_kw()))
+    # one untimed round trip
+    for c in range(2):
+        s.upload_from(c, host[c].data_ptr())
+    s.block(2, STEP_BRAGG_AD, None, pulse_train(s.t, 2))
+    for c in range(2):
+        s.download_to(c, host[c].data_ptr())
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        for c in range(2):
+            s.upload_from(c, host[c].data_ptr())
+        s.block(E2E_NK, STEP_BRAGG_AD, None, pulse_train(s.t, E2E_NK))
+        for c in range(2):
+            s.download_to(c, host[c].data_ptr())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    s.close()
+    return ms, 2 * 16 * npts, 2 * 16 * npts
+
+
+def run_cpu_baseline(n_steps_sample=(1, 3)):
+    """The reference program (oracle/_ref/bragg, built from the ATUS-2 sources
+    with the FFTW-API shim) on this host's cores: two runs of the 256^3 Bragg
+    workload of n1 and n2 Strang steps; (t2 - t1)/(n2 - n1) is the steady
+    per-step cost with the set-up cancelled."""
+    prog = os.path.join(ROOT, "oracle", "_ref", "bragg")
+    if not os.path.exists(prog):
+        return None
+    from atus2_b200 import binfmt
+
+    cores = os.cpu_count() or 1
+    h = header()
+    psi1, psi2 = initial_state(h)
+    times = []
+    with tempfile.TemporaryDirectory() as tmp:
+        binfmt.write_bin(os.path.join(tmp, "inp_1.bin"), h, psi1)
+        binfmt.write_bin(os.path.join(tmp, "inp_2.bin"), h, psi2)
+        for ns in n_steps_sample:
+            xml = f"""<SIMULATION>
+  <DIM>3</DIM><FILENAME>inp_1.bin</FILENAME><FILENAME_2>inp_2.bin</FILENAME_2>
+  <AMP_T>exp(-(t-{PULSE_TC!r})*(t-{PULSE_TC!r})/{2 * PULSE_SIGMA * PULSE_SIGMA!r})</AMP_T>
+  <CONSTANTS><laser_k>8</laser_k><laser_dk>0</laser_dk><laser_domh>16</laser_domh>
+    <rabi_threshold>1</rabi_threshold><chirp>0</chirp></CONSTANTS>
+  <VCONSTANTS><Amp_1>4,4</Amp_1><Alpha_1>0.5,0.5,0.5</Alpha_1><Delta_L>0,0</Delta_L>
+    <GS_1>100,100</GS_1><GS_2>100,100</GS_2><Beta>0,0,0</Beta></VCONSTANTS>
+  <ALGORITHM><DT>1</DT></ALGORITHM>
+  <SEQUENCE><bragg_ad dt="0.001" Nk="{ns}" output_freq="none" pn_freq="none">{ns * DT!r}</bragg_ad></SEQUENCE>
+</SIMULATION>"""
+            open(os.path.join(tmp, "run.xml"), "w").write(xml)
+            env = dict(os.environ, MY_NO_OF_THREADS=str(cores), OMP_NUM_THREADS=str(cores))
+            t0 = time.perf_counter()
+            r = subprocess.run([prog, "run.xml"], cwd=tmp, env=env, capture_output=True, text=True, timeout=900)
+            times.append(time.perf_counter() - t0)
+            if r.returncode != 0:
+                return None
+    n1, n2 = n_steps_sample
+    per_step = max((times[1] - times[0]) / (n2 - n1), 1e-9)
+    return {
+        "value": N ** 3 / per_step,
+        "unit": UNIT,
+        "cores": cores,
+        "kind": "reference",
+        "sample": f"ATUS-2 bragg (oracle/_ref, shim FFT) at 256^3 x 2 components, runs of {n1} and {n2} "
+                  f"Strang steps (Nk = steps), per-step = difference / {n2 - n1}; MY_NO_OF_THREADS={cores}",
+        "seconds": times,
+    }
+
+
+def roofline(s, kind, peak, peak_kind):
+    prof = s.profile_passes(kind, reps=5)
+    # dominant pass: largest device time per Strang step
+    best = max(prof, key=lambda p: p[0] * p[1])
+    ms, lps, by = best
+    achieved = by / (ms * 1e-3) / 1e9
+    return {
+        "bound": "hbm",
+        "achieved": achieved,
+        "peak": peak,
+        "unit": "GB/s",
+        "frac": achieved / peak,
+        "peak_source": peak_kind,
+        "traffic": None,
+        "kernel": "pass_kernel (see profiles/)",
+        "passes": [{"ms": p[0], "launches_per_step": p[1], "bytes": p[2], "GBps": p[2] / (p[0] * 1e-3) / 1e9} for p in prof],
+    }
+
+
+def atus_arm(args, rank, ws, local, dist):
+    import torch
+
+    from atus2_b200 import PREC_FP64, PREC_MIXED, STEP_BRAGG_AD
+
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    peak, peak_kind = peaks()
+    with ClockSampler(local) as clk:
+        barrier(dist)
+        s, ms, launches, h = run_gpu(PREC_FP64, args.steps, args.warmup, stream)
+        ms = max_over_ranks(dist, ms)
+    npts = N ** 3
+    value = ws * npts * args.steps / (ms * 1e-3)
+    out = {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": ws,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded Thomas-Fermi state, analytic potential parameters)",
+        "config": {
+            "workload": "3D two-component Bragg pulse (bragg_ad), 256^3 on [-32,32)^3, g=100, k_L=4, delta=16, "
+                        "Omega peak 8, sigma_t 0.5, dt=1e-3",
+            "grid": [N, N, N],
+            "components": 2,
+            "parallelism": f"replicas x{ws} (no inter-GPU exchange)",
+            "l2": "fields (2 x 268 MB) larger than the 126 MB L2; no flush needed",
+            "block": f"{args.steps} Strang steps as one run_sequence block",
+        },
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    if rank == 0:
+        out["roofline"] = roofline(s, STEP_BRAGG_AD, peak, peak_kind)
+    s.close()
+    # mixed precision variant (same workload, complex64 fields)
+    barrier(dist)
+    sm, msm, lm, _ = run_gpu(PREC_MIXED, args.steps, args.warmup, stream)
+    msm = max_over_ranks(dist, msm)
+    out["variants"] = {"mixed": {"value": ws * npts * args.steps / (msm * 1e-3), "ms_per_step": msm / args.steps,
+                                 "dtype": "c64 fields, f64 phase arguments", "speedup_vs_fp64": ms / msm}}
+    if rank == 0:
+        out["variants"]["mixed"]["roofline"] = roofline(sm, STEP_BRAGG_AD, peak, peak_kind)
+    sm.close()
+    # end-to-end through the C ABI with host buffers
+    barrier(dist)
+    e2e_steps = max(1, min(args.steps // 20, 5))
+    ms_e, bi, bo = run_e2e(e2e_steps, stream)
+    ms_e = max_over_ranks(dist, ms_e)
+    out["e2e"] = {"value": ws * npts * E2E_NK * e2e_steps / (ms_e * 1e-3), "unit": UNIT,
+                  "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo,
+                  "step": f"upload 2 components, {E2E_NK} Strang steps, download 2 components", "steps": e2e_steps}
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = run_cpu_baseline()
+    barrier(dist)
+    if rank == 0:
+        print(json.dumps(out))
+
+
+# ------------------------------------------------------------------ reference arm
+def reference_arm(args, rank, ws, dist):
+    if rank != 0:
+        return
+    cb = run_cpu_baseline()
+    if cb is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/bragg is not built (needs the ATUS-2 sources)"}))
+        return
+    # steps of the reference arm: each step one Strang step, timed from the difference runs
+    per_step_s = N ** 3 / cb["value"]
+    out = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": cb["value"],
+        "unit": UNIT,
+        "n_gpus": ws,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": per_step_s * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded Thomas-Fermi state)",
+        "config": {"workload": "3D two-component Bragg pulse (bragg_ad), 256^3, reference CPU program",
+                   "grid": [N, N, N], "components": 2},
+        "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="atus", choices=["atus", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank, ws, local, dist = dist_init()
+    try:
+        if args.impl == "reference":
+            reference_arm(args, rank, ws, dist)
+        else:
+            atus_arm(args, rank, ws, local, dist)
+    finally:
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

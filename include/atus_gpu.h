@@ -1,0 +1,178 @@
+/*
+ * atus_gpu.h -- C ABI of libatus_gpu.so, the B200 (sm_100a) split-step
+ * Gross-Pitaevskii engine behind the ATUS-2 solver classes.
+ *
+ * Plain C: no CUDA, no C++ and no torch types cross this boundary.  Every call
+ * returns ATUS_OK (0) or a negative ATUS_E* code; atus_last_error() gives the
+ * message of the last failure on a context.  A context is used by one host
+ * thread at a time.  Host buffers are borrowed for the duration of the call.
+ *
+ * Each entry point replaces one piece of the reference's FFTW/OpenMP path
+ * (paths relative to the ATUS-2 source tree):
+ *
+ *   atus_create / atus_destroy      CRT_Base ctor+dtor, Allocate, LoadFiles
+ *                                   (include/CRT_Base.h:138-240); the header
+ *                                   fields used are those of Read_header
+ *                                   (include/CRT_shared.h:131-172)
+ *   atus_set_alpha, atus_set_dt     Alpha_1/Alpha_2 and CRT_Base::Init / Set_dt
+ *                                   (include/CRT_Base.h:171-174, 252-274;
+ *                                   CRT_Base_2.h:194-221; CRT_shared.h:117-121)
+ *   atus_set_gs                     GS_i matrix (include/CRT_Base.h:161-169)
+ *   atus_set_potential              Init_Potential + Setup_Potential
+ *                                   (include/CRT_Base.h:276-298)
+ *   atus_set_laser                  CRT_Base_IF::UpdateParams members
+ *                                   (include/CRT_Base_IF.h:65-77, 144-168)
+ *   atus_upload_psi/atus_download_psi  m_fields[c]->Getp2In() contents
+ *                                   (source/libs/lib_myutils/cft_base.h:175)
+ *   atus_ft_step                    Do_FT_Step_full / Do_FT_Step_half
+ *                                   (include/CRT_Base.h:336-392)
+ *   atus_nl_step                    Do_NL_Step (include/CRT_Base.h:396-441),
+ *                                   CRT_Base_IF::Do_NL_Step (CRT_Base_IF.h:380-419),
+ *                                   Bragg_single::Do_Bragg_ad
+ *                                   (source/interferometry/src/bragg.cpp:185-304)
+ *   atus_strang_block               the inner loop of run_sequence,
+ *                                   half,(V,full)^(Nk-1),V,half
+ *                                   (include/CRT_Base.h:776-786,
+ *                                   CRT_Base_IF.h:779-789), fused on the GPU
+ *   atus_particle_number            Get_Particle_Number (include/CRT_Base.h:586-599)
+ *   atus_expval_position/momentum   Expval_Position / Expval_Momentum
+ *                                   (include/CRT_Base.h:480-580)
+ *   atus_setup_momentum             Setup_Momentum (include/CRT_Base.h:448-473)
+ *   atus_rabi_integrals             compute_rabi_integrals (CRT_Base_IF.h:207-281)
+ *   atus_sob_*                      CSOB_Base (include/CSOB_Base.h:96-543)
+ */
+#ifndef ATUS_GPU_H
+#define ATUS_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define ATUS_API __attribute__((visibility("default")))
+#else
+#define ATUS_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ATUS_OK 0
+#define ATUS_E_ARG (-1)         /* invalid argument */
+#define ATUS_E_UNSUPPORTED (-2) /* grid or mode this build does not handle */
+#define ATUS_E_CUDA (-3)        /* CUDA runtime error */
+#define ATUS_E_STATE (-4)       /* call not valid in the current state */
+#define ATUS_E_NOMEM (-5)       /* device allocation failed */
+
+#define ATUS_PREC_FP64 0  /* complex128 fields, FP64 FFTs: the drop-in */
+#define ATUS_PREC_MIXED 1 /* complex64 fields and FFTs, FP64 phase arguments */
+
+/* Potential-step kinds (the XML sequence tag that selects them). */
+#define ATUS_STEP_NL 0       /* "freeprop" of CRT_Base: V + g|psi|^2 */
+#define ATUS_STEP_NL_IF 1    /* "freeprop" of CRT_Base_IF: g|psi|^2 + beta.x - DeltaL */
+#define ATUS_STEP_BRAGG_AD 2 /* "bragg_ad": analytic 2x2 Bragg exponential */
+
+#define ATUS_MAX_COMP 4
+
+typedef struct atus_ctx atus_ctx;
+
+/* The grid part of the 1380-byte generic_header (include/my_structs.h:40-72). */
+typedef struct {
+  int dim;          /* nDims */
+  int64_t n[3];     /* nDimX, nDimY, nDimZ (unused axes: 1) */
+  double d[3];      /* dx, dy, dz */
+  double dk[3];     /* dkx, dky, dkz */
+  double t;         /* header time */
+} atus_grid;
+
+/* CRT_Base_IF laser members; arrays sized as in the reference. */
+typedef struct {
+  double beta[3];
+  double DeltaL[ATUS_MAX_COMP];
+  double Amp[2];
+  double laser_k[2];
+  double laser_dk[2];
+  double laser_domh[2];
+  double phase[2];
+  double chirp_rate[2];
+  double chirp;
+} atus_laser;
+
+/* ------------------------------------------------------------ context */
+ATUS_API int atus_create(const atus_grid *grid, int ncomp, int precision, atus_ctx **out);
+ATUS_API void atus_destroy(atus_ctx *ctx);
+ATUS_API const char *atus_last_error(const atus_ctx *ctx);
+/* Kernels run on this CUDA stream (a cudaStream_t; NULL = the context's own). */
+ATUS_API int atus_set_stream(atus_ctx *ctx, void *stream);
+ATUS_API int atus_synchronize(atus_ctx *ctx);
+/* Number of kernels this context has launched so far. */
+ATUS_API int atus_launch_count(const atus_ctx *ctx, int64_t *out);
+
+/* ------------------------------------------------------------ parameters */
+ATUS_API int atus_set_alpha(atus_ctx *ctx, int comp, const double *alpha /* dim */);
+/* Stores dt and rebuilds the kinetic phases from the alpha values set so far
+ * (CRT_Base::Init semantics: later atus_set_alpha calls take effect at the
+ * next atus_set_dt). */
+ATUS_API int atus_set_dt(atus_ctx *ctx, double dt);
+ATUS_API int atus_get_dt(const atus_ctx *ctx, double *dt);
+ATUS_API int atus_set_time(atus_ctx *ctx, double t);
+ATUS_API int atus_get_time(const atus_ctx *ctx, double *t);
+ATUS_API int atus_set_gs(atus_ctx *ctx, const double *gs /* ncomp*ncomp, row i = GS_(i+1) */);
+/* V: N doubles in grid order, or NULL to drop the potential of comp. */
+ATUS_API int atus_set_potential(atus_ctx *ctx, int comp, const double *V);
+ATUS_API int atus_set_laser(atus_ctx *ctx, const atus_laser *laser);
+
+/* ------------------------------------------------------------ fields */
+/* Interleaved complex128, N values, grid order (the .bin payload). */
+ATUS_API int atus_upload_psi(atus_ctx *ctx, int comp, const double *psi);
+ATUS_API int atus_download_psi(atus_ctx *ctx, int comp, double *psi);
+/* Device pointer of component comp (complex128 or complex64 per precision). */
+ATUS_API int atus_device_psi(atus_ctx *ctx, int comp, void **dptr);
+
+/* ------------------------------------------------------------ steps */
+ATUS_API int atus_ft_step(atus_ctx *ctx, int half);
+/* F: pulse amplitude AMP_T(t + dt/2) for ATUS_STEP_BRAGG_AD (1 without AMP_T). */
+ATUS_API int atus_nl_step(atus_ctx *ctx, int kind, double F);
+/* nk Strang steps: half, (V, full)^(nk-1), V, half.  F[j] is the pulse
+ * amplitude of the j-th potential step (NULL: all 1). */
+ATUS_API int atus_strang_block(atus_ctx *ctx, int nk, int kind, const double *F);
+
+/* ------------------------------------------------------------ measurement */
+/* Device time of the fused passes that make up one Strang step of `kind`,
+ * each launched `reps` times back to back on the context's stream and timed
+ * with CUDA events there.  ms[i] receives the average duration of one launch
+ * of pass i, launches_per_step[i] how often one Strang step launches it, and
+ * bytes[i] the field bytes one launch reads and writes (the algorithmic
+ * traffic).  *npass receives the number of pass kinds (<= 8).  The fields are
+ * advanced by the passes; restore them before using the results. */
+ATUS_API int atus_profile_passes(atus_ctx *ctx, int kind, int reps, double *ms, double *launches_per_step,
+                                 double *bytes, int *npass);
+
+/* ------------------------------------------------------------ observables */
+ATUS_API int atus_particle_number(atus_ctx *ctx, int comp, double *out);
+ATUS_API int atus_expval_position(atus_ctx *ctx, int comp, double *out /* dim */);
+ATUS_API int atus_expval_momentum(atus_ctx *ctx, int comp, double *out /* dim */);
+ATUS_API int atus_setup_momentum(atus_ctx *ctx, int comp, const double *p /* dim */);
+/* n momentum points k0 (n*dim), threshold thr: m_ar_k * sum |psi0^(k)|^2 per ball. */
+ATUS_API int atus_rabi_integrals(atus_ctx *ctx, const double *k0, int n, double thr, double *out);
+
+/* ------------------------------------------------------------ Sobolev gradient */
+/* Ground-state descent of CSOB_Base on the context's grid: alpha per
+ * component (Alpha_i[0] on every axis), gs already scaled by sqrt(N_i N_j),
+ * fixed stepsize.  The potential comes from atus_set_potential and the start
+ * from atus_upload_psi. */
+ATUS_API int atus_sob_init(atus_ctx *ctx, const double *alpha /* ncomp */, double stepsize);
+ATUS_API int atus_sob_renormalize(atus_ctx *ctx);
+/* n_iter iterations of CSOB_Base::run's loop body; res/N receive the values of
+ * the last one (N: ncomp entries). */
+ATUS_API int atus_sob_iterate(atus_ctx *ctx, int n_iter, double *res, double *N);
+/* CSOB_Base::run: renormalise, iterate until res <= epsilon (at most
+ * max_iter); iterations taken in *iters. */
+ATUS_API int atus_sob_run(atus_ctx *ctx, double epsilon, int max_iter, int *iters, double *res);
+/* mu_i = m_ar * sum[-Re(psi* Lap psi) + (V + sum_j g_ij |psi_j|^2) |psi_i|^2] */
+ATUS_API int atus_sob_mu(atus_ctx *ctx, double *mu /* ncomp */);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

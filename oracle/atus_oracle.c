@@ -36,6 +36,7 @@
 #include <string.h>
 
 #include "fft_cpu.h"
+#include <omp.h>
 
 #ifndef M_PI
 #define M_PI 3.14159265358979323846
@@ -109,6 +110,7 @@ static void scale(const orc_ctx *c, double *data, const double *s) {
   if (c->dim == 1) fak = s[0] / sqrt(2.0 * M_PI);
   else if (c->dim == 2) fak = 0.5 * s[0] * s[1] / M_PI;
   else fak = s[0] * s[1] * s[2] / pow(2 * M_PI, 1.5);
+  #pragma omp parallel for schedule(static)
   for (long i = 0; i < c->npts; i++) {
     data[2 * i] *= fak;
     data[2 * i + 1] *= fak;
@@ -204,6 +206,7 @@ void orc_set_dt(orc_ctx *c, double dt) {
     double *h = (double *)malloc(sizeof(double) * 2 * c->npts);
     double *f = (double *)malloc(sizeof(double) * 2 * c->npts);
     const double mdt = -dt;
+    #pragma omp parallel for schedule(static)
     for (long l = 0; l < c->npts; l++) {
       double k[3];
       orc_get_k(c, l, k);
@@ -227,6 +230,7 @@ void orc_ft_step(orc_ctx *c, int half) {
   for (int i = 0; i < c->ncomp; i++) {
     double *P = c->psi[i];
     const double *T = half ? c->half[i] : c->full[i];
+    #pragma omp parallel for schedule(static)
     for (long l = 0; l < c->npts; l++) {
       const double tmp1 = P[2 * l];
       P[2 * l] = P[2 * l] * T[2 * l] - P[2 * l + 1] * T[2 * l + 1];
@@ -252,6 +256,7 @@ static void apply_phases(orc_ctx *c, long l, const double *phi) {
 void orc_nl_step(orc_ctx *c) {
   const double dt = -c->dt;
   const int n = c->ncomp;
+  #pragma omp parallel for schedule(static)
   for (long l = 0; l < c->npts; l++) {
     double phi[ORC_MAXC];
     for (int i = 0; i < n; i++) {
@@ -269,6 +274,7 @@ void orc_nl_step(orc_ctx *c) {
 void orc_nl_if_step(orc_ctx *c, const orc_laser *L) {
   const double dt = -c->dt;
   const int n = c->ncomp;
+  #pragma omp parallel for schedule(static)
   for (long l = 0; l < c->npts; l++) {
     double phi[ORC_MAXC];
     for (int i = 0; i < n; i++) {
@@ -291,6 +297,7 @@ void orc_bragg_ad(orc_ctx *c, const orc_laser *L, double F) {
   const double t1 = c->t + 0.5 * dt;
   double *P1 = c->psi[0], *P2 = c->psi[1];
   const double *gs = c->gs;
+  #pragma omp parallel for schedule(static)
   for (long l = 0; l < c->npts; l++) {
     double x[3];
     orc_get_x(c, l, x);
@@ -612,4 +619,7 @@ void orc_sob_mu(orc_ctx *c, double *mu) {
 void orc_fft_raw(orc_ctx *c, double *data, int isign) {
   orc_fft_execute(isign < 0 ? c->fwd : c->bwd, data);
 }
-void orc_set_threads(int n) { orc_fft_set_threads(n); }
+void orc_set_threads(int n) {
+  orc_fft_set_threads(n);
+  if (n > 0) omp_set_num_threads(n);
+}

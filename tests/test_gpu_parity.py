@@ -1,0 +1,218 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle and the golden
+fixtures of the reference programs.
+
+Tolerances: FP64 path relative L2 <= 1e-11 against the reference / oracle
+(north-star bar); mixed path (complex64 fields, FP64 phase arguments)
+relative L2 <= 1e-5 after the stated number of steps.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from atus2_b200 import PREC_FP64, PREC_MIXED, Laser, Solver, binfmt
+from golden_io import BRAGG_CASES, RT_CASES, SOB_CASES, load, sob_inputs
+from gpu_util import rel_l2
+from oracle.oracle import Laser as OLaser
+from oracle.oracle import Oracle
+from replay import KIND_BRAGG_AD, KIND_NL, KIND_NL_IF, gaussian_pulse, run_rt
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-11
+MIXED_TOL = 1e-5
+
+
+@pytest.mark.parametrize("name", RT_CASES + BRAGG_CASES)
+def test_golden_realtime_fp64(name):
+    g = load(name)
+    p = g["params"]
+    s = Solver(g["header"], p["ncomp"], PREC_FP64)
+    outs, rabi = run_rt(s, p, g["psi0"], V=g.get("V"), make_laser=Laser.make)
+    assert len(outs) == len(g["t"])
+    for (t, psi), t_ref, psi_ref in zip(outs, g["t"], g["psi"]):
+        assert t == t_ref
+        for c in range(p["ncomp"]):
+            if np.linalg.norm(psi_ref[c]) > 1e-8:
+                assert rel_l2(psi[c], psi_ref[c]) < FP64_TOL, (name, c, t)
+            else:
+                assert np.abs(psi[c]).max() < 1e-8
+    if p["program"] == "bragg":
+        np.testing.assert_allclose(np.array(rabi), g["rabi"], rtol=5e-6, atol=1e-10)
+
+
+@pytest.mark.parametrize("name", SOB_CASES)
+def test_golden_sobmin_fp64(name):
+    g = load(name)
+    p = g["params"]
+    s = Solver(g["header"], 1, PREC_FP64)
+    guess, V = sob_inputs(p, g["header"])
+    s.set_psi(0, guess)
+    s.set_potential(0, V)
+    s.set_gs([p["g"] * math.sqrt(p["Nparticles"]) * math.sqrt(p["Nparticles"])])
+    s.sob_init([p["alpha"]], p["stepsize"])
+    it, res = s.sob_run(p["epsilon"], 100000)
+    assert abs(it - int(g["iterations"])) <= 1
+    assert res <= p["epsilon"]
+    assert rel_l2(s.psi(0) * math.sqrt(p["Nparticles"]), g["psi"]) < 1e-10
+
+
+def _grid(dim, n, L):
+    return binfmt.make_header(dim, n, [-L / 2] * dim, [L / 2] * dim)
+
+
+def _coords(h):
+    return np.meshgrid(*[binfmt.x_coords(h, a) for a in range(int(h["nDims"]))], indexing="ij")
+
+
+def _setup_pair(h, ncomp, psi0, alpha, gs, V, dt, prec=PREC_FP64):
+    o = Oracle(h, ncomp)
+    s = Solver(h, ncomp, prec)
+    for e in (o, s):
+        for c in range(ncomp):
+            e.set_psi(c, psi0[c])
+            e.set_alpha(c, alpha)
+        e.set_gs(gs)
+        if V is not None:
+            e.set_potential(0, V)
+        e.set_dt(dt)
+    return o, s
+
+
+def test_config1_1d_full_length_fp64():
+    """1D rt_solver workload: N=4096 on [-100,100), V=x^2/2, g=10, Gaussian
+    exp(-(x-5)^2/2) e^{2ix} plus 1e-6 complex noise (seed 0), dt=1e-3, 20000
+    steps in blocks of Nk=1000; psi and N compared at every block."""
+    h = _grid(1, [4096], 200.0)
+    (x,) = _coords(h)
+    rng = np.random.default_rng(0)
+    psi = np.exp(-0.5 * (x - 5) ** 2) * np.exp(2j * x) + 1e-6 * (rng.standard_normal(4096) + 1j * rng.standard_normal(4096))
+    psi /= math.sqrt(float(h["dx"]) * np.sum(np.abs(psi) ** 2))
+    o, s = _setup_pair(h, 1, [psi], [0.5], [10.0], 0.5 * x * x, 1e-3)
+    for b in range(20):
+        o.block(1000, KIND_NL)
+        s.block(1000, KIND_NL)
+        assert s.t == o.t
+        assert rel_l2(s.psi(0), o.psi(0)) < FP64_TOL, b
+        assert abs(s.particle_number(0) - o.particle_number(0)) < 1e-12
+
+
+@pytest.mark.parametrize("prec,tol", [(PREC_FP64, FP64_TOL), (PREC_MIXED, MIXED_TOL)])
+def test_2d_double_slit(prec, tol):
+    """2D double-slit workload on a reduced grid (256^2 on [-64,64)^2 keeps the
+    oracle within seconds): V=200 on |x|<0.5 except slits |y-+4|<1, packet
+    sigma=4 at x=-20 with kx=8, g=1, dt=5e-4, 400 steps."""
+    h = _grid(2, [256, 256], 128.0)
+    x, y = _coords(h)
+    V = np.where((np.abs(x) < 0.5) & ~((np.abs(y - 4) < 1) | (np.abs(y + 4) < 1)), 200.0, 0.0)
+    psi = np.exp(-((x + 20) ** 2 + y ** 2) / 32.0) * np.exp(8j * x)
+    psi /= math.sqrt(float(h["dx"] * h["dy"]) * np.sum(np.abs(psi) ** 2))
+    o, s = _setup_pair(h, 1, [psi], [0.5, 0.5], [1.0], V, 5e-4, prec)
+    for b in range(4):
+        o.block(100, KIND_NL)
+        s.block(100, KIND_NL)
+    assert rel_l2(s.psi(0), o.psi(0)) < tol
+    assert abs(s.particle_number(0) - o.particle_number(0)) < (1e-12 if prec == PREC_FP64 else 1e-6)
+
+
+def _bragg_3d(n, L, prec):
+    h = _grid(3, n, L)
+    x, y, z = _coords(h)
+    r2 = x * x + y * y + z * z
+    mu = 4.0
+    psi1 = np.sqrt(np.maximum(0.0, (mu - 0.5 * r2) / 100.0)).astype(np.complex128)
+    psi1 /= math.sqrt(float(h["dx"] * h["dy"] * h["dz"]) * np.sum(np.abs(psi1) ** 2))
+    psi2 = np.zeros_like(psi1)
+    o, s = _setup_pair(h, 2, [psi1, psi2], [0.5, 0.5, 0.5], [100.0] * 4, None, 1e-3, prec)
+    kw = dict(beta=[0, 0, 0], DeltaL=[0, 0, 0, 0], Amp=[4.0, 4.0], laser_k=[8.0, 0], laser_dk=[0, 0],
+              laser_domh=[16.0, 0], phase=[0, 0], chirp_rate=[0, 0], chirp=0.0)
+    return o, s, OLaser.make(**kw), Laser.make(**kw)
+
+
+@pytest.mark.parametrize("prec,tol", [(PREC_FP64, FP64_TOL), (PREC_MIXED, MIXED_TOL)])
+def test_3d_bragg_then_freeprop(prec, tol):
+    """3D two-component Bragg workload on a reduced grid (32x32x32 on
+    [-8,8)^3): g=100, k_L=4 (laser_k=8), delta=16, Gaussian pulse of peak 8
+    (Amp=4) centred at t=0.05; 100 bragg_ad steps then 100 freeprop steps."""
+    o, s, Lo, Ls = _bragg_3d([32, 32, 32], 16.0, prec)
+    F = gaussian_pulse(0.05, 2 * 0.02 ** 2)
+    for b in range(2):
+        t = o.t + 0.5e-3
+        Fv = []
+        for j in range(50):
+            Fv.append(F(t + 0.5e-3))
+            t += 1e-3
+        o.block(50, KIND_BRAGG_AD, Lo, np.array(Fv))
+        s.block(50, KIND_BRAGG_AD, Ls, np.array(Fv))
+    for b in range(2):
+        o.block(50, KIND_NL_IF, Lo)
+        s.block(50, KIND_NL_IF, Ls)
+    assert abs(s.t - o.t) == 0.0
+    for c in range(2):
+        assert rel_l2(s.psi(c), o.psi(c)) < tol, c
+    n_o = [o.particle_number(c) for c in range(2)]
+    n_s = [s.particle_number(c) for c in range(2)]
+    assert n_o[1] > 1e-3  # the pulse transferred population
+    np.testing.assert_allclose(n_s, n_o, rtol=(1e-11 if prec == PREC_FP64 else 1e-5))
+
+
+def test_primitives_match_oracle():
+    """ft_step, nl_step, bragg_ad, setup_momentum and the observables one by one."""
+    h = _grid(3, [16, 32, 8], 8.0)
+    x, y, z = _coords(h)
+    rng = np.random.default_rng(7)
+    psi = [np.exp(-0.5 * (x * x + y * y + z * z)) * (1 + 0.1 * rng.standard_normal(x.shape)) + 0j for _ in range(2)]
+    o, s = _setup_pair(h, 2, psi, [0.5, 0.3, 0.7], [10.0, 3.0, 3.0, 8.0], 0.5 * (x * x + y * y + z * z), 2e-3)
+    for e in (o, s):
+        e.ft_step(True)
+        e.nl_step()
+        e.ft_step(False)
+        e.setup_momentum(1, [0.5, -1.0, 2.0])
+    kw = dict(beta=[0.3, 0, 0], DeltaL=[0, -2.0, 0, 0], Amp=[3.0, 3.0], laser_k=[2.0, 0], laser_dk=[0.5, 0],
+              laser_domh=[1.0, 0], phase=[0, 0], chirp_rate=[0, 0], chirp=0.5)
+    o.bragg_ad(OLaser.make(**kw), 0.7)
+    s.bragg_ad(Laser.make(**kw), 0.7)
+    o.nl_if_step(OLaser.make(**kw))
+    s.nl_if_step(Laser.make(**kw))
+    assert s.t == o.t
+    for c in range(2):
+        assert rel_l2(s.psi(c), o.psi(c)) < 1e-13
+        assert abs(s.particle_number(c) - o.particle_number(c)) < 1e-13
+        np.testing.assert_allclose(s.expval_position(c), o.expval_position(c), atol=1e-12)
+        np.testing.assert_allclose(s.expval_momentum(c), o.expval_momentum(c), atol=1e-11)
+    k0 = [[0, 0, 0], [1.5, 0, 0], [-1.5, 0, 0]]
+    np.testing.assert_allclose(s.rabi_integrals(k0, 1.0), o.rabi_integrals(k0, 1.0), rtol=1e-12, atol=1e-14)
+
+
+def test_sobmin_mu_matches_oracle():
+    h = _grid(3, [32, 32, 16], 12.0)
+    x, y, z = _coords(h)
+    V = 0.5 * (x * x + 4 * y * y + 2.25 * z * z)
+    guess = np.sqrt(np.maximum(0.0, 3.0 - V)).astype(np.complex128) + 1e-3
+    o = Oracle(h, 1)
+    s = Solver(h, 1, PREC_FP64)
+    for e in (o, s):
+        e.set_psi(0, guess)
+        e.set_potential(0, V)
+        e.set_gs([50.0])
+        e.sob_init([0.5], 0.01)
+    o.sob_renormalize()
+    s.sob_renormalize()
+    for k in range(30):
+        ro, No = o.sob_iterate()
+        rs, Ns = s.sob_iterate()
+        assert abs(rs - ro) <= 1e-10 * ro
+    assert rel_l2(s.psi(0), o.psi(0)) < 1e-11
+    np.testing.assert_allclose(s.sob_mu(), o.sob_mu(), rtol=1e-11)
+
+
+def test_errors_are_reported():
+    from atus2_b200 import AtusError
+
+    with pytest.raises(AtusError):
+        Solver(_grid(1, [100], 10.0), 1)  # not a power of two
+    s = Solver(_grid(2, [32, 32], 10.0), 1)
+    with pytest.raises(AtusError):
+        s.block(4, KIND_BRAGG_AD)  # bragg_ad needs two components
+    with pytest.raises(AtusError):
+        s.sob_iterate()  # before sob_init
