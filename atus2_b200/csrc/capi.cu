@@ -4,6 +4,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -53,28 +54,39 @@ static double scale_fak(int dim, const double *s) {
 
 static int64_t wrapped(int64_t i, int64_t n) { return ((i + n / 2) % n) - n / 2; }
 
-template <typename R> static int build_kinetic(atus_ctx *ctx) {
-  using C = cplx<R>;
+// Scale of one forward+inverse round trip, folded into the kinetic phase.  For
+// headers written as gen_psi_0 / Get_Header write them (dx = L/N, dk = 2 pi/L)
+// the product is exactly 1/N_total, a power of two; it is used exactly then,
+// so the folded scale adds no rounding (what matters for complex64 fields).
+static double round_trip_scale(const atus_ctx *ctx) {
   const double s = scale_fak(ctx->dim, ctx->d) * scale_fak(ctx->dim, ctx->dk);
+  const double exact = 1.0 / (double)ctx->npts;
+  return (fabs(s - exact) <= 1e-12 * exact) ? exact : s;
+}
+
+// Kinetic phase factors per axis, in FP64 for both precisions, evaluated with
+// the reference's own double arithmetic (include/CRT_Base.h:257-271):
+// phi = (-dt) * ((k alpha) k), factor (cos(phi/2), sin(phi/2)) for the half
+// step and (cos phi, sin phi) for the full one.  In 1D this is the reference's
+// table bit for bit; in 2D/3D the factor of a k-point is the product of the
+// axis factors.  The transform scales stay separate (applied in the kernel).
+static int build_kinetic(atus_ctx *ctx) {
   for (int hf = 0; hf < 2; hf++) {
     for (int c = 0; c < ctx->ncomp; c++) {
       for (int ax = 0; ax < 3; ax++) {
         const int64_t n = ctx->n[ax];
-        std::vector<C> tab(n);
+        std::vector<double2> tab(n);
         for (int64_t i = 0; i < n; i++) {
-          long double ph = 0.0L;
+          double phi = 0.0;
           if (ax < ctx->dim) {
-            const long double k = (long double)ctx->dk[ax] * (long double)wrapped(i, n);
-            ph = -(long double)ctx->dt * (long double)ctx->alpha[c][ax] * k * k;
-            if (hf == 0) ph *= 0.5L;
+            const double k = ctx->dk[ax] * (double)wrapped(i, n);
+            phi = (-ctx->dt) * ((k * ctx->alpha[c][ax]) * k);
           }
-          long double cr = cosl(ph), ci = sinl(ph);
-          if (ax == 0) { cr *= s; ci *= s; }
-          tab[i].x = (R)cr;
-          tab[i].y = (R)ci;
+          tab[i].x = (hf == 0) ? cos(0.5 * phi) : cos(phi);
+          tab[i].y = (hf == 0) ? sin(0.5 * phi) : sin(phi);
         }
-        if (!ctx->kt[hf][c][ax]) CK(cudaMalloc(&ctx->kt[hf][c][ax], sizeof(C) * n));
-        CK(cudaMemcpyAsync(ctx->kt[hf][c][ax], tab.data(), sizeof(C) * n, cudaMemcpyHostToDevice, ctx->stream));
+        if (!ctx->kt[hf][c][ax]) CK(cudaMalloc(&ctx->kt[hf][c][ax], sizeof(double2) * n));
+        CK(cudaMemcpyAsync(ctx->kt[hf][c][ax], tab.data(), sizeof(double2) * n, cudaMemcpyHostToDevice, ctx->stream));
       }
     }
   }
@@ -125,6 +137,8 @@ static int run_pass(atus_ctx *ctx, int axis, int t1, int op, int t2, const NLArg
   if (op == OP_KIN)
     for (int c = 0; c < MAXC; c++)
       for (int ax = 0; ax < 3; ax++) a.kt[c][ax] = (c < ctx->ncomp) ? ctx->kt[half ? 0 : 1][c][ax] : nullptr;
+  a.s_f = scale_fak(ctx->dim, ctx->d);
+  a.s_b = scale_fak(ctx->dim, ctx->dk);
   if (nl) a.nl = *nl;
   // per-component passes launch ncomp CTAs in y; override when the field set differs
   if (a.per_comp && nf != ctx->ncomp) {
@@ -151,9 +165,38 @@ static int run_pass(atus_ctx *ctx, int axis, int t1, int op, int t2, const NLArg
     if (_r != ATUS_OK) return _r; \
   } while (0)
 
+// One cluster slab pass over the context's fields (3D); ATUS_E_UNSUPPORTED
+// when the grid has no slab kernel, after which the axis passes are used.
+static int slab_pass(atus_ctx *ctx, int load_rows, int inv_y, int inv_z, const NLArgs *nl, int fwd_z, int fwd_y,
+                     int store_rows) {
+  if (!ctx->use_slab || ctx->dim != 3 || ctx->ncomp > 2) return ATUS_E_UNSUPPORTED;
+  SlabArgs a;
+  memset(&a, 0, sizeof(a));
+  for (int c = 0; c < MAXC; c++) a.psi[c] = ctx->psi[c];
+  a.nc = ctx->ncomp;
+  a.load_rows = load_rows;
+  a.inv_y = inv_y;
+  a.inv_z = inv_z;
+  a.fwd_z = fwd_z;
+  a.fwd_y = fwd_y;
+  a.store_rows = store_rows;
+  if (nl) {
+    a.nl = *nl;
+    a.do_nl = 1;
+  }
+  const int tc = tc_for(ctx->ncomp);
+  const int r = (ctx->prec == ATUS_PREC_FP64) ? launch_slab_d(ctx, a, tc) : launch_slab_f(ctx, a, tc);
+  if (r == ATUS_E_UNSUPPORTED) ctx->use_slab = false;
+  return r;
+}
+
 // Forward (dir -1) or inverse (+1) transform of the axes other than 0.
 static int transform_inner(atus_ctx *ctx, int dir, void *const *f = nullptr, int nf = -1) {
   if (ctx->dim == 2) return run_pass(ctx, 1, dir, OP_NONE, T_NONE, nullptr, 0, f, nf);
+  if (ctx->dim == 3 && f == nullptr) {
+    const int r = (dir == T_FWD) ? slab_pass(ctx, 1, 0, 0, nullptr, 1, 1, 0) : slab_pass(ctx, 0, 1, 1, nullptr, 0, 0, 1);
+    if (r != ATUS_E_UNSUPPORTED) return r;
+  }
   if (ctx->dim == 3) {
     if (dir == T_FWD) {
       RUN(run_pass(ctx, 2, T_FWD, OP_NONE, T_NONE, nullptr, 0, f, nf));
@@ -172,6 +215,10 @@ static int kinetic_pass(atus_ctx *ctx, int half) {
 
 // Real-space potential pass: 2D one pass over rows; 3D inverse y, rows, forward y.
 static int potential_pass(atus_ctx *ctx, const NLArgs &nl) {
+  if (ctx->dim == 3) {
+    const int r = slab_pass(ctx, 0, 1, 1, &nl, 1, 1, 0);
+    if (r != ATUS_E_UNSUPPORTED) return r;
+  }
   const int last = ctx->dim - 1;
   if (ctx->dim == 3) RUN(run_pass(ctx, 1, T_INV, OP_NONE, T_NONE, nullptr, 0));
   RUN(run_pass(ctx, last, T_INV, OP_NL, T_FWD, &nl, 0));
@@ -264,6 +311,10 @@ int atus_create(const atus_grid *grid, int ncomp, int precision, atus_ctx **out)
   else if (grid->dim == 2) { ctx->ar = ctx->d[0] * ctx->d[1]; ctx->ar_k = ctx->dk[0] * ctx->dk[1]; }
   else { ctx->ar = ctx->d[0] * ctx->d[1] * ctx->d[2]; ctx->ar_k = ctx->dk[0] * ctx->dk[1] * ctx->dk[2]; }
   ctx->t = grid->t;
+  {
+    const char *e = getenv("ATUS_SLAB");  // ATUS_SLAB=0: axis passes only (A/B measurements)
+    ctx->use_slab = !(e && e[0] == '0');
+  }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) { delete ctx; return ATUS_E_CUDA; }
   if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return ATUS_E_CUDA; }
@@ -297,7 +348,7 @@ int atus_create(const atus_grid *grid, int ncomp, int precision, atus_ctx **out)
     return ATUS_E_NOMEM;
   }
   // CRT_Base's constructor builds the tables once (alpha still zero).
-  int r = precision == ATUS_PREC_FP64 ? build_kinetic<double>(ctx) : build_kinetic<float>(ctx);
+  int r = build_kinetic(ctx);
   if (r != ATUS_OK) {
     atus_destroy(ctx);
     return r;
@@ -358,7 +409,7 @@ int atus_set_alpha(atus_ctx *ctx, int comp, const double *alpha) {
 int atus_set_dt(atus_ctx *ctx, double dt) {
   if (!ctx) return ATUS_E_ARG;
   ctx->dt = dt;
-  return ctx->prec == ATUS_PREC_FP64 ? build_kinetic<double>(ctx) : build_kinetic<float>(ctx);
+  return build_kinetic(ctx);
 }
 
 int atus_get_dt(const atus_ctx *ctx, double *dt) {
@@ -483,6 +534,8 @@ int atus_strang_block(atus_ctx *ctx, int nk, int kind, const double *F) {
       a.kh[c] = (c < ctx->ncomp) ? ctx->kt[0][c][0] : nullptr;
       a.kf[c] = (c < ctx->ncomp) ? ctx->kt[1][c][0] : nullptr;
     }
+    a.s_f = scale_fak(ctx->dim, ctx->d);
+    a.s_b = scale_fak(ctx->dim, ctx->dk);
     a.tw = ctx->tw;
     a.nl = nl_args(ctx, kind, 0.0, 1.0);
     a.nk = nk;
@@ -563,15 +616,28 @@ int atus_profile_passes(atus_ctx *ctx, int kind, int reps, double *ms, double *l
     auto kin = [&]() { return kinetic_pass(ctx, 0); };
     r = timed(kin, 1.0, fb);
     const int last = ctx->dim - 1;
-    if (r == ATUS_OK && ctx->dim == 3) {
+    bool slab_done = false;
+    if (r == ATUS_OK && ctx->dim == 3) {  // the fused (y,z) cluster pass, when the grid has one
+      const int probe = slab_pass(ctx, 0, 1, 1, &nl, 1, 1, 0);
+      if (probe == ATUS_OK) {
+        auto slab = [&]() { return slab_pass(ctx, 0, 1, 1, &nl, 1, 1, 0); };
+        r = timed(slab, 1.0, fb + vb);
+        slab_done = true;
+      } else if (probe != ATUS_E_UNSUPPORTED) {
+        r = probe;
+      }
+    }
+    if (slab_done) {
+      // one cluster pass replaces the three axis passes below
+    } else if (r == ATUS_OK && ctx->dim == 3) {
       auto yinv = [&]() { return run_pass(ctx, 1, T_INV, OP_NONE, T_NONE, nullptr, 0); };
       r = timed(yinv, 1.0, fb);
     }
-    if (r == ATUS_OK) {
+    if (r == ATUS_OK && !slab_done) {
       auto pot = [&]() { return run_pass(ctx, last, T_INV, OP_NL, T_FWD, &nl, 0); };
       r = timed(pot, 1.0, fb + vb);
     }
-    if (r == ATUS_OK && ctx->dim == 3) {
+    if (r == ATUS_OK && ctx->dim == 3 && !slab_done) {
       auto yfwd = [&]() { return run_pass(ctx, 1, T_FWD, OP_NONE, T_NONE, nullptr, 0); };
       r = timed(yfwd, 1.0, fb);
     }
@@ -682,7 +748,7 @@ static int sob_filter(atus_ctx *ctx, void *buf, int mode, double alpha) {
     a.nc = 1;
     a.filt_mode = mode;
     a.filt_alpha = alpha;
-    a.filt_scale = scale_fak(ctx->dim, ctx->d) * scale_fak(ctx->dim, ctx->dk);
+    a.filt_scale = round_trip_scale(ctx);
     const int saved_nc = ctx->ncomp;
     ctx->ncomp = 1;
     r = launch_pass_d1(ctx, a, 0);

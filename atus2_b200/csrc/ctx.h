@@ -25,10 +25,11 @@ struct atus_ctx {
   void *scratch = nullptr;      // N complex128 (FP64 staging / spectra)
   void *tw = nullptr;           // twiddles in the field precision
   void *tw64 = nullptr;         // FP64 twiddles (spectra of the FP64 scratch buffer)
-  void *kt[2][MAXC][3] = {};    // [half=0/full=1][comp][axis]
+  double2 *kt[2][MAXC][3] = {}; // kinetic phase factors [half=0/full=1][comp][axis], FP64
   double *red_partial = nullptr, *red_out = nullptr, *h_red = nullptr;
   cudaStream_t own_stream = nullptr, stream = nullptr;
   int64_t launches = 0;
+  bool use_slab = true;         // 3D: fused (y,z) cluster pass when available
   std::string err;
   // Sobolev state
   bool sob_ready = false;

@@ -46,9 +46,12 @@ template <int DIR, typename C> __device__ __forceinline__ C mul_i(C a) {
   return r;
 }
 
-// Shared-memory index of element i of pencil b: one pad element per 16.
+// Shared-memory index of element i of pencil b: one pad element per 16 inside
+// a pencil (radix-16 stores), and an odd pencil pitch NP so that the same
+// element of consecutive pencils falls into different banks (tile loads that
+// walk across pencils, and the cluster transposes).
 template <int N> struct Pad {
-  static constexpr int NP = (N >= 16) ? (N + N / 16) : N;
+  static constexpr int NP = ((N >= 16) ? (N + N / 16) : N) | 1;
   static __device__ __forceinline__ int idx(int b, int i) { return b * NP + ((N >= 16) ? (i + (i >> 4)) : i); }
   static constexpr int words(int B) { return B * NP; }
 };

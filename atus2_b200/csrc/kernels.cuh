@@ -26,8 +26,10 @@ constexpr int TWN = 8192;  // twiddle table length (largest supported pencil)
 
 // Per-CTA tile budget in complex elements and threads per CTA.
 template <typename R> struct Tile;
-template <> struct Tile<double> { static constexpr int E = 4096; static constexpr int NT = 256; };
-template <> struct Tile<float> { static constexpr int E = 8192; static constexpr int NT = 512; };
+// MINB: CTAs per SM the register budget is sized for (two tiles resident per
+// SM, so one CTA's loads overlap the other's transforms).
+template <> struct Tile<double> { static constexpr int E = 4096; static constexpr int NT = 256; static constexpr int MINB = 2; };
+template <> struct Tile<float> { static constexpr int E = 8192; static constexpr int NT = 512; static constexpr int MINB = 2; };
 
 enum { T_NONE = 0, T_FWD = -1, T_INV = 1 };
 enum { OP_NONE = 0, OP_KIN = 1, OP_NL = 2, OP_FILT = 3 };
@@ -66,7 +68,8 @@ struct PassArgs {
   int64_t inner_tiles;      // strided: tiles per outer block; contiguous: unused
   int64_t npencils;         // contiguous: number of pencils
   int t1, op, t2;
-  const void *kt[MAXC][3];  // kinetic phase tables per component and axis
+  const double2 *kt[MAXC][3];  // kinetic phase factors per component and axis (FP64)
+  double s_f, s_b;          // forward / backward transform scales (cft_*d::scale)
   const void *tw;           // twiddles exp(-2 pi i m / TWN)
   Geo g;
   NLArgs nl;
@@ -96,17 +99,56 @@ __device__ __forceinline__ double reduce_2pi(double a) {
   return fma(-q, P3, r);
 }
 
-// e^{i phi} with an FP64 argument.
-template <typename R> __device__ __forceinline__ cplx<R> expi(double phi);
+// sin and cos of an FP64 argument.  The phases of a time step are small
+// (|dt V| << 1 in practice), so |x| <= 1/32 takes the Taylor polynomials
+//   sin x = x (1 - x^2/3! + x^4/5! - x^6/7! + x^8/9!)
+//   cos x = 1 - x^2/2! + x^4/4! - x^6/6! + x^8/8! - x^10/10!
+// whose truncation errors (x^11/11!, x^12/12!) are below 2^-70 there, in
+// Horner form on x^2; larger arguments call sincos().
+__device__ __forceinline__ void sincos_step(double x, double *s, double *c) {
+  if (fabs(x) <= 0.03125) {
+    const double x2 = x * x;
+    double ps = fma(x2, 1.0 / 362880.0, -1.0 / 5040.0);
+    ps = fma(ps, x2, 1.0 / 120.0);
+    ps = fma(ps, x2, -1.0 / 6.0);
+    *s = fma(ps * x2, x, x);
+    double pc = fma(x2, -1.0 / 3628800.0, 1.0 / 40320.0);
+    pc = fma(pc, x2, -1.0 / 720.0);
+    pc = fma(pc, x2, 1.0 / 24.0);
+    pc = fma(pc, x2, -0.5);
+    *c = fma(pc, x2, 1.0);
+  } else {
+    sincos(x, s, c);
+  }
+}
+
+// Element of MAXC-entry arrays by a runtime index without local memory.
+template <typename T> __device__ __forceinline__ T pick(const T (&a)[MAXC], int i) {
+  T r = a[0];
+  if (i == 1) r = a[1];
+  if (i == 2) r = a[2];
+  if (i == 3) r = a[3];
+  return r;
+}
+
+template <typename R> __device__ __forceinline__ double2 to_d(cplx<R> v) { return make_double2((double)v.x, (double)v.y); }
+template <typename R> __device__ __forceinline__ cplx<R> from_d(double2 v) { return mk<R>((R)v.x, (R)v.y); }
+
+// Unit phase factor e^{i phi} in FP64.  Mixed precision: FP64 argument
+// reduced modulo 2 pi, sincosf, then renormalised in FP64 so that |e| = 1 to
+// FP64 accuracy (a fixed modulus error would drift the norm every step).
+template <typename R> __device__ __forceinline__ double2 expi(double phi);
 template <> __device__ __forceinline__ double2 expi<double>(double phi) {
   double s, c;
-  sincos(phi, &s, &c);
+  sincos_step(phi, &s, &c);
   return make_double2(c, s);
 }
-template <> __device__ __forceinline__ float2 expi<float>(double phi) {
+template <> __device__ __forceinline__ double2 expi<float>(double phi) {
   float s, c;
   sincosf((float)reduce_2pi(phi), &s, &c);
-  return make_float2(c, s);
+  const double cd = c, sd = s;
+  const double inv = rsqrt(cd * cd + sd * sd);
+  return make_double2(cd * inv, sd * inv);
 }
 
 // ------------------------------------------------------------ potential step
@@ -141,8 +183,8 @@ __device__ __forceinline__ void nl_point(const NLArgs &a, cplx<R> *v, int64_t l,
         phi += a.L.beta0 * x0 - a.L.DeltaL[i];
       }
       phi *= a.mdt;
-      const C e = expi<R>(phi);
-      v[i] = cmul(v[i], e);
+      const double2 e = expi<R>(phi);
+      v[i] = from_d<R>(cmul(to_d<R>(v[i]), e));
     }
     return;
   }
@@ -153,9 +195,9 @@ __device__ __forceinline__ void nl_point(const NLArgs &a, cplx<R> *v, int64_t l,
   if constexpr (sizeof(R) == 8) {
     double re1, im1;
     if (Omega == 0.0) {
-      sincos(-dt * V11, &im1, &re1);
+      sincos_step(-dt * V11, &im1, &re1);
       v[0] = cmul(v[0], make_double2(re1, im1));
-      sincos(-dt * V22, &im1, &re1);
+      sincos_step(-dt * V22, &im1, &re1);
       v[1] = cmul(v[1], make_double2(re1, im1));
       return;
     }
@@ -163,10 +205,10 @@ __device__ __forceinline__ void nl_point(const NLArgs &a, cplx<R> *v, int64_t l,
     const double Ep = 0.5 * (V11 + V22 + tmp1);
     const double Em = 0.5 * (V11 + V22 - tmp1);
     double2 gp, gm;
-    sincos(-dt * Ep, &im1, &re1);
+    sincos_step(-dt * Ep, &im1, &re1);
     tmp1 = 1.0 / fabs((V11 - Ep) * (V11 - Ep) + Omega * Omega);
     gp = make_double2(tmp1 * re1, tmp1 * im1);
-    sincos(-dt * Em, &im1, &re1);
+    sincos_step(-dt * Em, &im1, &re1);
     tmp1 = 1.0 / fabs((V11 - Em) * (V11 - Em) + Omega * Omega);
     gm = make_double2(tmp1 * re1, tmp1 * im1);
     const double O2 = Omega * Omega;
@@ -183,23 +225,23 @@ __device__ __forceinline__ void nl_point(const NLArgs &a, cplx<R> *v, int64_t l,
   } else {
     // U = e^{-i dt m} [cos(r dt) I - i sin(r dt)/r [[d, W], [W, -d]]], m = (V11+V22)/2,
     // d = (V11-V22)/2, W = Omega, r = sqrt(d^2 + W^2); off-diagonals times eta / conj(eta).
+    // The matrix is built in FP64 from renormalised (cos, sin) pairs, so it is
+    // unitary to FP64 accuracy; only the fields are complex64.
     const double m = 0.5 * (V11 + V22), d = 0.5 * (V11 - V22);
     const double r = sqrt(d * d + Omega * Omega);
-    float sm, cm, sr, cr;
-    sincosf((float)reduce_2pi(-dt * m), &sm, &cm);
-    sincosf((float)reduce_2pi(dt * r), &sr, &cr);
-    const float sr_over_r = (r > 0.0) ? (float)((double)sr / r) : (float)dt;
-    const float fd = sr_over_r * (float)d, fw = sr_over_r * (float)Omega;
-    // U11 = e(cr - i fd), U22 = e(cr + i fd), Uoff = e(-i fw)
-    const float2 e = make_float2(cm, sm);
-    const float2 U11 = cmul(e, make_float2(cr, -fd));
-    const float2 U22 = cmul(e, make_float2(cr, fd));
-    const float2 Uo = cmul(e, make_float2(0.f, -fw));
-    const float2 et = make_float2((float)eta_c, (float)eta_s);
-    const float2 U12 = cmul(Uo, et), U21 = cmulc(Uo, et);
-    const float2 p1 = v[0], p2 = v[1];
-    v[0] = cadd(cmul(U11, p1), cmul(U12, p2));
-    v[1] = cadd(cmul(U21, p1), cmul(U22, p2));
+    const double2 e = expi<float>(-dt * m);   // e^{-i dt m}
+    const double2 rr = expi<float>(dt * r);   // (cos r dt, sin r dt)
+    const double sor = (r > 0.0) ? rr.y / r : dt;
+    const double fd = sor * d, fw = sor * Omega;
+    // U11 = e(cos - i fd), U22 = e(cos + i fd), Uoff = e(-i fw)
+    const double2 U11 = cmul(e, make_double2(rr.x, -fd));
+    const double2 U22 = cmul(e, make_double2(rr.x, fd));
+    const double2 Uo = cmul(e, make_double2(0.0, -fw));
+    const double2 et = make_double2(eta_c, eta_s);
+    const double2 U12 = cmul(Uo, et), U21 = cmulc(Uo, et);
+    const double2 p1 = to_d<R>(v[0]), p2 = to_d<R>(v[1]);
+    v[0] = from_d<R>(cadd(cmul(U11, p1), cmul(U12, p2)));
+    v[1] = from_d<R>(cadd(cmul(U21, p1), cmul(U22, p2)));
   }
 }
 
@@ -229,7 +271,7 @@ struct PassCfg {
 };
 
 template <typename R, int N, int TC>
-__global__ void __launch_bounds__(Tile<R>::NT) pass_kernel(PassArgs a) {
+__global__ void __launch_bounds__(Tile<R>::NT, Tile<R>::MINB) pass_kernel(PassArgs a) {
   using C = cplx<R>;
   using Cfg = PassCfg<R, N, TC>;
   constexpr int B = Cfg::B, NT = Cfg::NT, NP = Cfg::NP;
@@ -256,22 +298,29 @@ __global__ void __launch_bounds__(Tile<R>::NT) pass_kernel(PassArgs a) {
     nb = (int)((a.npencils - p0) < B ? (a.npencils - p0) : B);
   }
   C *fld[TC];
-  {
-    void *P[MAXC];
-    #pragma unroll
-    for (int c = 0; c < MAXC; c++) P[c] = a.psi[c];
-    #pragma unroll
-    for (int c = 0; c < TC; c++) fld[c] = (C *)P[(comp0 + c) < MAXC ? (comp0 + c) : 0];
-  }
-  // load
+  #pragma unroll
+  for (int c = 0; c < TC; c++) fld[c] = (C *)pick(a.psi, comp0 + c);
+  // load: all of a thread's loads are issued before the first shared-memory
+  // store, so each thread keeps B*N/NT requests in flight
+  static_assert((B * N) % NT == 0, "tile must be a multiple of the CTA size");
+  constexpr int LPT = B * N / NT;
   #pragma unroll
   for (int c = 0; c < TC; c++) {
-    for (int r = threadIdx.x; r < B * N; r += NT) {
+    C val[LPT];
+    #pragma unroll
+    for (int k = 0; k < LPT; k++) {
+      const int r = threadIdx.x + k * NT;
       int b, i;
       if (a.sa > 1) { b = r % B; i = r / B; } else { i = r % N; b = r / N; }
-      C val = mk<R>(0, 0);
-      if (c < nc && b < nb) val = fld[c][base0 + b * pstride + (int64_t)i * a.sa];
-      s[c * B * NP + Pad<N>::idx(b, i)] = val;
+      val[k] = mk<R>(0, 0);
+      if (c < nc && b < nb) val[k] = fld[c][base0 + b * pstride + (int64_t)i * a.sa];
+    }
+    #pragma unroll
+    for (int k = 0; k < LPT; k++) {
+      const int r = threadIdx.x + k * NT;
+      int b, i;
+      if (a.sa > 1) { b = r % B; i = r / B; } else { i = r % N; b = r / N; }
+      s[c * B * NP + Pad<N>::idx(b, i)] = val[k];
     }
   }
   __syncthreads();
@@ -280,24 +329,28 @@ __global__ void __launch_bounds__(Tile<R>::NT) pass_kernel(PassArgs a) {
   else if (a.t1 == T_INV) fft_tile<R, N, TC * B, NT, +1, TWN>(s, tw);
 
   if (a.op == OP_KIN) {
-    const C *kx, *ky, *kz;
-    {
-      const void *T[MAXC][3];
-      #pragma unroll
-      for (int c = 0; c < MAXC; c++)
-        #pragma unroll
-        for (int ax = 0; ax < 3; ax++) T[c][ax] = a.kt[c][ax];
-      kx = (const C *)T[comp0][0]; ky = (const C *)T[comp0][1]; kz = (const C *)T[comp0][2];
-    }
+    // psi^ <- ((psi^ s_f) K) s_b with K = Kx Ky Kz in FP64: the two scales of
+    // the reference's ft(-1) / ft(+1) as separate products (no folded,
+    // once-rounded constant that would bias every step the same way)
+    const double2 *kx = a.kt[0][0], *ky = a.kt[0][1], *kz = a.kt[0][2];
+    #pragma unroll
+    for (int c = 1; c < MAXC; c++)
+      if (comp0 == c) { kx = a.kt[c][0]; ky = a.kt[c][1]; kz = a.kt[c][2]; }
     for (int e = threadIdx.x; e < B * N; e += NT) {
       const int b = e / N, i = e % N;
       if (b < nb) {
         const int64_t l = base0 + b * pstride + (int64_t)i * a.sa;
         int ix, iy, iz;
         idx3(a.g, l, ix, iy, iz);
-        const C k = kin_phase(kx, ky, kz, ix, iy, iz);
+        const double2 k = kin_phase(kx, ky, kz, ix, iy, iz);
         const int si = Pad<N>::idx(b, i);
-        s[si] = cmul(s[si], k);
+        double2 v = to_d<R>(s[si]);
+        v.x *= a.s_f;
+        v.y *= a.s_f;
+        v = cmul(v, k);
+        v.x *= a.s_b;
+        v.y *= a.s_b;
+        s[si] = from_d<R>(v);
       }
     }
     __syncthreads();
@@ -367,7 +420,9 @@ __global__ void __launch_bounds__(Tile<R>::NT) pass_kernel(PassArgs a) {
   #pragma unroll
   for (int c = 0; c < TC; c++) {
     if (c < nc) {
-      for (int r = threadIdx.x; r < B * N; r += NT) {
+      #pragma unroll
+      for (int k = 0; k < LPT; k++) {
+        const int r = threadIdx.x + k * NT;
         int b, i;
         if (a.sa > 1) { b = r % B; i = r / B; } else { i = r % N; b = r / N; }
         if (b < nb) fld[c][base0 + b * pstride + (int64_t)i * a.sa] = s[c * B * NP + Pad<N>::idx(b, i)];
@@ -379,7 +434,8 @@ __global__ void __launch_bounds__(Tile<R>::NT) pass_kernel(PassArgs a) {
 // ------------------------------------------------------------ 1D Strang block
 struct Block1DArgs {
   void *psi[MAXC];
-  const void *kh[MAXC], *kf[MAXC];  // half / full kinetic tables (scale folded in)
+  const double2 *kh[MAXC], *kf[MAXC];  // half / full kinetic phase factors (FP64)
+  double s_f, s_b;                     // forward / backward transform scales
   const void *tw;
   NLArgs nl;
   int nk;
@@ -388,15 +444,20 @@ struct Block1DArgs {
 };
 
 template <typename R, int N, int TC>
-__device__ __forceinline__ void kin_1d(cplx<R> *s, const cplx<R> *const (&tab)[TC], int nc) {
-  using C = cplx<R>;
+__device__ __forceinline__ void kin_1d(cplx<R> *s, const double2 *const (&tab)[TC], int nc, double s_f, double s_b) {
   constexpr int NT = Tile<R>::NT, NP = Pad<N>::NP;
   #pragma unroll
   for (int c = 0; c < TC; c++) {
     if (c < nc) {
       for (int i = threadIdx.x; i < N; i += NT) {
-        C &x = s[c * NP + Pad<N>::idx(0, i)];
-        x = cmul(x, __ldg(&tab[c][i]));
+        const int si = c * NP + Pad<N>::idx(0, i);
+        double2 v = to_d<R>(s[si]);
+        v.x *= s_f;
+        v.y *= s_f;
+        v = cmul(v, __ldg(&tab[c][i]));
+        v.x *= s_b;
+        v.y *= s_b;
+        s[si] = from_d<R>(v);
       }
     }
   }
@@ -412,12 +473,12 @@ __global__ void __launch_bounds__(Tile<R>::NT) block1d_kernel(Block1DArgs a) {
   const int nc = a.nl.ncomp;
   const C *tw = (const C *)a.tw;
   C *fld[TC];
-  const C *kh[TC], *kf[TC];
+  const double2 *kh[TC], *kf[TC];
   #pragma unroll
   for (int c = 0; c < TC; c++) {
     fld[c] = (C *)a.psi[c];
-    kh[c] = (const C *)a.kh[c];
-    kf[c] = (const C *)a.kf[c];
+    kh[c] = a.kh[c];
+    kf[c] = a.kf[c];
   }
   #pragma unroll
   for (int c = 0; c < TC; c++)
@@ -427,7 +488,7 @@ __global__ void __launch_bounds__(Tile<R>::NT) block1d_kernel(Block1DArgs a) {
   const double dt = a.nl.dt;
   // half kinetic step
   fft_tile<R, N, TC, NT, -1, TWN>(s, tw);
-  kin_1d<R, N, TC>(s, kh, nc);
+  kin_1d<R, N, TC>(s, kh, nc, a.s_f, a.s_b);
   fft_tile<R, N, TC, NT, +1, TWN>(s, tw);
   t += 0.5 * dt;
   NLArgs nl = a.nl;
@@ -448,8 +509,8 @@ __global__ void __launch_bounds__(Tile<R>::NT) block1d_kernel(Block1DArgs a) {
     __syncthreads();
     const bool last = (j == a.nk - 1);
     fft_tile<R, N, TC, NT, -1, TWN>(s, tw);
-    if (last) kin_1d<R, N, TC>(s, kh, nc);
-    else kin_1d<R, N, TC>(s, kf, nc);
+    if (last) kin_1d<R, N, TC>(s, kh, nc, a.s_f, a.s_b);
+    else kin_1d<R, N, TC>(s, kf, nc, a.s_f, a.s_b);
     fft_tile<R, N, TC, NT, +1, TWN>(s, tw);
     t += last ? 0.5 * dt : dt;
   }
@@ -498,7 +559,7 @@ __global__ void momentum_kernel(void *psi, Geo g, double p0, double p1, double p
     idx3(g, l, ix, iy, iz);
     const double dot = p0 * ((double)(ix - s0) * dx0) + p1 * ((double)(iy - s1) * dx1) + p2 * ((double)(iz - s2) * dx2);
     C *P = (C *)psi;
-    P[l] = cmul(P[l], expi<R>(dot));
+    P[l] = from_d<R>(cmul(to_d<R>(P[l]), expi<R>(dot)));
   }
 }
 

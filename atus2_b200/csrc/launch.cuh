@@ -12,6 +12,10 @@ static inline int launch_pass_t(atus_ctx *ctx, PassArgs &a, int axis) {
   static bool attr_set = false;
   if (!attr_set) {
     CK(cudaFuncSetAttribute(pass_kernel<R, N, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // all of the unified L1/shared storage as shared memory: the tiles are
+    // the working set, global accesses are streaming
+    CK(cudaFuncSetAttribute(pass_kernel<R, N, TC>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                            cudaSharedmemCarveoutMaxShared));
     attr_set = true;
   }
   int64_t sa = 1;

@@ -327,7 +327,8 @@ def atus_arm(args, rank, ws, local, dist):
     from atus2_b200 import PREC_FP64, PREC_MIXED, STEP_BRAGG_AD
 
     torch.cuda.set_device(local)
-    stream = torch.cuda.current_stream()
+    # a stream of its own: the library launches on it and the events are recorded on it
+    stream = torch.cuda.Stream()
     peak, peak_kind = peaks()
     with ClockSampler(local) as clk:
         barrier(dist)
