@@ -73,7 +73,33 @@ def build(jobs: int | None = None, force: bool = False, verbose: bool = False) -
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
         os.replace(tmp, LIB)
+    build_programs(verbose=verbose)
     return LIB
+
+
+HOST = os.path.join(HERE, "host")
+PROGRAMS = ("rt_solver", "bragg", "sobmin", "gen_psi_0")
+
+
+def build_programs(verbose: bool = False) -> None:
+    """The XML programs (host/programs/*.cpp) linked against libatus_gpu.so,
+    found at run time next to the package (rpath $ORIGIN/../..)."""
+    out = os.path.join(HOST, "bin")
+    os.makedirs(out, exist_ok=True)
+    deps = [LIB] + glob.glob(os.path.join(HOST, "*.h")) + [os.path.join(INCLUDE, "atus_gpu.h")]
+    newest = max(os.path.getmtime(d) for d in deps)
+    for p in PROGRAMS:
+        src = os.path.join(HOST, "programs", p + ".cpp")
+        exe = os.path.join(out, p)
+        if os.path.exists(exe) and os.path.getmtime(exe) >= max(newest, os.path.getmtime(src)):
+            continue
+        cmd = ["g++", "-O2", "-std=c++17", "-fopenmp", "-I", INCLUDE, "-o", exe, src, "-L", HERE,
+               "-l:libatus_gpu.so", "-Wl,-rpath,$ORIGIN/../.."]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"g++ failed on {p}:\n{r.stdout}\n{r.stderr}")
+        if verbose:
+            print("built", exe)
 
 
 if __name__ == "__main__":

@@ -312,8 +312,10 @@ int atus_create(const atus_grid *grid, int ncomp, int precision, atus_ctx **out)
   else { ctx->ar = ctx->d[0] * ctx->d[1] * ctx->d[2]; ctx->ar_k = ctx->dk[0] * ctx->dk[1] * ctx->dk[2]; }
   ctx->t = grid->t;
   {
-    const char *e = getenv("ATUS_SLAB");  // ATUS_SLAB=0: axis passes only (A/B measurements)
-    ctx->use_slab = !(e && e[0] == '0');
+    // ATUS_SLAB=1: 3D real-space passes as one cluster slab pass instead of
+    // three axis passes (measured slower on B200 so far; kept for A/B runs)
+    const char *e = getenv("ATUS_SLAB");
+    ctx->use_slab = (e && e[0] == '1');
   }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) { delete ctx; return ATUS_E_CUDA; }

@@ -28,8 +28,10 @@ constexpr int TWN = 8192;  // twiddle table length (largest supported pencil)
 template <typename R> struct Tile;
 // MINB: CTAs per SM the register budget is sized for (two tiles resident per
 // SM, so one CTA's loads overlap the other's transforms).
-template <> struct Tile<double> { static constexpr int E = 4096; static constexpr int NT = 256; static constexpr int MINB = 2; };
-template <> struct Tile<float> { static constexpr int E = 8192; static constexpr int NT = 512; static constexpr int MINB = 2; };
+template <> struct Tile<double> { static constexpr int E = 2048; static constexpr int NT = 128; static constexpr int MINB = 3; };
+template <> struct Tile<float> { static constexpr int E = 4096; static constexpr int NT = 256; static constexpr int MINB = 3; };
+
+constexpr int BLOCK1D_NT = 256;  // threads of the resident 1D Strang-block kernel
 
 enum { T_NONE = 0, T_FWD = -1, T_INV = 1 };
 enum { OP_NONE = 0, OP_KIN = 1, OP_NL = 2, OP_FILT = 3 };
@@ -67,6 +69,8 @@ struct PassArgs {
   int64_t sa;               // pencil stride in elements
   int64_t inner_tiles;      // strided: tiles per outer block; contiguous: unused
   int64_t npencils;         // contiguous: number of pencils
+  int64_t ntiles;           // tiles per component
+  int ncomp_grid;           // components walked by per-component passes
   int t1, op, t2;
   const double2 *kt[MAXC][3];  // kinetic phase factors per component and axis (FP64)
   double s_f, s_b;          // forward / backward transform scales (cft_*d::scale)
@@ -260,6 +264,19 @@ __device__ __forceinline__ C kin_phase(const C *kx, const C *ky, const C *kz, in
 }
 
 // ------------------------------------------------------------ pass kernel
+// Asynchronous global -> shared copies (cp.async): a tile's loads are issued
+// without registers and complete while the previous tile is transformed.
+__device__ __forceinline__ void cp_async(void *smem, const void *gmem, double2) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async(void *smem, const void *gmem, float2) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::); }
+
 template <typename R, int N, int TC>
 struct PassCfg {
   static constexpr int NT = Tile<R>::NT;
@@ -267,168 +284,212 @@ struct PassCfg {
   static constexpr int B1 = B0 > 0 ? B0 : 1;
   static constexpr int B = B1 < 256 ? B1 : 256;  // pencils per tile
   static constexpr int NP = Pad<N>::NP;
-  static constexpr size_t smem = sizeof(cplx<R>) * (size_t)TC * B * NP;
+  static constexpr int TILE = TC * B * NP;       // complex values per buffer
+  // two buffers (prefetch of the next work item) when they fit, else one
+  static constexpr int NBUF = (2 * sizeof(cplx<R>) * (size_t)TILE + 3 * 8 * B <= 227 * 1024) ? 2 : 1;
+  static constexpr size_t smem = NBUF * sizeof(cplx<R>) * (size_t)TILE;
 };
 
+struct TileGeo {
+  int64_t base0;    // grid index of element 0 of pencil 0
+  int64_t pstride;  // distance between the tile's pencils
+  int nb;           // pencils of the tile inside the grid
+  int comp0;        // first component
+};
+
+template <int B, int N>
+__device__ __forceinline__ TileGeo tile_geo(const PassArgs &a, int64_t w) {
+  TileGeo g;
+  int64_t t = w;
+  g.comp0 = 0;
+  if (a.per_comp) {
+    g.comp0 = (int)(w / a.ntiles);
+    t = w % a.ntiles;
+  }
+  if (a.sa > 1) {
+    const int64_t o = t / a.inner_tiles;
+    const int64_t r0 = (t % a.inner_tiles) * B;
+    g.base0 = o * (int64_t)N * a.sa + r0;
+    g.pstride = 1;
+    g.nb = (int)((a.sa - r0) < B ? (a.sa - r0) : B);
+  } else {
+    const int64_t p0 = t * B;
+    g.base0 = p0 * N;
+    g.pstride = N;
+    g.nb = (int)((a.npencils - p0) < B ? (a.npencils - p0) : B);
+  }
+  return g;
+}
+
+// Persistent pass kernel: each CTA walks work items (tile, component) with a
+// stride of the grid size, double buffered -- the cp.async loads of item w+1
+// fly while item w is transformed and stored.
 template <typename R, int N, int TC>
 __global__ void __launch_bounds__(Tile<R>::NT, Tile<R>::MINB) pass_kernel(PassArgs a) {
   using C = cplx<R>;
   using Cfg = PassCfg<R, N, TC>;
-  constexpr int B = Cfg::B, NT = Cfg::NT, NP = Cfg::NP;
+  constexpr int B = Cfg::B, NT = Cfg::NT, NP = Cfg::NP, TILE = Cfg::TILE;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C *s = reinterpret_cast<C *>(smem_raw);
+  C *const sbase = reinterpret_cast<C *>(smem_raw);
   __shared__ double s_om[B], s_ec[B], s_es[B];
-
-  const int comp0 = a.per_comp ? blockIdx.y : 0;
-  const int nc = a.per_comp ? 1 : a.nc;
-  // tile -> pencil bases
-  int64_t base0;
-  int64_t pstride;  // distance between pencils of the tile
-  int nb;
-  if (a.sa > 1) {
-    const int64_t o = blockIdx.x / a.inner_tiles;
-    const int64_t r0 = (blockIdx.x % a.inner_tiles) * B;
-    base0 = o * (int64_t)N * a.sa + r0;
-    pstride = 1;
-    nb = (int)((a.sa - r0) < B ? (a.sa - r0) : B);
-  } else {
-    const int64_t p0 = (int64_t)blockIdx.x * B;
-    base0 = p0 * N;
-    pstride = N;
-    nb = (int)((a.npencils - p0) < B ? (a.npencils - p0) : B);
-  }
-  C *fld[TC];
-  #pragma unroll
-  for (int c = 0; c < TC; c++) fld[c] = (C *)pick(a.psi, comp0 + c);
-  // load: all of a thread's loads are issued before the first shared-memory
-  // store, so each thread keeps B*N/NT requests in flight
   static_assert((B * N) % NT == 0, "tile must be a multiple of the CTA size");
   constexpr int LPT = B * N / NT;
-  #pragma unroll
-  for (int c = 0; c < TC; c++) {
-    C val[LPT];
-    #pragma unroll
-    for (int k = 0; k < LPT; k++) {
-      const int r = threadIdx.x + k * NT;
-      int b, i;
-      if (a.sa > 1) { b = r % B; i = r / B; } else { i = r % N; b = r / N; }
-      val[k] = mk<R>(0, 0);
-      if (c < nc && b < nb) val[k] = fld[c][base0 + b * pstride + (int64_t)i * a.sa];
-    }
-    #pragma unroll
-    for (int k = 0; k < LPT; k++) {
-      const int r = threadIdx.x + k * NT;
-      int b, i;
-      if (a.sa > 1) { b = r % B; i = r / B; } else { i = r % N; b = r / N; }
-      s[c * B * NP + Pad<N>::idx(b, i)] = val[k];
-    }
-  }
-  __syncthreads();
+  const int64_t W = a.per_comp ? a.ntiles * a.ncomp_grid : a.ntiles;
   const C *tw = (const C *)a.tw;
-  if (a.t1 == T_FWD) fft_tile<R, N, TC * B, NT, -1, TWN>(s, tw);
-  else if (a.t1 == T_INV) fft_tile<R, N, TC * B, NT, +1, TWN>(s, tw);
 
-  if (a.op == OP_KIN) {
-    // psi^ <- ((psi^ s_f) K) s_b with K = Kx Ky Kz in FP64: the two scales of
-    // the reference's ft(-1) / ft(+1) as separate products (no folded,
-    // once-rounded constant that would bias every step the same way)
-    const double2 *kx = a.kt[0][0], *ky = a.kt[0][1], *kz = a.kt[0][2];
+  auto issue = [&](int64_t w, C *s) {
+    const TileGeo g = tile_geo<B, N>(a, w);
+    const int nc = a.per_comp ? 1 : a.nc;
     #pragma unroll
-    for (int c = 1; c < MAXC; c++)
-      if (comp0 == c) { kx = a.kt[c][0]; ky = a.kt[c][1]; kz = a.kt[c][2]; }
-    for (int e = threadIdx.x; e < B * N; e += NT) {
-      const int b = e / N, i = e % N;
-      if (b < nb) {
-        const int64_t l = base0 + b * pstride + (int64_t)i * a.sa;
-        int ix, iy, iz;
-        idx3(a.g, l, ix, iy, iz);
-        const double2 k = kin_phase(kx, ky, kz, ix, iy, iz);
-        const int si = Pad<N>::idx(b, i);
-        double2 v = to_d<R>(s[si]);
-        v.x *= a.s_f;
-        v.y *= a.s_f;
-        v = cmul(v, k);
-        v.x *= a.s_b;
-        v.y *= a.s_b;
-        s[si] = from_d<R>(v);
-      }
-    }
-    __syncthreads();
-  } else if (a.op == OP_FILT) {
-    for (int e = threadIdx.x; e < B * N; e += NT) {
-      const int b = e / N, i = e % N;
-      if (b < nb) {
-        const int64_t l = base0 + b * pstride + (int64_t)i * a.sa;
-        int ijk[3];
-        idx3(a.g, l, ijk[0], ijk[1], ijk[2]);
-        double phi = 0;
-        #pragma unroll
-        for (int ax = 0; ax < 3; ax++) {
-          const int t = (ijk[ax] + a.n[ax] / 2) % a.n[ax];
-          const double k = a.dk[ax] * (double)(t - a.n[ax] / 2);
-          phi += (k * a.filt_alpha) * k;
-        }
-        const double f = (a.filt_mode == FILT_SOBOLEV ? 1.0 / (1.0 + phi) : -phi) * a.filt_scale;
-        const int si = Pad<N>::idx(b, i);
-        C v = s[si];
-        v.x = (R)((double)v.x * f);
-        v.y = (R)((double)v.y * f);
-        s[si] = v;
-      }
-    }
-    __syncthreads();
-  } else if (a.op == OP_NL) {
-    const bool bragg = (a.nl.kind == K_BRAGG);
-    if (bragg && !a.x_along) {
-      for (int b = threadIdx.x; b < B; b += NT) {
-        double om = 0, ec = 1, es = 0;
-        if (b < nb) {
-          int ix, iy, iz;
-          idx3(a.g, base0 + b * pstride, ix, iy, iz);
-          bragg_coupling(a.nl, (double)(ix - a.nl.shift0) * a.nl.dx0, om, ec, es);
-        }
-        s_om[b] = om; s_ec[b] = ec; s_es[b] = es;
-      }
-      __syncthreads();
-    }
-    for (int e = threadIdx.x; e < B * N; e += NT) {
-      const int b = e / N, i = e % N;
-      if (b < nb) {
-        const int64_t l = base0 + b * pstride + (int64_t)i * a.sa;
-        int ix, iy, iz;
-        idx3(a.g, l, ix, iy, iz);
-        const double x0 = (double)(ix - a.nl.shift0) * a.nl.dx0;
-        double om = 0, ec = 1, es = 0;
-        if (bragg) {
-          if (a.x_along) bragg_coupling(a.nl, x0, om, ec, es);
-          else { om = s_om[b]; ec = s_ec[b]; es = s_es[b]; }
-        }
-        C v[MAXC];
-        #pragma unroll
-        for (int c = 0; c < TC; c++) v[c] = s[c * B * NP + Pad<N>::idx(b, i)];
-        nl_point<R>(a.nl, v, l, x0, om, ec, es);
-        #pragma unroll
-        for (int c = 0; c < TC; c++) s[c * B * NP + Pad<N>::idx(b, i)] = v[c];
-      }
-    }
-    __syncthreads();
-  }
-
-  if (a.t2 == T_FWD) fft_tile<R, N, TC * B, NT, -1, TWN>(s, tw);
-  else if (a.t2 == T_INV) fft_tile<R, N, TC * B, NT, +1, TWN>(s, tw);
-
-  #pragma unroll
-  for (int c = 0; c < TC; c++) {
-    if (c < nc) {
+    for (int c = 0; c < TC; c++) {
+      const C *src = (const C *)pick(a.psi, g.comp0 + c);
       #pragma unroll
       for (int k = 0; k < LPT; k++) {
         const int r = threadIdx.x + k * NT;
         int b, i;
         if (a.sa > 1) { b = r % B; i = r / B; } else { i = r % N; b = r / N; }
-        if (b < nb) fld[c][base0 + b * pstride + (int64_t)i * a.sa] = s[c * B * NP + Pad<N>::idx(b, i)];
+        C *dst = &s[c * B * NP + Pad<N>::idx(b, i)];
+        if (c < nc && b < g.nb) cp_async(dst, &src[g.base0 + b * g.pstride + (int64_t)i * a.sa], C{});
+        else *dst = mk<R>(0, 0);
       }
     }
+  };
+
+  int64_t w = blockIdx.x;
+  int buf = 0;
+  if (Cfg::NBUF == 2) {
+    if (w < W) issue(w, sbase);
+    cp_commit();
   }
+  for (; w < W; w += gridDim.x) {
+    C *s = sbase + buf * TILE;
+    if (Cfg::NBUF == 2) {
+      const int64_t wn = w + gridDim.x;
+      if (wn < W) issue(wn, sbase + (buf ^ 1) * TILE);
+      cp_commit();
+      cp_wait_prev();
+    } else {
+      issue(w, s);
+      cp_commit();
+      asm volatile("cp.async.wait_all;\n" ::);
+    }
+    __syncthreads();
+
+    const TileGeo g = tile_geo<B, N>(a, w);
+    const int nc = a.per_comp ? 1 : a.nc;
+    const int64_t base0 = g.base0, pstride = g.pstride;
+    const int nb = g.nb, comp0 = g.comp0;
+    if (a.t1 == T_FWD) fft_tile<R, N, TC * B, NT, -1, TWN>(s, tw);
+    else if (a.t1 == T_INV) fft_tile<R, N, TC * B, NT, +1, TWN>(s, tw);
+
+    if (a.op == OP_KIN) {
+      // psi^ <- ((psi^ s_f) K) s_b with K = Kx Ky Kz in FP64: the two scales of
+      // the reference's ft(-1) / ft(+1) as separate products (no folded,
+      // once-rounded constant that would bias every step the same way)
+      const double2 *kx = a.kt[0][0], *ky = a.kt[0][1], *kz = a.kt[0][2];
+      #pragma unroll
+      for (int c = 1; c < MAXC; c++)
+        if (comp0 == c) { kx = a.kt[c][0]; ky = a.kt[c][1]; kz = a.kt[c][2]; }
+      #pragma unroll 4
+      for (int e = threadIdx.x; e < B * N; e += NT) {
+        const int b = e / N, i = e % N;
+        if (b < nb) {
+          const int64_t l = base0 + b * pstride + (int64_t)i * a.sa;
+          int ix, iy, iz;
+          idx3(a.g, l, ix, iy, iz);
+          const double2 k = kin_phase(kx, ky, kz, ix, iy, iz);
+          const int si = Pad<N>::idx(b, i);
+          double2 v = to_d<R>(s[si]);
+          v.x *= a.s_f;
+          v.y *= a.s_f;
+          v = cmul(v, k);
+          v.x *= a.s_b;
+          v.y *= a.s_b;
+          s[si] = from_d<R>(v);
+        }
+      }
+      __syncthreads();
+    } else if (a.op == OP_FILT) {
+      for (int e = threadIdx.x; e < B * N; e += NT) {
+        const int b = e / N, i = e % N;
+        if (b < nb) {
+          const int64_t l = base0 + b * pstride + (int64_t)i * a.sa;
+          int ijk[3];
+          idx3(a.g, l, ijk[0], ijk[1], ijk[2]);
+          double phi = 0;
+          #pragma unroll
+          for (int ax = 0; ax < 3; ax++) {
+            const int t = (ijk[ax] + a.n[ax] / 2) % a.n[ax];
+            const double k = a.dk[ax] * (double)(t - a.n[ax] / 2);
+            phi += (k * a.filt_alpha) * k;
+          }
+          const double f = (a.filt_mode == FILT_SOBOLEV ? 1.0 / (1.0 + phi) : -phi) * a.filt_scale;
+          const int si = Pad<N>::idx(b, i);
+          C v = s[si];
+          v.x = (R)((double)v.x * f);
+          v.y = (R)((double)v.y * f);
+          s[si] = v;
+        }
+      }
+      __syncthreads();
+    } else if (a.op == OP_NL) {
+      const bool bragg = (a.nl.kind == K_BRAGG);
+      if (bragg && !a.x_along) {
+        for (int b = threadIdx.x; b < B; b += NT) {
+          double om = 0, ec = 1, es = 0;
+          if (b < nb) {
+            int ix, iy, iz;
+            idx3(a.g, base0 + b * pstride, ix, iy, iz);
+            bragg_coupling(a.nl, (double)(ix - a.nl.shift0) * a.nl.dx0, om, ec, es);
+          }
+          s_om[b] = om; s_ec[b] = ec; s_es[b] = es;
+        }
+        __syncthreads();
+      }
+      #pragma unroll 2
+      for (int e = threadIdx.x; e < B * N; e += NT) {
+        const int b = e / N, i = e % N;
+        if (b < nb) {
+          const int64_t l = base0 + b * pstride + (int64_t)i * a.sa;
+          int ix, iy, iz;
+          idx3(a.g, l, ix, iy, iz);
+          const double x0 = (double)(ix - a.nl.shift0) * a.nl.dx0;
+          double om = 0, ec = 1, es = 0;
+          if (bragg) {
+            if (a.x_along) bragg_coupling(a.nl, x0, om, ec, es);
+            else { om = s_om[b]; ec = s_ec[b]; es = s_es[b]; }
+          }
+          C v[MAXC];
+          #pragma unroll
+          for (int c = 0; c < TC; c++) v[c] = s[c * B * NP + Pad<N>::idx(b, i)];
+          nl_point<R>(a.nl, v, l, x0, om, ec, es);
+          #pragma unroll
+          for (int c = 0; c < TC; c++) s[c * B * NP + Pad<N>::idx(b, i)] = v[c];
+        }
+      }
+      __syncthreads();
+    }
+
+    if (a.t2 == T_FWD) fft_tile<R, N, TC * B, NT, -1, TWN>(s, tw);
+    else if (a.t2 == T_INV) fft_tile<R, N, TC * B, NT, +1, TWN>(s, tw);
+
+    #pragma unroll
+    for (int c = 0; c < TC; c++) {
+      if (c < nc) {
+        C *dst = (C *)pick(a.psi, comp0 + c);
+        #pragma unroll
+        for (int k = 0; k < LPT; k++) {
+          const int r = threadIdx.x + k * NT;
+          int b, i;
+          if (a.sa > 1) { b = r % B; i = r / B; } else { i = r % N; b = r / N; }
+          if (b < nb) dst[base0 + b * pstride + (int64_t)i * a.sa] = s[c * B * NP + Pad<N>::idx(b, i)];
+        }
+      }
+    }
+    __syncthreads();  // the buffer is refilled two items later
+    if (Cfg::NBUF == 2) buf ^= 1;
+  }
+  asm volatile("cp.async.wait_all;\n" ::);
 }
 
 // ------------------------------------------------------------ 1D Strang block
@@ -445,7 +506,7 @@ struct Block1DArgs {
 
 template <typename R, int N, int TC>
 __device__ __forceinline__ void kin_1d(cplx<R> *s, const double2 *const (&tab)[TC], int nc, double s_f, double s_b) {
-  constexpr int NT = Tile<R>::NT, NP = Pad<N>::NP;
+  constexpr int NT = BLOCK1D_NT, NP = Pad<N>::NP;
   #pragma unroll
   for (int c = 0; c < TC; c++) {
     if (c < nc) {
@@ -465,9 +526,9 @@ __device__ __forceinline__ void kin_1d(cplx<R> *s, const double2 *const (&tab)[T
 }
 
 template <typename R, int N, int TC>
-__global__ void __launch_bounds__(Tile<R>::NT) block1d_kernel(Block1DArgs a) {
+__global__ void __launch_bounds__(BLOCK1D_NT) block1d_kernel(Block1DArgs a) {
   using C = cplx<R>;
-  constexpr int NT = Tile<R>::NT, NP = Pad<N>::NP;
+  constexpr int NT = BLOCK1D_NT, NP = Pad<N>::NP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *s = reinterpret_cast<C *>(smem_raw);
   const int nc = a.nl.ncomp;

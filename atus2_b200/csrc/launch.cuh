@@ -9,14 +9,19 @@ static inline int launch_pass_t(atus_ctx *ctx, PassArgs &a, int axis) {
   using Cfg = PassCfg<R, N, TC>;
   constexpr size_t smem = Cfg::smem;
   if (smem + 3 * sizeof(double) * Cfg::B > 227 * 1024) return fail(ctx, ATUS_E_UNSUPPORTED, "pencil too long for this component count");
-  static bool attr_set = false;
-  if (!attr_set) {
+  static int resident = 0;  // CTAs of this instantiation per SM
+  static int nsm = 0;
+  if (!resident) {
     CK(cudaFuncSetAttribute(pass_kernel<R, N, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     // all of the unified L1/shared storage as shared memory: the tiles are
     // the working set, global accesses are streaming
     CK(cudaFuncSetAttribute(pass_kernel<R, N, TC>, cudaFuncAttributePreferredSharedMemoryCarveout,
                             cudaSharedmemCarveoutMaxShared));
-    attr_set = true;
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, pass_kernel<R, N, TC>, Cfg::NT, smem));
+    if (resident < 1) return fail(ctx, ATUS_E_UNSUPPORTED, "pass kernel does not fit on an SM");
   }
   int64_t sa = 1;
   for (int b = axis + 1; b < 3; b++) sa *= ctx->n[b];
@@ -38,7 +43,12 @@ static inline int launch_pass_t(atus_ctx *ctx, PassArgs &a, int axis) {
     a.dk[ax] = ctx->dk[ax];
     a.n[ax] = (int)ctx->n[ax];
   }
-  dim3 grid((unsigned)ntiles, a.per_comp ? ctx->ncomp : 1);
+  a.ntiles = ntiles;
+  a.ncomp_grid = ctx->ncomp;
+  // persistent grid: every resident CTA walks work items with stride gridDim
+  const int64_t work = a.per_comp ? ntiles * ctx->ncomp : ntiles;
+  const int64_t slots = (int64_t)nsm * resident;
+  const unsigned grid = (unsigned)(work < slots ? work : slots);
   pass_kernel<R, N, TC><<<grid, Cfg::NT, smem, ctx->stream>>>(a);
   LAUNCHED(ctx);
   return ATUS_OK;
@@ -73,7 +83,7 @@ static inline int launch_block1d_t(atus_ctx *ctx, Block1DArgs &a) {
     CK(cudaFuncSetAttribute(block1d_kernel<R, N, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     attr_set = true;
   }
-  block1d_kernel<R, N, TC><<<1, Tile<R>::NT, smem, ctx->stream>>>(a);
+  block1d_kernel<R, N, TC><<<1, BLOCK1D_NT, smem, ctx->stream>>>(a);
   LAUNCHED(ctx);
   return ATUS_OK;
 }
