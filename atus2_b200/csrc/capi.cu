@@ -338,10 +338,18 @@ int atus_create(const atus_grid *grid, int ncomp, int precision, atus_ctx **out)
     }
     ctx->tw = ctx->tw64;
     if (ok && precision == ATUS_PREC_MIXED) {
-      ok = cudaMalloc(&ctx->tw, 8 * TWN) == cudaSuccess;
+      // float4 (hi, lo) split of the FP64 table for the compensated FP32 multiply
+      ok = cudaMalloc(&ctx->tw, sizeof(float4) * TWN) == cudaSuccess;
       if (ok) {
-        auto t = twiddles<float>();
-        ok = cudaMemcpy(ctx->tw, t.data(), 8 * TWN, cudaMemcpyHostToDevice) == cudaSuccess;
+        const auto t = twiddles<double>();
+        std::vector<float4> t4(TWN);
+        for (int m = 0; m < TWN; m++) {
+          t4[m].x = (float)t[m].x;
+          t4[m].y = (float)t[m].y;
+          t4[m].z = (float)(t[m].x - (double)t4[m].x);
+          t4[m].w = (float)(t[m].y - (double)t4[m].y);
+        }
+        ok = cudaMemcpy(ctx->tw, t4.data(), sizeof(float4) * TWN, cudaMemcpyHostToDevice) == cudaSuccess;
       }
     }
   }

@@ -72,21 +72,29 @@ template <int DIR, typename C> __device__ __forceinline__ void dft4(C &a0, C &a1
 }
 template <int DIR, typename C> __device__ __forceinline__ void dft4(C *v) { dft4<DIR>(v[0], v[1], v[2], v[3]); }
 
+// x * k for a compile-time constant k given in FP64.  In FP32 the constant
+// is split k = hi + lo and the product formed as fma(x, hi, x lo): the
+// rounding error of a float constant would otherwise be the same in every
+// transform and bias the norm the same way each step.
+__device__ __forceinline__ double kmul(double x, double k) { return x * k; }
+__device__ __forceinline__ float kmul(float x, double k) {
+  const float hi = (float)k;
+  const float lo = (float)(k - (double)hi);
+  return fmaf(x, hi, x * lo);
+}
+
 // exp(DIR * 2 pi i * m / 8) * a for m = 1, 3 (m = 2 is mul_i).
+constexpr double SQRT1_2 = 0.70710678118654752440;
 template <int DIR, typename C> __device__ __forceinline__ C w8_1(C a) {
-  using R = decltype(a.x);
-  const R h = (R)0.70710678118654752440;
   C r;  // (1 + DIR i) / sqrt 2
-  if (DIR < 0) { r.x = h * (a.x + a.y); r.y = h * (a.y - a.x); }
-  else { r.x = h * (a.x - a.y); r.y = h * (a.x + a.y); }
+  if (DIR < 0) { r.x = kmul(a.x + a.y, SQRT1_2); r.y = kmul(a.y - a.x, SQRT1_2); }
+  else { r.x = kmul(a.x - a.y, SQRT1_2); r.y = kmul(a.x + a.y, SQRT1_2); }
   return r;
 }
 template <int DIR, typename C> __device__ __forceinline__ C w8_3(C a) {
-  using R = decltype(a.x);
-  const R h = (R)0.70710678118654752440;
   C r;  // (-1 + DIR i) / sqrt 2
-  if (DIR < 0) { r.x = h * (a.y - a.x); r.y = -h * (a.x + a.y); }
-  else { r.x = -h * (a.x + a.y); r.y = h * (a.x - a.y); }
+  if (DIR < 0) { r.x = kmul(a.y - a.x, SQRT1_2); r.y = -kmul(a.x + a.y, SQRT1_2); }
+  else { r.x = -kmul(a.x + a.y, SQRT1_2); r.y = kmul(a.x - a.y, SQRT1_2); }
   return r;
 }
 
@@ -108,18 +116,18 @@ template <int DIR, typename C> __device__ __forceinline__ void dft8(C *v) {
 // 16-point DFT as 4 x 4: X[m + 4p] = sum_q W4^{qp} W16^{qm} sum_s v[q+4s] W4^{sm}
 template <int DIR, typename C> __device__ __forceinline__ void dft16(C *v) {
   using R = decltype(v[0].x);
-  const R c1 = (R)0.92387953251128675613;  // cos(pi/8)
-  const R s1 = (R)0.38268343236508977173;  // sin(pi/8)
-  const R d = (R)DIR;
+  constexpr double c1 = 0.92387953251128675613;  // cos(pi/8)
+  constexpr double s1 = 0.38268343236508977173;  // sin(pi/8)
+  constexpr double ds1 = DIR * s1, dc1 = DIR * c1;
   #pragma unroll
   for (int q = 0; q < 4; q++) dft4<DIR>(v[q], v[q + 4], v[q + 8], v[q + 12]);
   // twiddles W16^{q m}: element (q, m) lives in v[q + 4m]
   {  // q = 1: m = 1, 2, 3 -> W16^1, W16^2, W16^3
     C a = v[5];
-    v[5] = mk<R>(c1 * a.x - d * s1 * a.y, c1 * a.y + d * s1 * a.x);
+    v[5] = mk<R>(kmul(a.x, c1) - kmul(a.y, ds1), kmul(a.y, c1) + kmul(a.x, ds1));
     v[9] = w8_1<DIR>(v[9]);
     a = v[13];
-    v[13] = mk<R>(s1 * a.x - d * c1 * a.y, s1 * a.y + d * c1 * a.x);
+    v[13] = mk<R>(kmul(a.x, s1) - kmul(a.y, dc1), kmul(a.y, s1) + kmul(a.x, dc1));
   }
   {  // q = 2: W16^2, W16^4, W16^6
     v[6] = w8_1<DIR>(v[6]);
@@ -128,10 +136,10 @@ template <int DIR, typename C> __device__ __forceinline__ void dft16(C *v) {
   }
   {  // q = 3: W16^3, W16^6, W16^9
     C a = v[7];
-    v[7] = mk<R>(s1 * a.x - d * c1 * a.y, s1 * a.y + d * c1 * a.x);
+    v[7] = mk<R>(kmul(a.x, s1) - kmul(a.y, dc1), kmul(a.y, s1) + kmul(a.x, dc1));
     v[11] = w8_3<DIR>(v[11]);
-    a = v[15];  // W16^9 = -c1 + DIR*(-s1)... exp(DIR i 9pi/8) = -cos(pi/8) - DIR i sin(pi/8)
-    v[15] = mk<R>(-c1 * a.x + d * s1 * a.y, -c1 * a.y - d * s1 * a.x);
+    a = v[15];  // W16^9 = exp(DIR i 9 pi/8) = -cos(pi/8) - DIR i sin(pi/8)
+    v[15] = mk<R>(kmul(a.y, ds1) - kmul(a.x, c1), -kmul(a.y, c1) - kmul(a.x, ds1));
   }
   C o[16];
   #pragma unroll
@@ -161,10 +169,28 @@ __host__ __device__ constexpr int pass_ns(int N, int p) {  // product of radices
   return p == 0 ? 1 : pass_ns(N, p - 1) * pass_radix(N, p - 1);
 }
 
+// Twiddle tables: exp(-2 pi i m / TWN) as double2 for FP64 transforms, and as
+// float4 (hi.x, hi.y, lo.x, lo.y) with hi + lo = the FP64 value for FP32
+// transforms, multiplied in compensated form (see kmul).
+template <typename R> struct TwTab;
+template <> struct TwTab<double> { using type = double2; };
+template <> struct TwTab<float> { using type = float4; };
+
+template <int DIR> __device__ __forceinline__ double2 twmul(double2 v, double2 w) {
+  return (DIR < 0) ? cmul(v, w) : cmulc(v, w);
+}
+template <int DIR> __device__ __forceinline__ float2 twmul(float2 v, float4 w) {
+  const float wy = DIR < 0 ? w.y : -w.y, ly = DIR < 0 ? w.w : -w.w;
+  float2 r;
+  r.x = fmaf(v.x, w.x, fmaf(-v.y, wy, v.x * w.z - v.y * ly));
+  r.y = fmaf(v.x, wy, fmaf(v.y, w.x, v.x * ly + v.y * w.z));
+  return r;
+}
+
 // One Stockham pass over B pencils held in shared memory.  tw is the global
 // twiddle table exp(-2 pi i m / TWN), m in [0, TWN).
 template <typename R, int N, int B, int NT, int RAD, int NS, int DIR, int TWN>
-__device__ __forceinline__ void stockham_pass(cplx<R> *s, const cplx<R> *__restrict__ tw) {
+__device__ __forceinline__ void stockham_pass(cplx<R> *s, const typename TwTab<R>::type *__restrict__ tw) {
   using C = cplx<R>;
   using P = Pad<N>;
   constexpr int NB = B * N / RAD;                 // butterflies in the tile
@@ -182,8 +208,7 @@ __device__ __forceinline__ void stockham_pass(cplx<R> *s, const cplx<R> *__restr
       if (NS > 1) {
         #pragma unroll
         for (int r = 1; r < RAD; r++) {
-          const C w = __ldg(&tw[(r * k) * TWS]);
-          v[u][r] = (DIR < 0) ? cmul(v[u][r], w) : cmulc(v[u][r], w);
+          v[u][r] = twmul<DIR>(v[u][r], __ldg(&tw[(r * k) * TWS]));
         }
       }
       dftR<RAD, DIR>(v[u]);
@@ -205,7 +230,7 @@ __device__ __forceinline__ void stockham_pass(cplx<R> *s, const cplx<R> *__restr
 }
 
 template <typename R, int N, int B, int NT, int DIR, int TWN, int P>
-__device__ __forceinline__ void fft_passes(cplx<R> *s, const cplx<R> *__restrict__ tw) {
+__device__ __forceinline__ void fft_passes(cplx<R> *s, const typename TwTab<R>::type *__restrict__ tw) {
   if constexpr (P < n_passes(N)) {
     stockham_pass<R, N, B, NT, pass_radix(N, P), pass_ns(N, P), DIR, TWN>(s, tw);
     fft_passes<R, N, B, NT, DIR, TWN, P + 1>(s, tw);
@@ -215,7 +240,7 @@ __device__ __forceinline__ void fft_passes(cplx<R> *s, const cplx<R> *__restrict
 // In-place transform of the B pencils in shared memory (natural order in and
 // out).  Caller synchronises before (data written) -- the first pass reads.
 template <typename R, int N, int B, int NT, int DIR, int TWN>
-__device__ __forceinline__ void fft_tile(cplx<R> *s, const cplx<R> *__restrict__ tw) {
+__device__ __forceinline__ void fft_tile(cplx<R> *s, const typename TwTab<R>::type *__restrict__ tw) {
   if constexpr (N > 1) fft_passes<R, N, B, NT, DIR, TWN, 0>(s, tw);
 }
 

@@ -335,7 +335,7 @@ __global__ void __launch_bounds__(Tile<R>::NT, Tile<R>::MINB) pass_kernel(PassAr
   static_assert((B * N) % NT == 0, "tile must be a multiple of the CTA size");
   constexpr int LPT = B * N / NT;
   const int64_t W = a.per_comp ? a.ntiles * a.ncomp_grid : a.ntiles;
-  const C *tw = (const C *)a.tw;
+  const typename TwTab<R>::type *tw = (const typename TwTab<R>::type *)a.tw;
 
   auto issue = [&](int64_t w, C *s) {
     const TileGeo g = tile_geo<B, N>(a, w);
@@ -532,7 +532,7 @@ __global__ void __launch_bounds__(BLOCK1D_NT) block1d_kernel(Block1DArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *s = reinterpret_cast<C *>(smem_raw);
   const int nc = a.nl.ncomp;
-  const C *tw = (const C *)a.tw;
+  const typename TwTab<R>::type *tw = (const typename TwTab<R>::type *)a.tw;
   C *fld[TC];
   const double2 *kh[TC], *kf[TC];
   #pragma unroll

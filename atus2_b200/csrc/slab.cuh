@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(512) slab_kernel(SlabArgs a) {
   const int r = (int)cluster.block_rank();
   const int64_t x = blockIdx.x / CS;
   const int64_t base = x * (int64_t)NY * NZ;
-  const C *tw = (const C *)a.tw;
+  const typename TwTab<R>::type *tw = (const typename TwTab<R>::type *)a.tw;
   C *fld[TC];
   #pragma unroll
   for (int c = 0; c < TC; c++) fld[c] = (C *)a.psi[c];
