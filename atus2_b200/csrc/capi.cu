@@ -122,6 +122,33 @@ static NLArgs nl_args(const atus_ctx *ctx, int kind, double t1, double F) {
 
 static int tc_for(int ncomp) { return ncomp <= 1 ? 1 : (ncomp <= 2 ? 2 : 4); }
 
+// The register-staged kernel where it has an instantiation (pencils of 32..256
+// points, the pass shapes of the split-step schedule), else the tile kernel.
+static int dispatch_pass(atus_ctx *ctx, PassArgs &a, int axis, int tc) {
+  const bool dbl = (ctx->prec == ATUS_PREC_FP64);
+  if (ctx->use_pass2) {
+    const bool strided = axis < ctx->dim - 1;
+    int r = ATUS_E_UNSUPPORTED;
+    if (a.op == OP_NONE && a.t2 == T_NONE && (a.t1 == T_FWD || a.t1 == T_INV)) {
+      const int mode = (a.t1 == T_FWD) ? M2_FWD : M2_INV;
+      r = dbl ? launch_pass2_d_t(ctx, a, axis, mode, strided) : launch_pass2_f_t(ctx, a, axis, mode, strided);
+    } else if ((a.op == OP_KIN || a.op == OP_FILT) && a.t1 == T_FWD && a.t2 == T_INV && strided) {
+      r = dbl ? launch_pass2_d_k(ctx, a, axis) : launch_pass2_f_k(ctx, a, axis);
+    } else if (a.op == OP_NL && a.t1 == T_INV && a.t2 == T_FWD && !strided && tc <= 2) {
+      r = dbl ? launch_pass2_d_nl(ctx, a, axis, tc) : launch_pass2_f_nl(ctx, a, axis, tc);
+    }
+    if (r != ATUS_E_UNSUPPORTED) return r;
+  }
+  if (dbl) {
+    if (tc == 1) return launch_pass_d1(ctx, a, axis);
+    if (tc == 2) return launch_pass_d2(ctx, a, axis);
+    return launch_pass_d4(ctx, a, axis);
+  }
+  if (tc == 1) return launch_pass_f1(ctx, a, axis);
+  if (tc == 2) return launch_pass_f2(ctx, a, axis);
+  return launch_pass_f4(ctx, a, axis);
+}
+
 // One pass along `axis` over `fields` (nullptr: the context's fields).
 static int run_pass(atus_ctx *ctx, int axis, int t1, int op, int t2, const NLArgs *nl, int half,
                     void *const *fields = nullptr, int nfields = -1) {
@@ -144,19 +171,12 @@ static int run_pass(atus_ctx *ctx, int axis, int t1, int op, int t2, const NLArg
   if (a.per_comp && nf != ctx->ncomp) {
     int saved = ctx->ncomp;
     ctx->ncomp = nf;
-    int r = (ctx->prec == ATUS_PREC_FP64) ? launch_pass_d1(ctx, a, axis) : launch_pass_f1(ctx, a, axis);
+    int r = dispatch_pass(ctx, a, axis, 1);
     ctx->ncomp = saved;
     return r;
   }
   const int tc = a.per_comp ? 1 : tc_for(nf);
-  if (ctx->prec == ATUS_PREC_FP64) {
-    if (tc == 1) return launch_pass_d1(ctx, a, axis);
-    if (tc == 2) return launch_pass_d2(ctx, a, axis);
-    return launch_pass_d4(ctx, a, axis);
-  }
-  if (tc == 1) return launch_pass_f1(ctx, a, axis);
-  if (tc == 2) return launch_pass_f2(ctx, a, axis);
-  return launch_pass_f4(ctx, a, axis);
+  return dispatch_pass(ctx, a, axis, tc);
 }
 
 #define RUN(x)                  \
@@ -316,6 +336,9 @@ int atus_create(const atus_grid *grid, int ncomp, int precision, atus_ctx **out)
     // three axis passes (measured slower on B200 so far; kept for A/B runs)
     const char *e = getenv("ATUS_SLAB");
     ctx->use_slab = (e && e[0] == '1');
+    // ATUS_PASS2=0: tile kernel only (A/B comparisons of the two pass kernels)
+    const char *p2 = getenv("ATUS_PASS2");
+    ctx->use_pass2 = !(p2 && p2[0] == '0');
   }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) { delete ctx; return ATUS_E_CUDA; }

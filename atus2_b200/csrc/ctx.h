@@ -30,6 +30,7 @@ struct atus_ctx {
   cudaStream_t own_stream = nullptr, stream = nullptr;
   int64_t launches = 0;
   bool use_slab = true;         // 3D: fused (y,z) cluster pass when available
+  bool use_pass2 = true;        // register-staged passes for pencils of 32..256 points
   std::string err;
   // Sobolev state
   bool sob_ready = false;

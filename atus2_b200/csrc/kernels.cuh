@@ -37,6 +37,8 @@ enum { T_NONE = 0, T_FWD = -1, T_INV = 1 };
 enum { OP_NONE = 0, OP_KIN = 1, OP_NL = 2, OP_FILT = 3 };
 enum { FILT_SOBOLEV = 0, FILT_LAPLACE = 1 };
 enum { K_NL = 0, K_NL_IF = 1, K_BRAGG = 2 };
+// modes of the register-staged pass kernel (pass2.cuh)
+enum { M2_FWD = 0, M2_INV = 1, M2_KIN = 2, M2_NL = 3 };
 
 struct LaserD {
   double beta0, DeltaL[MAXC], Amp0, laser_k0, laser_dk0, laser_domh0, phase0, chirp_rate0, chirp;
@@ -78,6 +80,7 @@ struct PassArgs {
   Geo g;
   NLArgs nl;
   int x_along;              // 1 when the pencil runs along axis 0 (x varies inside a pencil)
+  int axis;                 // axis the pencils run along
   // OP_FILT: real k-space filter of CSOB_Base (include/CSOB_Base.h:228-248):
   // 1/(1 + alpha k^2) or -alpha k^2, times the transform scale.
   int filt_mode;

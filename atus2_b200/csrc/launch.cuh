@@ -3,6 +3,7 @@
 // combination, so the kernels compile in parallel.
 #pragma once
 #include "ctx.h"
+#include "pass2.cuh"
 
 template <typename R, int N, int TC>
 static inline int launch_pass_t(atus_ctx *ctx, PassArgs &a, int axis) {
@@ -37,6 +38,7 @@ static inline int launch_pass_t(atus_ctx *ctx, PassArgs &a, int axis) {
     ntiles = (a.npencils + Cfg::B - 1) / Cfg::B;
   }
   a.x_along = (axis == 0);
+  a.axis = axis;
   a.g = geo(ctx);
   a.tw = (sizeof(R) == 8) ? ctx->tw64 : ctx->tw;
   for (int ax = 0; ax < 3; ax++) {
@@ -108,3 +110,66 @@ static inline int launch_block1d_n(atus_ctx *ctx, Block1DArgs &a) {
   }
 }
 
+
+// ------------------------------------------------------------ register-staged passes
+// Launch of pass2_kernel (pencils of 32..256 points); ATUS_E_UNSUPPORTED,
+// without an error message, for lengths it has no instantiation for.
+template <typename R, int N, int TC, int MODE, bool STRIDED>
+static inline int launch_pass2_t(atus_ctx *ctx, PassArgs &a, int axis) {
+  using Cfg = P2Cfg<R, N, TC>;
+  constexpr size_t smem = Cfg::smem;
+  static int resident = 0;
+  static int nsm = 0;
+  if (!resident) {
+    CK(cudaFuncSetAttribute(pass2_kernel<R, N, TC, MODE, STRIDED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)smem));
+    CK(cudaFuncSetAttribute(pass2_kernel<R, N, TC, MODE, STRIDED>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                            cudaSharedmemCarveoutMaxShared));
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, pass2_kernel<R, N, TC, MODE, STRIDED>, Cfg::NT, smem));
+    if (resident < 1) return fail(ctx, ATUS_E_UNSUPPORTED, "pass kernel does not fit on an SM");
+  }
+  int64_t sa = 1;
+  for (int b = axis + 1; b < 3; b++) sa *= ctx->n[b];
+  if ((sa > 1) != STRIDED) return ATUS_E_UNSUPPORTED;
+  a.sa = sa;
+  int64_t ntiles;
+  if (sa > 1) {
+    a.inner_tiles = (sa + Cfg::B - 1) / Cfg::B;
+    ntiles = (ctx->npts / (N * sa)) * a.inner_tiles;
+    a.npencils = 0;
+  } else {
+    a.inner_tiles = 1;
+    a.npencils = ctx->npts / N;
+    ntiles = (a.npencils + Cfg::B - 1) / Cfg::B;
+  }
+  a.x_along = (axis == 0);
+  a.axis = axis;
+  a.g = geo(ctx);
+  a.tw = (sizeof(R) == 8) ? ctx->tw64 : ctx->tw;
+  for (int ax = 0; ax < 3; ax++) {
+    a.dk[ax] = ctx->dk[ax];
+    a.n[ax] = (int)ctx->n[ax];
+  }
+  a.ntiles = ntiles;
+  a.ncomp_grid = ctx->ncomp;
+  const int64_t work = a.per_comp ? ntiles * ctx->ncomp : ntiles;
+  const int64_t slots = (int64_t)nsm * resident;
+  const unsigned grid = (unsigned)(work < slots ? work : slots);
+  pass2_kernel<R, N, TC, MODE, STRIDED><<<grid, Cfg::NT, smem, ctx->stream>>>(a);
+  LAUNCHED(ctx);
+  return ATUS_OK;
+}
+
+template <typename R, int TC, int MODE, bool STRIDED>
+static inline int launch_pass2_n(atus_ctx *ctx, PassArgs &a, int axis) {
+  switch (ctx->n[axis]) {
+    case 32: return launch_pass2_t<R, 32, TC, MODE, STRIDED>(ctx, a, axis);
+    case 64: return launch_pass2_t<R, 64, TC, MODE, STRIDED>(ctx, a, axis);
+    case 128: return launch_pass2_t<R, 128, TC, MODE, STRIDED>(ctx, a, axis);
+    case 256: return launch_pass2_t<R, 256, TC, MODE, STRIDED>(ctx, a, axis);
+    default: return ATUS_E_UNSUPPORTED;
+  }
+}

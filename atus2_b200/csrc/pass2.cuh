@@ -1,0 +1,257 @@
+// pass2.cuh -- register-staged pass kernel for pencils of 32..256 points.
+//
+// A pencil of N = 16 R2 points is transformed in the two Stockham stages of
+// fft_tile (radix 16 over inputs j + R2 r, then radix R2 with twiddles
+// exp(-+2 pi i r k / N)), with the same arithmetic in the same order.  What
+// differs is where the data lives between the stages:
+//
+//   HBM -> registers (stage-1 inputs)  -> stage 1 -> shared exchange ->
+//   stage 2 -> registers (outputs j + R2 m, m < 16) -> HBM
+//
+// The thread that reads inputs j + R2 r (r < 16) of stage 1 ends up with the
+// outputs j + R2 m of stage 2, which are again the inputs of a stage 1.  So
+// FFT -> point-wise operator -> IFFT runs in registers with one shared-memory
+// exchange per transform, where the tile kernel (pass_kernel) makes six sweeps
+// through shared memory per transform plus the tile load and store.  Twiddles
+// come from a padded per-pencil-length table in shared memory.
+//
+// Thread layout: along a strided axis consecutive threads take consecutive
+// pencils (the inner grid index), so one warp-wide load covers whole 128-byte
+// rows; along the contiguous axis consecutive threads take consecutive points.
+#pragma once
+#include "kernels.cuh"
+
+namespace atus {
+
+// Tile budget (complex values) and threads; one thread owns 16 values.
+template <typename R> struct Tile2;
+template <> struct Tile2<double> { static constexpr int E = 2048, NT = 128, MINB = 4; };
+template <> struct Tile2<float> { static constexpr int E = 4096, NT = 256, MINB = 3; };
+
+template <typename R, int N, int TC>
+struct P2Cfg {
+  static constexpr int R2 = N / 16;        // stage-2 radix
+  static constexpr int T2 = 16 / R2;       // stage-2 butterflies per thread
+  static constexpr int E = Tile2<R>::E;
+  static constexpr int NT = Tile2<R>::NT;
+  static constexpr int B = E / (N * TC);   // pencils per tile
+  static constexpr int NPC = B * TC;       // pencil-components per tile
+  static constexpr int PB = 17 * R2 + 1;   // exchange pitch: R2 rows of 16 + 1 pad, odd
+  static constexpr int TWP = N + N / 8;    // twiddle table with one pad per 8 entries
+  static constexpr size_t smem_ex = sizeof(cplx<R>) * NPC * PB;
+  static constexpr size_t smem = smem_ex + sizeof(typename TwTab<R>::type) * TWP;
+};
+
+// Exchange layout of one pencil-component: row-major R2 x 16 with row pitch
+// 17.  Stage-1 butterfly j writes row j (its 16 outputs, Stockham index
+// 16 j + q); stage-2 butterfly k reads column k.  Point i of the natural order
+// sits at row i / 16, column i % 16.
+__device__ __forceinline__ int ex_at(int row, int col) { return 17 * row + col; }
+
+// Stage 2 of a transform: butterflies k = j + R2 t (t < T2) of the pencil whose
+// exchange rows start at ex; o[t + T2 r] = output k + 16 r = point j + R2 (t + T2 r).
+template <typename R, int N, int DIR>
+__device__ __forceinline__ void p2_stage2(const cplx<R> *ex, const typename TwTab<R>::type *twS, int j, cplx<R> *o) {
+  using C = cplx<R>;
+  constexpr int R2 = N / 16, T2 = 16 / R2;
+  #pragma unroll
+  for (int t = 0; t < T2; t++) {
+    const int k = j + R2 * t;
+    C u[R2];
+    #pragma unroll
+    for (int r = 0; r < R2; r++) u[r] = ex[ex_at(r, k)];
+    #pragma unroll
+    for (int r = 1; r < R2; r++) {
+      const int m = r * k;
+      u[r] = twmul<DIR>(u[r], twS[m + (m >> 3)]);
+    }
+    dftR<R2, DIR>(u);
+    #pragma unroll
+    for (int r = 0; r < R2; r++) o[t + T2 * r] = u[r];
+  }
+}
+
+// One transform of the thread's 16 values v (stage-1 inputs j + R2 r on entry,
+// points j + R2 m on return).  The leading barrier protects the exchange rows
+// that other threads may still be reading from the previous use.
+template <typename R, int N, int DIR>
+__device__ __forceinline__ void p2_transform(cplx<R> *v, cplx<R> *ex, const typename TwTab<R>::type *twS, int j) {
+  dft16<DIR>(v);
+  __syncthreads();
+  #pragma unroll
+  for (int q = 0; q < 16; q++) ex[ex_at(j, q)] = v[q];
+  __syncthreads();
+  p2_stage2<R, N, DIR>(ex, twS, j, v);
+}
+
+template <typename R, int N, int TC, int MODE, bool STRIDED>
+__global__ void __launch_bounds__(Tile2<R>::NT, Tile2<R>::MINB) pass2_kernel(PassArgs a) {
+  using C = cplx<R>;
+  using TW = typename TwTab<R>::type;
+  using Cfg = P2Cfg<R, N, TC>;
+  constexpr int R2 = Cfg::R2, B = Cfg::B, NT = Cfg::NT, PB = Cfg::PB;
+  static_assert(N >= 32 && N <= 256, "two-stage pencils only");
+  static_assert(Cfg::NPC * R2 == NT, "one thread per stage-1 butterfly");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *const ex = reinterpret_cast<C *>(smem_raw);
+  TW *const twS = reinterpret_cast<TW *>(smem_raw + Cfg::smem_ex);
+  __shared__ double s_om[B], s_ec[B], s_es[B];
+
+  const int tid = threadIdx.x;
+  int b, j, c;
+  if (STRIDED) { b = tid % B; j = (tid / B) % R2; c = tid / (B * R2); }
+  else { j = tid % R2; b = (tid / R2) % B; c = tid / (R2 * B); }
+  C *const my = ex + (c * B + b) * PB;
+
+  {  // exp(-2 pi i m / N), m < N, from the TWN-point table
+    const TW *tw = (const TW *)a.tw;
+    for (int m = tid; m < N; m += NT) twS[m + (m >> 3)] = tw[m * (TWN / N)];
+  }
+  const int64_t W = a.per_comp ? a.ntiles * a.ncomp_grid : a.ntiles;
+  const int nc = a.per_comp ? 1 : a.nc;
+  for (int64_t w = blockIdx.x; w < W; w += gridDim.x) {
+    const TileGeo g = tile_geo<B, N>(a, w);
+    const bool live = (b < g.nb) && (c < nc);
+    C *const f = (C *)pick(a.psi, g.comp0 + c);
+    const int64_t lb = g.base0 + b * g.pstride;  // grid index of the pencil's point 0
+    const int64_t step = (int64_t)R2 * a.sa;     // distance of points j + R2 m and j + R2 (m+1)
+    const C *src = live ? f + lb + (int64_t)j * a.sa : nullptr;
+
+    if constexpr (MODE == M2_NL && TC > 1) {
+      // coupling of each pencil (x is constant along it); read after the
+      // barriers of the first transform
+      if (a.nl.kind == K_BRAGG && a.axis != 0)
+      for (int p = tid; p < B; p += NT) {
+        double om = 0, ec = 1, es = 0;
+        if (p < g.nb) {
+          int ix, iy, iz;
+          idx3(a.g, g.base0 + p * g.pstride, ix, iy, iz);
+          bragg_coupling(a.nl, (double)(ix - a.nl.shift0) * a.nl.dx0, om, ec, es);
+        }
+        s_om[p] = om; s_ec[p] = ec; s_es[p] = es;
+      }
+    }
+
+    C v[16];
+    #pragma unroll
+    for (int r = 0; r < 16; r++) v[r] = live ? src[r * step] : mk<R>(0, 0);
+
+    if constexpr (MODE == M2_FWD) {
+      p2_transform<R, N, -1>(v, my, twS, j);
+    } else if constexpr (MODE == M2_INV) {
+      p2_transform<R, N, +1>(v, my, twS, j);
+    } else if constexpr (MODE == M2_KIN) {
+      p2_transform<R, N, -1>(v, my, twS, j);
+      int p0[3];
+      idx3(a.g, lb, p0[0], p0[1], p0[2]);
+      if (a.op == OP_KIN) {
+        // ((psi^ s_f) K) s_b with K = (Kx Ky) Kz in FP64, as in pass_kernel
+        const double2 *kx = a.kt[0][0], *ky = a.kt[0][1], *kz = a.kt[0][2];
+        #pragma unroll
+        for (int cc = 1; cc < MAXC; cc++)
+          if (g.comp0 == cc) { kx = a.kt[cc][0]; ky = a.kt[cc][1]; kz = a.kt[cc][2]; }
+        const double2 KX = __ldg(&kx[p0[0]]), KY = __ldg(&ky[p0[1]]), KZ = __ldg(&kz[p0[2]]);
+        #pragma unroll
+        for (int m = 0; m < 16; m++) {
+          const int i = j + R2 * m;
+          const double2 fx = (a.axis == 0) ? __ldg(&kx[i]) : KX;
+          const double2 fy = (a.axis == 1) ? __ldg(&ky[i]) : KY;
+          const double2 fz = (a.axis == 2) ? __ldg(&kz[i]) : KZ;
+          const double2 K = cmul(cmul(fx, fy), fz);
+          double2 u = to_d<R>(v[m]);
+          u.x *= a.s_f;
+          u.y *= a.s_f;
+          u = cmul(u, K);
+          u.x *= a.s_b;
+          u.y *= a.s_b;
+          v[m] = from_d<R>(u);
+        }
+      } else if (a.op == OP_FILT) {
+        #pragma unroll
+        for (int m = 0; m < 16; m++) {
+          const int i = j + R2 * m;
+          double phi = 0;
+          #pragma unroll
+          for (int ax = 0; ax < 3; ax++) {
+            const int ii = (ax == a.axis) ? i : p0[ax];
+            const int t = (ii + a.n[ax] / 2) % a.n[ax];
+            const double k = a.dk[ax] * (double)(t - a.n[ax] / 2);
+            phi += (k * a.filt_alpha) * k;
+          }
+          const double fk = (a.filt_mode == FILT_SOBOLEV ? 1.0 / (1.0 + phi) : -phi) * a.filt_scale;
+          v[m].x = (R)((double)v[m].x * fk);
+          v[m].y = (R)((double)v[m].y * fk);
+        }
+      }
+      p2_transform<R, N, +1>(v, my, twS, j);
+    } else {  // M2_NL: IFFT -> potential step -> FFT
+      p2_transform<R, N, +1>(v, my, twS, j);
+      if constexpr (TC == 1) {
+        int p0[3];
+        idx3(a.g, lb, p0[0], p0[1], p0[2]);
+        #pragma unroll
+        for (int m = 0; m < 16; m++) {
+          const int i = j + R2 * m;
+          const int64_t l = lb + (int64_t)i * a.sa;
+          const int ix = (a.axis == 0) ? i : p0[0];
+          const double x0 = (double)(ix - a.nl.shift0) * a.nl.dx0;
+          double om = 0, ec = 1, es = 0;
+          if (a.nl.kind == K_BRAGG) bragg_coupling(a.nl, x0, om, ec, es);
+          C u[MAXC];
+          u[0] = v[m];
+          if (live) nl_point<R>(a.nl, u, l, x0, om, ec, es);
+          v[m] = u[0];
+        }
+      } else {
+        // all components of a point meet in shared memory (natural order)
+        __syncthreads();
+        #pragma unroll
+        for (int m = 0; m < 16; m++) {
+          const int i = j + R2 * m;
+          my[ex_at(i >> 4, i & 15)] = v[m];
+        }
+        __syncthreads();
+        constexpr int PPT = 16 / TC;  // points per thread
+        const bool bragg = (a.nl.kind == K_BRAGG);
+        #pragma unroll 2
+        for (int u_ = 0; u_ < PPT; u_++) {
+          const int p = tid + NT * u_;
+          int pb, i;
+          if (STRIDED) { pb = p % B; i = p / B; } else { i = p % N; pb = p / N; }
+          if (pb < g.nb) {
+            const int64_t l = g.base0 + pb * g.pstride + (int64_t)i * a.sa;
+            int ix, iy, iz;
+            idx3(a.g, l, ix, iy, iz);
+            const double x0 = (double)(ix - a.nl.shift0) * a.nl.dx0;
+            double om = 0, ec = 1, es = 0;
+            if (bragg) {
+              if (a.axis == 0) bragg_coupling(a.nl, x0, om, ec, es);
+              else { om = s_om[pb]; ec = s_ec[pb]; es = s_es[pb]; }
+            }
+            C u[MAXC];
+            #pragma unroll
+            for (int cc = 0; cc < TC; cc++) u[cc] = ex[(cc * B + pb) * PB + ex_at(i >> 4, i & 15)];
+            nl_point<R>(a.nl, u, l, x0, om, ec, es);
+            #pragma unroll
+            for (int cc = 0; cc < TC; cc++) ex[(cc * B + pb) * PB + ex_at(i >> 4, i & 15)] = u[cc];
+          }
+        }
+        __syncthreads();
+        #pragma unroll
+        for (int r = 0; r < 16; r++) {
+          const int i = j + R2 * r;
+          v[r] = my[ex_at(i >> 4, i & 15)];
+        }
+      }
+      p2_transform<R, N, -1>(v, my, twS, j);
+    }
+
+    if (live) {
+      C *dst = f + lb + (int64_t)j * a.sa;
+      #pragma unroll
+      for (int m = 0; m < 16; m++) dst[m * step] = v[m];
+    }
+  }
+}
+
+}  // namespace atus

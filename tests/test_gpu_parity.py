@@ -267,3 +267,63 @@ def test_slab_cluster_pass_matches_axis_passes(prec, monkeypatch):
         s.block(20, KIND_BRAGG_AD, Laser.make(**kw), np.full(20, 0.8))
         res.append([s.psi(c) for c in range(2)])
     state_close(res[0], res[1], 1e-12 if prec == PREC_FP64 else 1e-6)
+
+
+def _run_cfg(h, ncomp, prec, psis, kind, nsteps, V=None, laser=None, F=None):
+    s = Solver(h, ncomp, prec)
+    for c in range(ncomp):
+        s.set_psi(c, psis[c])
+        s.set_alpha(c, [0.5, 0.4, 0.3])
+        if V is not None:
+            s.set_potential(c, V)
+    s.set_gs(list(np.linspace(30.0, 60.0, ncomp * ncomp)))
+    s.set_dt(1e-3)
+    s.block(nsteps, kind, laser, F)
+    return [s.psi(c) for c in range(ncomp)]
+
+
+@pytest.mark.parametrize("prec", [PREC_FP64, PREC_MIXED])
+@pytest.mark.parametrize("shape,ncomp,kind", [
+    ([32, 64, 128], 2, KIND_BRAGG_AD),   # 32/64/128-point pencils, two-component potential pass
+    ([256, 128], 1, KIND_NL),            # 2D, single component with a potential
+    ([64, 32, 256], 3, KIND_NL),         # three components: potential pass on the tile kernel
+])
+def test_register_staged_passes_match_tile_kernel(prec, shape, ncomp, kind, monkeypatch):
+    """The register-staged pass kernel and the shared-memory tile kernel run
+    the same Stockham stages, so whole Strang blocks agree to rounding."""
+    h = _grid(len(shape), shape, 16.0)
+    xs = _coords(h)
+    r2 = sum(x * x for x in xs)
+    psis = [(np.exp(-0.5 * r2 - 0.1 * c * r2) * np.exp(1j * (c + 1) * xs[0])).astype(np.complex128)
+            for c in range(ncomp)]
+    V = 0.5 * r2 if kind == KIND_NL else None
+    laser = Laser.make(Amp=[4.0, 4.0], laser_k=[3.0, 0], laser_domh=[2.0, 0]) if kind == KIND_BRAGG_AD else None
+    F = np.full(12, 0.8) if kind == KIND_BRAGG_AD else None
+    res = []
+    for p2 in ("1", "0"):
+        monkeypatch.setenv("ATUS_PASS2", p2)
+        res.append(_run_cfg(h, ncomp, prec, psis, kind, 12, V, laser, F))
+    err = np.linalg.norm(np.stack(res[0]) - np.stack(res[1])) / np.linalg.norm(np.stack(res[1]))
+    print(f"register-staged vs tile kernel: rel L2 {err:.3e}")
+    state_close(res[0], res[1], 1e-13 if prec == PREC_FP64 else 1e-5)
+
+
+def test_register_staged_sobolev_matches_tile_kernel(monkeypatch):
+    """Sobolev iterations (k-space filter inside the axis-0 pass) with both pass kernels."""
+    h = _grid(3, [64, 32, 16], 12.0)
+    x, y, z = _coords(h)
+    V = 0.5 * (x * x + 4 * y * y + 2.25 * z * z)
+    guess = np.sqrt(np.maximum(0.0, 3.0 - V)).astype(np.complex128) + 1e-3
+    res = []
+    for p2 in ("1", "0"):
+        monkeypatch.setenv("ATUS_PASS2", p2)
+        s = Solver(h, 1, PREC_FP64)
+        s.set_psi(0, guess)
+        s.set_potential(0, V)
+        s.set_gs([50.0])
+        s.sob_init([0.5], 0.01)
+        s.sob_renormalize()
+        for k in range(10):
+            s.sob_iterate()
+        res.append(s.psi(0))
+    assert rel_l2(res[0], res[1]) < 1e-13
