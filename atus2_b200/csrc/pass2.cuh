@@ -37,9 +37,14 @@ struct P2Cfg {
   static constexpr int B = E / (N * TC);   // pencils per tile
   static constexpr int NPC = B * TC;       // pencil-components per tile
   static constexpr int PB = 17 * R2 + 1;   // exchange pitch: R2 rows of 16 + 1 pad, odd
-  static constexpr int TWP = N + N / 8;    // twiddle table with one pad per 8 entries
+  static constexpr int TP = R2 + 1;        // twiddle row pitch (odd)
+  static constexpr int TWP = 16 * TP;      // twiddle table: row k holds W_N^{r k}, r < R2
   static constexpr size_t smem_ex = sizeof(cplx<R>) * NPC * PB;
-  static constexpr size_t smem = smem_ex + sizeof(typename TwTab<R>::type) * TWP;
+  static constexpr size_t smem_tw = sizeof(typename TwTab<R>::type) * TWP;
+  static constexpr size_t smem = smem_ex + smem_tw;
+  // k-space passes also keep the along-axis kinetic factors of up to two
+  // components in shared memory (FP64)
+  static constexpr size_t smem_kin = smem + 2 * N * sizeof(double2);
 };
 
 // Exchange layout of one pencil-component: row-major R2 x 16 with row pitch
@@ -50,6 +55,9 @@ __device__ __forceinline__ int ex_at(int row, int col) { return 17 * row + col; 
 
 // Stage 2 of a transform: butterflies k = j + R2 t (t < T2) of the pencil whose
 // exchange rows start at ex; o[t + T2 r] = output k + 16 r = point j + R2 (t + T2 r).
+// Twiddle W_N^{r k} is entry r of row k (pitch R2 + 1, odd): the eight threads
+// of a quarter warp, which hold eight different k on the contiguous axis, hit
+// eight different bank groups.
 template <typename R, int N, int DIR>
 __device__ __forceinline__ void p2_stage2(const cplx<R> *ex, const typename TwTab<R>::type *twS, int j, cplx<R> *o) {
   using C = cplx<R>;
@@ -61,10 +69,7 @@ __device__ __forceinline__ void p2_stage2(const cplx<R> *ex, const typename TwTa
     #pragma unroll
     for (int r = 0; r < R2; r++) u[r] = ex[ex_at(r, k)];
     #pragma unroll
-    for (int r = 1; r < R2; r++) {
-      const int m = r * k;
-      u[r] = twmul<DIR>(u[r], twS[m + (m >> 3)]);
-    }
+    for (int r = 1; r < R2; r++) u[r] = twmul<DIR>(u[r], twS[k * (R2 + 1) + r]);
     dftR<R2, DIR>(u);
     #pragma unroll
     for (int r = 0; r < R2; r++) o[t + T2 * r] = u[r];
@@ -103,9 +108,23 @@ __global__ void __launch_bounds__(Tile2<R>::NT, Tile2<R>::MINB) pass2_kernel(Pas
   else { j = tid % R2; b = (tid / R2) % B; c = tid / (R2 * B); }
   C *const my = ex + (c * B + b) * PB;
 
-  {  // exp(-2 pi i m / N), m < N, from the TWN-point table
+  {  // W_N^{r k} = exp(-2 pi i r k / N) from the TWN-point table
     const TW *tw = (const TW *)a.tw;
-    for (int m = tid; m < N; m += NT) twS[m + (m >> 3)] = tw[m * (TWN / N)];
+    for (int e = tid; e < 16 * R2; e += NT) {
+      const int k = e / R2, r = e % R2;
+      twS[k * Cfg::TP + r] = tw[(r * k) * (TWN / N)];
+    }
+  }
+  // k-space passes: along-axis kinetic factors of components 0 and 1
+  double2 *const s_kt = reinterpret_cast<double2 *>(smem_raw + Cfg::smem);
+  const bool kt_shared = (MODE == M2_KIN) && a.op == OP_KIN && a.ncomp_grid <= 2;
+  if (kt_shared) {
+    for (int e = tid; e < a.ncomp_grid * N; e += NT) {
+      const int cc = e / N, i = e % N;
+      const double2 *t0 = (a.axis == 0) ? a.kt[0][0] : (a.axis == 1) ? a.kt[0][1] : a.kt[0][2];
+      const double2 *t1 = (a.axis == 0) ? a.kt[1][0] : (a.axis == 1) ? a.kt[1][1] : a.kt[1][2];
+      s_kt[e] = (cc == 0) ? t0[i] : t1[i];
+    }
   }
   const int64_t W = a.per_comp ? a.ntiles * a.ncomp_grid : a.ntiles;
   const int nc = a.per_comp ? 1 : a.nc;
@@ -145,25 +164,36 @@ __global__ void __launch_bounds__(Tile2<R>::NT, Tile2<R>::MINB) pass2_kernel(Pas
       int p0[3];
       idx3(a.g, lb, p0[0], p0[1], p0[2]);
       if (a.op == OP_KIN) {
-        // ((psi^ s_f) K) s_b with K = (Kx Ky) Kz in FP64, as in pass_kernel
+        // psi^ <- ((psi^ s_f) K) s_b in FP64, K = K_along (product of the other
+        // two axis factors, x before y before z); complex64 fields take the
+        // scales folded into K
         const double2 *kx = a.kt[0][0], *ky = a.kt[0][1], *kz = a.kt[0][2];
         #pragma unroll
         for (int cc = 1; cc < MAXC; cc++)
           if (g.comp0 == cc) { kx = a.kt[cc][0]; ky = a.kt[cc][1]; kz = a.kt[cc][2]; }
         const double2 KX = __ldg(&kx[p0[0]]), KY = __ldg(&ky[p0[1]]), KZ = __ldg(&kz[p0[2]]);
+        double2 Kp = (a.axis == 0) ? cmul(KY, KZ) : (a.axis == 1) ? cmul(KX, KZ) : cmul(KX, KY);
+        const double2 *along = (a.axis == 0) ? kx : (a.axis == 1) ? ky : kz;
+        const double2 *sk = s_kt + (g.comp0 == 1 ? N : 0);
+        if (sizeof(R) == 4) {
+          const double sc = a.s_f * a.s_b;
+          Kp.x *= sc;
+          Kp.y *= sc;
+        }
         #pragma unroll
         for (int m = 0; m < 16; m++) {
           const int i = j + R2 * m;
-          const double2 fx = (a.axis == 0) ? __ldg(&kx[i]) : KX;
-          const double2 fy = (a.axis == 1) ? __ldg(&ky[i]) : KY;
-          const double2 fz = (a.axis == 2) ? __ldg(&kz[i]) : KZ;
-          const double2 K = cmul(cmul(fx, fy), fz);
+          const double2 K = cmul(kt_shared ? sk[i] : __ldg(&along[i]), Kp);
           double2 u = to_d<R>(v[m]);
-          u.x *= a.s_f;
-          u.y *= a.s_f;
+          if (sizeof(R) == 8) {
+            u.x *= a.s_f;
+            u.y *= a.s_f;
+          }
           u = cmul(u, K);
-          u.x *= a.s_b;
-          u.y *= a.s_b;
+          if (sizeof(R) == 8) {
+            u.x *= a.s_b;
+            u.y *= a.s_b;
+          }
           v[m] = from_d<R>(u);
         }
       } else if (a.op == OP_FILT) {
