@@ -100,6 +100,7 @@ SIGNATURES = {
     "atus_strang_block": (_i, [_vp, _i, _i, _dp]),
     "atus_profile_passes": (_i, [_vp, _i, _i, _dp, _dp, _dp, C.POINTER(C.c_int)]),
     "atus_particle_number": (_i, [_vp, _i, _dp]),
+    "atus_particle_number_noalloc": (_i, [_vp, C.c_int64, _i, C.c_double, _vp, _vp]),
     "atus_expval_position": (_i, [_vp, _i, _dp]),
     "atus_expval_momentum": (_i, [_vp, _i, _dp]),
     "atus_setup_momentum": (_i, [_vp, _i, _dp]),

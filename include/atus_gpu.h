@@ -40,6 +40,8 @@
  *   atus_setup_momentum             Setup_Momentum (include/CRT_Base.h:448-473)
  *   atus_rabi_integrals             compute_rabi_integrals (CRT_Base_IF.h:207-281)
  *   atus_sob_*                      CSOB_Base (include/CSOB_Base.h:96-543)
+ *   atus_particle_number_noalloc    no counterpart in the reference (see its
+ *                                   declaration below)
  */
 #ifndef ATUS_GPU_H
 #define ATUS_GPU_H
@@ -63,6 +65,7 @@ extern "C" {
 #define ATUS_E_CUDA (-3)        /* CUDA runtime error */
 #define ATUS_E_STATE (-4)       /* call not valid in the current state */
 #define ATUS_E_NOMEM (-5)       /* device allocation failed */
+#define ATUS_E_LIMIT (-6)       /* input larger than a fixed, documented limit */
 
 #define ATUS_PREC_FP64 0  /* complex128 fields, FP64 FFTs: the drop-in */
 #define ATUS_PREC_MIXED 1 /* complex64 fields and FFTs, FP64 phase arguments */
@@ -150,6 +153,31 @@ ATUS_API int atus_profile_passes(atus_ctx *ctx, int kind, int reps, double *ms, 
 
 /* ------------------------------------------------------------ observables */
 ATUS_API int atus_particle_number(atus_ctx *ctx, int comp, double *out);
+/* Particle number  ar * sum_l |psi_l|^2  of one field in device memory, with
+ * no allocation of any kind.  No counterpart in the reference: it is the
+ * reduction of atus_particle_number for callers that cannot allocate device
+ * memory -- a host framework whose caching allocator or fixed pool owns the
+ * device memory (a foreign cudaMalloc would fragment it or fail), or a time
+ * step that cannot take cudaFree's device-wide synchronisation.  It needs no
+ * context; its partial sums live in a fixed device array inside the library.
+ *
+ *   psi_dev    npts complex values (complex128 for ATUS_PREC_FP64, complex64
+ *              for ATUS_PREC_MIXED), device memory of the current device
+ *   ar         volume element (dx, dx*dy or dx*dy*dz)
+ *   out_dev    one double in device memory, written on `stream`
+ *   stream     cudaStream_t, NULL for the legacy default stream
+ *
+ * npts is limited to ATUS_NOALLOC_MAX_POINTS (2^27 points: one partial sum
+ * per 32768 points in a 32 KB array); larger fields return ATUS_E_LIMIT and
+ * launch nothing.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) with that device current; make that first
+ * call before any stream capture.  All calls on a device share the array, so
+ * calls whose kernels overlap on the GPU (other streams, other host threads)
+ * race and may return wrong sums: order them on one stream.  The result
+ * equals atus_particle_number's to rounding (another summation order). */
+#define ATUS_NOALLOC_MAX_POINTS 134217728LL
+ATUS_API int atus_particle_number_noalloc(const void *psi_dev, int64_t npts, int precision, double ar,
+                                          double *out_dev, void *stream);
 ATUS_API int atus_expval_position(atus_ctx *ctx, int comp, double *out /* dim */);
 ATUS_API int atus_expval_momentum(atus_ctx *ctx, int comp, double *out /* dim */);
 ATUS_API int atus_setup_momentum(atus_ctx *ctx, int comp, const double *p /* dim */);
