@@ -233,10 +233,96 @@ static int kinetic_pass(atus_ctx *ctx, int half) {
   return run_pass(ctx, 0, T_FWD, OP_KIN, T_INV, nullptr, half);
 }
 
+// Arguments of one pass over the context's fields, with the geometry the
+// launchers fill in (the plane pipeline takes three of them as they are).
+static PassArgs pass_args(const atus_ctx *ctx, int axis, int t1, int op, int t2, const NLArgs *nl) {
+  PassArgs a;
+  memset(&a, 0, sizeof(a));
+  for (int c = 0; c < MAXC; c++) a.psi[c] = (c < ctx->ncomp) ? ctx->psi[c] : nullptr;
+  a.t1 = t1;
+  a.op = op;
+  a.t2 = t2;
+  a.per_comp = (op != OP_NL) ? 1 : 0;
+  a.nc = (op == OP_NL) ? ctx->ncomp : 1;
+  a.s_f = scale_fak(ctx->dim, ctx->d);
+  a.s_b = scale_fak(ctx->dim, ctx->dk);
+  if (nl) a.nl = *nl;
+  int64_t sa = 1;
+  for (int b = axis + 1; b < 3; b++) sa *= ctx->n[b];
+  a.sa = sa;
+  a.x_along = (axis == 0);
+  a.axis = axis;
+  a.g = geo(ctx);
+  a.tw = (ctx->prec == ATUS_PREC_FP64) ? ctx->tw64 : ctx->tw;
+  for (int ax = 0; ax < 3; ax++) {
+    a.dk[ax] = ctx->dk[ax];
+    a.n[ax] = (int)ctx->n[ax];
+  }
+  a.ncomp_grid = ctx->ncomp;
+  return a;
+}
+
+// 3D real-space half step as one plane pipeline (pipe.cuh):
+// IFFT_y, IFFT_z -> potential -> FFT_z, FFT_y with the planes in flight held
+// in L2.  ATUS_E_UNSUPPORTED when the grid has no pipeline instantiation.
+static int pipe_pass(atus_ctx *ctx, const NLArgs &nl) {
+  if (!ctx->use_pipe || ctx->dim != 3 || ctx->ncomp > 2 || ctx->n[0] > PIPE_MAX_PLANES) return ATUS_E_UNSUPPORTED;
+  // complex64 fields: the three separate passes measured faster on B200
+  if (ctx->prec != ATUS_PREC_FP64 && !ctx->pipe_mixed) return ATUS_E_UNSUPPORTED;
+  if (ctx->n[1] != ctx->n[2] || ctx->n[1] < 32 || ctx->n[1] > 256) return ATUS_E_UNSUPPORTED;
+  if (!ctx->pipe) {
+    CK(cudaMalloc(&ctx->pipe, sizeof(PipeQueue)));
+    CK(cudaMemsetAsync(ctx->pipe, 0, sizeof(PipeQueue), ctx->stream));
+    ctx->pipe_epoch = 0;
+  }
+  if (ctx->pipe_epoch >= (1u << 20)) {  // keep epoch * items below 2^32
+    CK(cudaMemsetAsync(ctx->pipe, 0, sizeof(PipeQueue), ctx->stream));
+    ctx->pipe_epoch = 0;
+  }
+  PipeArgs a;
+  memset(&a, 0, sizeof(a));
+  a.pa = pass_args(ctx, 1, T_INV, OP_NONE, T_NONE, nullptr);
+  a.pb = pass_args(ctx, 2, T_INV, OP_NL, T_FWD, &nl);
+  a.pc = pass_args(ctx, 1, T_FWD, OP_NONE, T_NONE, nullptr);
+  a.q = ctx->pipe;
+  a.epoch = ctx->pipe_epoch + 1;
+  a.P = (int)ctx->n[0];
+  a.n1 = (int)ctx->n[1];
+  a.n2 = (int)ctx->n[2];
+  const int tc = tc_for(ctx->ncomp);
+  const int r = (ctx->prec == ATUS_PREC_FP64) ? launch_pipe_d(ctx, a, tc) : launch_pipe_f(ctx, a, tc);
+  if (r == ATUS_OK) {
+    ctx->pipe_epoch++;
+    ctx->pipe_pending = true;
+  }
+  return r;
+}
+
+// Reads the pipeline's error flag after the launches of a call (one small
+// copy and a stream synchronisation); a wait that gave up is a CUDA error.
+static int pipe_check(atus_ctx *ctx) {
+  if (!ctx->pipe_pending) return ATUS_OK;
+  ctx->pipe_pending = false;
+  unsigned *h = reinterpret_cast<unsigned *>(ctx->h_red);
+  CK(cudaMemcpyAsync(h, &ctx->pipe->err, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (*h != 0) {
+    CK(cudaMemsetAsync(ctx->pipe, 0, sizeof(PipeQueue), ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->pipe_epoch = 0;
+    return fail(ctx, ATUS_E_CUDA, "plane pipeline: a wait for another tile's results gave up");
+  }
+  return ATUS_OK;
+}
+
 // Real-space potential pass: 2D one pass over rows; 3D inverse y, rows, forward y.
 static int potential_pass(atus_ctx *ctx, const NLArgs &nl) {
   if (ctx->dim == 3) {
     const int r = slab_pass(ctx, 0, 1, 1, &nl, 1, 1, 0);
+    if (r != ATUS_E_UNSUPPORTED) return r;
+  }
+  if (ctx->dim == 3) {
+    const int r = pipe_pass(ctx, nl);
     if (r != ATUS_E_UNSUPPORTED) return r;
   }
   const int last = ctx->dim - 1;
@@ -339,6 +425,10 @@ int atus_create(const atus_grid *grid, int ncomp, int precision, atus_ctx **out)
     // ATUS_PASS2=0: tile kernel only (A/B comparisons of the two pass kernels)
     const char *p2 = getenv("ATUS_PASS2");
     ctx->use_pass2 = !(p2 && p2[0] == '0');
+    // ATUS_PIPE=0: 3D real-space half step as three separate passes
+    const char *pp = getenv("ATUS_PIPE");
+    ctx->use_pipe = ctx->use_pass2 && !(pp && pp[0] == '0');
+    ctx->pipe_mixed = (pp && pp[0] == '1');  // ATUS_PIPE=1 also pipelines complex64 fields
   }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) { delete ctx; return ATUS_E_CUDA; }
@@ -403,6 +493,7 @@ void atus_destroy(atus_ctx *ctx) {
       for (int ax = 0; ax < 3; ax++) cudaFree(ctx->kt[hf][c][ax]);
   }
   cudaFree(ctx->scratch);
+  cudaFree(ctx->pipe);
   if (ctx->tw != ctx->tw64) cudaFree(ctx->tw);
   cudaFree(ctx->tw64);
   cudaFree(ctx->red_partial);
@@ -609,7 +700,7 @@ int atus_strang_block(atus_ctx *ctx, int nk, int kind, const double *F) {
     ctx->t += last ? 0.5 * dt : dt;
   }
   RUN(transform_inner(ctx, T_INV));
-  return ATUS_OK;
+  return pipe_check(ctx);
 }
 
 int atus_profile_passes(atus_ctx *ctx, int kind, int reps, double *ms, double *lps, double *bytes, int *npass) {
@@ -660,8 +751,20 @@ int atus_profile_passes(atus_ctx *ctx, int kind, int reps, double *ms, double *l
         r = probe;
       }
     }
+    if (!slab_done && r == ATUS_OK && ctx->dim == 3) {  // the plane pipeline, when the grid has one
+      const int probe = pipe_pass(ctx, nl);
+      if (probe == ATUS_OK) {
+        r = pipe_check(ctx);
+        auto pipe = [&]() { return pipe_pass(ctx, nl); };
+        if (r == ATUS_OK) r = timed(pipe, 1.0, fb + vb);
+        if (r == ATUS_OK) r = pipe_check(ctx);
+        slab_done = true;
+      } else if (probe != ATUS_E_UNSUPPORTED) {
+        r = probe;
+      }
+    }
     if (slab_done) {
-      // one cluster pass replaces the three axis passes below
+      // one fused launch replaces the three axis passes below
     } else if (r == ATUS_OK && ctx->dim == 3) {
       auto yinv = [&]() { return run_pass(ctx, 1, T_INV, OP_NONE, T_NONE, nullptr, 0); };
       r = timed(yinv, 1.0, fb);

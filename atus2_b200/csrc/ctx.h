@@ -7,6 +7,7 @@
 #include "../../include/atus_gpu.h"
 #include "kernels.cuh"
 
+namespace atus { struct PipeQueue; }
 using namespace atus;
 
 struct atus_ctx {
@@ -31,6 +32,11 @@ struct atus_ctx {
   int64_t launches = 0;
   bool use_slab = true;         // 3D: fused (y,z) cluster pass when available
   bool use_pass2 = true;        // register-staged passes for pencils of 32..256 points
+  bool use_pipe = true;         // 3D: real-space half step as one plane pipeline
+  bool pipe_mixed = false;      // ... also for complex64 fields
+  PipeQueue *pipe = nullptr;    // its device-resident work queue
+  unsigned pipe_epoch = 0;      // pipeline launches since the queue was zeroed
+  bool pipe_pending = false;    // a launch whose error flag is not read yet
   std::string err;
   // Sobolev state
   bool sob_ready = false;

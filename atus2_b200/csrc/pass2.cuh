@@ -89,25 +89,16 @@ __device__ __forceinline__ void p2_transform(cplx<R> *v, cplx<R> *ex, const type
   p2_stage2<R, N, DIR>(ex, twS, j, v);
 }
 
-template <typename R, int N, int TC, int MODE, bool STRIDED>
-__global__ void __launch_bounds__(Tile2<R>::NT, Tile2<R>::MINB) pass2_kernel(PassArgs a) {
-  using C = cplx<R>;
+// Shared-memory set-up of a CTA, once per launch: the twiddle rows and, for
+// k-space passes, the along-axis kinetic factors of components 0 and 1.
+// Returns whether those factors are in shared memory.
+template <typename R, int N, int TC, int MODE>
+__device__ __forceinline__ bool p2_setup(const PassArgs &a, unsigned char *smem_raw) {
   using TW = typename TwTab<R>::type;
   using Cfg = P2Cfg<R, N, TC>;
-  constexpr int R2 = Cfg::R2, B = Cfg::B, NT = Cfg::NT, PB = Cfg::PB;
-  static_assert(N >= 32 && N <= 256, "two-stage pencils only");
-  static_assert(Cfg::NPC * R2 == NT, "one thread per stage-1 butterfly");
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C *const ex = reinterpret_cast<C *>(smem_raw);
-  TW *const twS = reinterpret_cast<TW *>(smem_raw + Cfg::smem_ex);
-  __shared__ double s_om[B], s_ec[B], s_es[B];
-
+  constexpr int R2 = Cfg::R2, NT = Cfg::NT;
   const int tid = threadIdx.x;
-  int b, j, c;
-  if (STRIDED) { b = tid % B; j = (tid / B) % R2; c = tid / (B * R2); }
-  else { j = tid % R2; b = (tid / R2) % B; c = tid / (R2 * B); }
-  C *const my = ex + (c * B + b) * PB;
-
+  TW *const twS = reinterpret_cast<TW *>(smem_raw + Cfg::smem_ex);
   {  // W_N^{r k} = exp(-2 pi i r k / N) from the TWN-point table
     const TW *tw = (const TW *)a.tw;
     for (int e = tid; e < 16 * R2; e += NT) {
@@ -126,162 +117,192 @@ __global__ void __launch_bounds__(Tile2<R>::NT, Tile2<R>::MINB) pass2_kernel(Pas
       s_kt[e] = (cc == 0) ? t0[i] : t1[i];
     }
   }
-  const int64_t W = a.per_comp ? a.ntiles * a.ncomp_grid : a.ntiles;
+  return kt_shared;
+}
+
+// One work item: the tile g of the pass described by a.  Field loads go
+// through L2 only (ld.global.cg) when L2LOAD is set -- the fused plane
+// pipeline reads data that other CTAs of the same launch wrote.
+template <typename R, int N, int TC, int MODE, bool STRIDED, bool L2LOAD>
+__device__ __forceinline__ void p2_item(const PassArgs &a, const TileGeo &g, unsigned char *smem_raw, bool kt_shared,
+                                        double *s_om, double *s_ec, double *s_es) {
+  using C = cplx<R>;
+  using TW = typename TwTab<R>::type;
+  using Cfg = P2Cfg<R, N, TC>;
+  constexpr int R2 = Cfg::R2, B = Cfg::B, NT = Cfg::NT, PB = Cfg::PB;
+  static_assert(N >= 32 && N <= 256, "two-stage pencils only");
+  static_assert(Cfg::NPC * R2 == NT, "one thread per stage-1 butterfly");
+  C *const ex = reinterpret_cast<C *>(smem_raw);
+  const TW *const twS = reinterpret_cast<const TW *>(smem_raw + Cfg::smem_ex);
+  const double2 *const s_kt = reinterpret_cast<const double2 *>(smem_raw + Cfg::smem);
+  const int tid = threadIdx.x;
+  int b, j, c;
+  if (STRIDED) { b = tid % B; j = (tid / B) % R2; c = tid / (B * R2); }
+  else { j = tid % R2; b = (tid / R2) % B; c = tid / (R2 * B); }
+  C *const my = ex + (c * B + b) * PB;
   const int nc = a.per_comp ? 1 : a.nc;
-  for (int64_t w = blockIdx.x; w < W; w += gridDim.x) {
-    const TileGeo g = tile_geo<B, N>(a, w);
-    const bool live = (b < g.nb) && (c < nc);
-    C *const f = (C *)pick(a.psi, g.comp0 + c);
-    const int64_t lb = g.base0 + b * g.pstride;  // grid index of the pencil's point 0
-    const int64_t step = (int64_t)R2 * a.sa;     // distance of points j + R2 m and j + R2 (m+1)
-    const C *src = live ? f + lb + (int64_t)j * a.sa : nullptr;
+  const bool live = (b < g.nb) && (c < nc);
+  C *const f = (C *)pick(a.psi, g.comp0 + c);
+  const int64_t lb = g.base0 + b * g.pstride;  // grid index of the pencil's point 0
+  const int64_t step = (int64_t)R2 * a.sa;     // distance of points j + R2 m and j + R2 (m+1)
+  const C *src = live ? f + lb + (int64_t)j * a.sa : nullptr;
 
-    if constexpr (MODE == M2_NL && TC > 1) {
-      // coupling of each pencil (x is constant along it); read after the
-      // barriers of the first transform
-      if (a.nl.kind == K_BRAGG && a.axis != 0)
-      for (int p = tid; p < B; p += NT) {
-        double om = 0, ec = 1, es = 0;
-        if (p < g.nb) {
-          int ix, iy, iz;
-          idx3(a.g, g.base0 + p * g.pstride, ix, iy, iz);
-          bragg_coupling(a.nl, (double)(ix - a.nl.shift0) * a.nl.dx0, om, ec, es);
-        }
-        s_om[p] = om; s_ec[p] = ec; s_es[p] = es;
+  if constexpr (MODE == M2_NL && TC > 1) {
+    // coupling of each pencil (x is constant along it); read after the
+    // barriers of the first transform
+    if (a.nl.kind == K_BRAGG && a.axis != 0)
+    for (int p = tid; p < B; p += NT) {
+      double om = 0, ec = 1, es = 0;
+      if (p < g.nb) {
+        int ix, iy, iz;
+        idx3(a.g, g.base0 + p * g.pstride, ix, iy, iz);
+        bragg_coupling(a.nl, (double)(ix - a.nl.shift0) * a.nl.dx0, om, ec, es);
       }
-    }
-
-    C v[16];
-    #pragma unroll
-    for (int r = 0; r < 16; r++) v[r] = live ? src[r * step] : mk<R>(0, 0);
-
-    if constexpr (MODE == M2_FWD) {
-      p2_transform<R, N, -1>(v, my, twS, j);
-    } else if constexpr (MODE == M2_INV) {
-      p2_transform<R, N, +1>(v, my, twS, j);
-    } else if constexpr (MODE == M2_KIN) {
-      p2_transform<R, N, -1>(v, my, twS, j);
-      int p0[3];
-      idx3(a.g, lb, p0[0], p0[1], p0[2]);
-      if (a.op == OP_KIN) {
-        // psi^ <- ((psi^ s_f) K) s_b in FP64, K = K_along (product of the other
-        // two axis factors, x before y before z); complex64 fields take the
-        // scales folded into K
-        const double2 *kx = a.kt[0][0], *ky = a.kt[0][1], *kz = a.kt[0][2];
-        #pragma unroll
-        for (int cc = 1; cc < MAXC; cc++)
-          if (g.comp0 == cc) { kx = a.kt[cc][0]; ky = a.kt[cc][1]; kz = a.kt[cc][2]; }
-        const double2 KX = __ldg(&kx[p0[0]]), KY = __ldg(&ky[p0[1]]), KZ = __ldg(&kz[p0[2]]);
-        double2 Kp = (a.axis == 0) ? cmul(KY, KZ) : (a.axis == 1) ? cmul(KX, KZ) : cmul(KX, KY);
-        const double2 *along = (a.axis == 0) ? kx : (a.axis == 1) ? ky : kz;
-        const double2 *sk = s_kt + (g.comp0 == 1 ? N : 0);
-        if (sizeof(R) == 4) {
-          const double sc = a.s_f * a.s_b;
-          Kp.x *= sc;
-          Kp.y *= sc;
-        }
-        #pragma unroll
-        for (int m = 0; m < 16; m++) {
-          const int i = j + R2 * m;
-          const double2 K = cmul(kt_shared ? sk[i] : __ldg(&along[i]), Kp);
-          double2 u = to_d<R>(v[m]);
-          if (sizeof(R) == 8) {
-            u.x *= a.s_f;
-            u.y *= a.s_f;
-          }
-          u = cmul(u, K);
-          if (sizeof(R) == 8) {
-            u.x *= a.s_b;
-            u.y *= a.s_b;
-          }
-          v[m] = from_d<R>(u);
-        }
-      } else if (a.op == OP_FILT) {
-        #pragma unroll
-        for (int m = 0; m < 16; m++) {
-          const int i = j + R2 * m;
-          double phi = 0;
-          #pragma unroll
-          for (int ax = 0; ax < 3; ax++) {
-            const int ii = (ax == a.axis) ? i : p0[ax];
-            const int t = (ii + a.n[ax] / 2) % a.n[ax];
-            const double k = a.dk[ax] * (double)(t - a.n[ax] / 2);
-            phi += (k * a.filt_alpha) * k;
-          }
-          const double fk = (a.filt_mode == FILT_SOBOLEV ? 1.0 / (1.0 + phi) : -phi) * a.filt_scale;
-          v[m].x = (R)((double)v[m].x * fk);
-          v[m].y = (R)((double)v[m].y * fk);
-        }
-      }
-      p2_transform<R, N, +1>(v, my, twS, j);
-    } else {  // M2_NL: IFFT -> potential step -> FFT
-      p2_transform<R, N, +1>(v, my, twS, j);
-      if constexpr (TC == 1) {
-        int p0[3];
-        idx3(a.g, lb, p0[0], p0[1], p0[2]);
-        #pragma unroll
-        for (int m = 0; m < 16; m++) {
-          const int i = j + R2 * m;
-          const int64_t l = lb + (int64_t)i * a.sa;
-          const int ix = (a.axis == 0) ? i : p0[0];
-          const double x0 = (double)(ix - a.nl.shift0) * a.nl.dx0;
-          double om = 0, ec = 1, es = 0;
-          if (a.nl.kind == K_BRAGG) bragg_coupling(a.nl, x0, om, ec, es);
-          C u[MAXC];
-          u[0] = v[m];
-          if (live) nl_point<R>(a.nl, u, l, x0, om, ec, es);
-          v[m] = u[0];
-        }
-      } else {
-        // all components of a point meet in shared memory (natural order)
-        __syncthreads();
-        #pragma unroll
-        for (int m = 0; m < 16; m++) {
-          const int i = j + R2 * m;
-          my[ex_at(i >> 4, i & 15)] = v[m];
-        }
-        __syncthreads();
-        constexpr int PPT = 16 / TC;  // points per thread
-        const bool bragg = (a.nl.kind == K_BRAGG);
-        #pragma unroll 2
-        for (int u_ = 0; u_ < PPT; u_++) {
-          const int p = tid + NT * u_;
-          int pb, i;
-          if (STRIDED) { pb = p % B; i = p / B; } else { i = p % N; pb = p / N; }
-          if (pb < g.nb) {
-            const int64_t l = g.base0 + pb * g.pstride + (int64_t)i * a.sa;
-            int ix, iy, iz;
-            idx3(a.g, l, ix, iy, iz);
-            const double x0 = (double)(ix - a.nl.shift0) * a.nl.dx0;
-            double om = 0, ec = 1, es = 0;
-            if (bragg) {
-              if (a.axis == 0) bragg_coupling(a.nl, x0, om, ec, es);
-              else { om = s_om[pb]; ec = s_ec[pb]; es = s_es[pb]; }
-            }
-            C u[MAXC];
-            #pragma unroll
-            for (int cc = 0; cc < TC; cc++) u[cc] = ex[(cc * B + pb) * PB + ex_at(i >> 4, i & 15)];
-            nl_point<R>(a.nl, u, l, x0, om, ec, es);
-            #pragma unroll
-            for (int cc = 0; cc < TC; cc++) ex[(cc * B + pb) * PB + ex_at(i >> 4, i & 15)] = u[cc];
-          }
-        }
-        __syncthreads();
-        #pragma unroll
-        for (int r = 0; r < 16; r++) {
-          const int i = j + R2 * r;
-          v[r] = my[ex_at(i >> 4, i & 15)];
-        }
-      }
-      p2_transform<R, N, -1>(v, my, twS, j);
-    }
-
-    if (live) {
-      C *dst = f + lb + (int64_t)j * a.sa;
-      #pragma unroll
-      for (int m = 0; m < 16; m++) dst[m * step] = v[m];
+      s_om[p] = om; s_ec[p] = ec; s_es[p] = es;
     }
   }
+
+  C v[16];
+  #pragma unroll
+  for (int r = 0; r < 16; r++) v[r] = live ? (L2LOAD ? __ldcg(&src[r * step]) : src[r * step]) : mk<R>(0, 0);
+
+  if constexpr (MODE == M2_FWD) {
+    p2_transform<R, N, -1>(v, my, twS, j);
+  } else if constexpr (MODE == M2_INV) {
+    p2_transform<R, N, +1>(v, my, twS, j);
+  } else if constexpr (MODE == M2_KIN) {
+    p2_transform<R, N, -1>(v, my, twS, j);
+    int p0[3];
+    idx3(a.g, lb, p0[0], p0[1], p0[2]);
+    if (a.op == OP_KIN) {
+      // psi^ <- ((psi^ s_f) K) s_b in FP64, K = K_along (product of the other
+      // two axis factors, x before y before z); complex64 fields take the
+      // scales folded into K
+      const double2 *kx = a.kt[0][0], *ky = a.kt[0][1], *kz = a.kt[0][2];
+      #pragma unroll
+      for (int cc = 1; cc < MAXC; cc++)
+        if (g.comp0 == cc) { kx = a.kt[cc][0]; ky = a.kt[cc][1]; kz = a.kt[cc][2]; }
+      const double2 KX = __ldg(&kx[p0[0]]), KY = __ldg(&ky[p0[1]]), KZ = __ldg(&kz[p0[2]]);
+      double2 Kp = (a.axis == 0) ? cmul(KY, KZ) : (a.axis == 1) ? cmul(KX, KZ) : cmul(KX, KY);
+      const double2 *along = (a.axis == 0) ? kx : (a.axis == 1) ? ky : kz;
+      const double2 *sk = s_kt + (g.comp0 == 1 ? N : 0);
+      if (sizeof(R) == 4) {
+        const double sc = a.s_f * a.s_b;
+        Kp.x *= sc;
+        Kp.y *= sc;
+      }
+      #pragma unroll
+      for (int m = 0; m < 16; m++) {
+        const int i = j + R2 * m;
+        const double2 K = cmul(kt_shared ? sk[i] : __ldg(&along[i]), Kp);
+        double2 u = to_d<R>(v[m]);
+        if (sizeof(R) == 8) {
+          u.x *= a.s_f;
+          u.y *= a.s_f;
+        }
+        u = cmul(u, K);
+        if (sizeof(R) == 8) {
+          u.x *= a.s_b;
+          u.y *= a.s_b;
+        }
+        v[m] = from_d<R>(u);
+      }
+    } else if (a.op == OP_FILT) {
+      #pragma unroll
+      for (int m = 0; m < 16; m++) {
+        const int i = j + R2 * m;
+        double phi = 0;
+        #pragma unroll
+        for (int ax = 0; ax < 3; ax++) {
+          const int ii = (ax == a.axis) ? i : p0[ax];
+          const int t = (ii + a.n[ax] / 2) % a.n[ax];
+          const double k = a.dk[ax] * (double)(t - a.n[ax] / 2);
+          phi += (k * a.filt_alpha) * k;
+        }
+        const double fk = (a.filt_mode == FILT_SOBOLEV ? 1.0 / (1.0 + phi) : -phi) * a.filt_scale;
+        v[m].x = (R)((double)v[m].x * fk);
+        v[m].y = (R)((double)v[m].y * fk);
+      }
+    }
+    p2_transform<R, N, +1>(v, my, twS, j);
+  } else {  // M2_NL: IFFT -> potential step -> FFT
+    p2_transform<R, N, +1>(v, my, twS, j);
+    if constexpr (TC == 1) {
+      int p0[3];
+      idx3(a.g, lb, p0[0], p0[1], p0[2]);
+      #pragma unroll
+      for (int m = 0; m < 16; m++) {
+        const int i = j + R2 * m;
+        const int64_t l = lb + (int64_t)i * a.sa;
+        const int ix = (a.axis == 0) ? i : p0[0];
+        const double x0 = (double)(ix - a.nl.shift0) * a.nl.dx0;
+        double om = 0, ec = 1, es = 0;
+        if (a.nl.kind == K_BRAGG) bragg_coupling(a.nl, x0, om, ec, es);
+        C u[MAXC];
+        u[0] = v[m];
+        if (live) nl_point<R>(a.nl, u, l, x0, om, ec, es);
+        v[m] = u[0];
+      }
+    } else {
+      // all components of a point meet in shared memory (natural order)
+      __syncthreads();
+      #pragma unroll
+      for (int m = 0; m < 16; m++) {
+        const int i = j + R2 * m;
+        my[ex_at(i >> 4, i & 15)] = v[m];
+      }
+      __syncthreads();
+      constexpr int PPT = 16 / TC;  // points per thread
+      const bool bragg = (a.nl.kind == K_BRAGG);
+      #pragma unroll 2
+      for (int u_ = 0; u_ < PPT; u_++) {
+        const int p = tid + NT * u_;
+        int pb, i;
+        if (STRIDED) { pb = p % B; i = p / B; } else { i = p % N; pb = p / N; }
+        if (pb < g.nb) {
+          const int64_t l = g.base0 + pb * g.pstride + (int64_t)i * a.sa;
+          int ix, iy, iz;
+          idx3(a.g, l, ix, iy, iz);
+          const double x0 = (double)(ix - a.nl.shift0) * a.nl.dx0;
+          double om = 0, ec = 1, es = 0;
+          if (bragg) {
+            if (a.axis == 0) bragg_coupling(a.nl, x0, om, ec, es);
+            else { om = s_om[pb]; ec = s_ec[pb]; es = s_es[pb]; }
+          }
+          C u[MAXC];
+          #pragma unroll
+          for (int cc = 0; cc < TC; cc++) u[cc] = ex[(cc * B + pb) * PB + ex_at(i >> 4, i & 15)];
+          nl_point<R>(a.nl, u, l, x0, om, ec, es);
+          #pragma unroll
+          for (int cc = 0; cc < TC; cc++) ex[(cc * B + pb) * PB + ex_at(i >> 4, i & 15)] = u[cc];
+        }
+      }
+      __syncthreads();
+      #pragma unroll
+      for (int r = 0; r < 16; r++) {
+        const int i = j + R2 * r;
+        v[r] = my[ex_at(i >> 4, i & 15)];
+      }
+    }
+    p2_transform<R, N, -1>(v, my, twS, j);
+  }
+
+  if (live) {
+    C *dst = f + lb + (int64_t)j * a.sa;
+    #pragma unroll
+    for (int m = 0; m < 16; m++) dst[m * step] = v[m];
+  }
+}
+
+template <typename R, int N, int TC, int MODE, bool STRIDED>
+__global__ void __launch_bounds__(Tile2<R>::NT, Tile2<R>::MINB) pass2_kernel(PassArgs a) {
+  using Cfg = P2Cfg<R, N, TC>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double s_om[Cfg::B], s_ec[Cfg::B], s_es[Cfg::B];
+  const bool kt_shared = p2_setup<R, N, TC, MODE>(a, smem_raw);
+  const int64_t W = a.per_comp ? a.ntiles * a.ncomp_grid : a.ntiles;
+  for (int64_t w = blockIdx.x; w < W; w += gridDim.x)
+    p2_item<R, N, TC, MODE, STRIDED, false>(a, tile_geo<Cfg::B, N>(a, w), smem_raw, kt_shared, s_om, s_ec, s_es);
 }
 
 }  // namespace atus
