@@ -12,6 +12,7 @@ from .engine import (  # noqa: F401
     STEP_NL,
     STEP_NL_IF,
     AtusError,
+    Batch,
     Laser,
     Solver,
     load_library,

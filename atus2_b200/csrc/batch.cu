@@ -1,0 +1,662 @@
+// batch.cu -- host side of the batched sweep (atus_batch_* in include/atus_gpu.h).
+//
+// Instances are grouped into size classes (1D length, or 2D edge).  A class
+// runs with one kernel variant, chosen by atus_batch_tune from timed probe
+// runs (default before tuning: the first candidate).  atus_batch_run captures
+// one Strang block of every class into a CUDA graph -- the 1D classes as one
+// persistent kernel each on a side stream, the 2D classes as their pass
+// sequence on the main stream -- and launches it; graphs are cached per
+// block length.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/atus_gpu.h"
+#include "batch.cuh"
+
+using namespace atus;
+
+bool batch1d_info_f(int N, int NT, int RES, BKernel *k);
+bool batch1d_info_d(int N, int NT, int RES, BKernel *k);
+bool batch2d_p2_info_f(int N, int mode, BKernel *k);
+bool batch2d_p2_info_d(int N, int mode, BKernel *k);
+bool batch2d_tile_info_f(int N, int mode, BKernel *k);
+bool batch2d_tile_info_d(int N, int mode, BKernel *k);
+
+namespace {
+
+enum { P_FWD = 0, P_INV = 1, P_KH = 2, P_KF = 3, P_POT = 4, NPASS = 5 };
+
+struct Variant {
+  int a = 0, b = 0;  // 1D: threads, resident components; 2D: BV_P2 / BV_TILE
+};
+
+struct Class {
+  int dim = 0, n = 0;
+  std::vector<int> ids;       // batch indices
+  std::vector<Variant> cands; // candidates of the autotuner
+  Variant v;                  // chosen
+  double probe_ms = -1;       // probe time of the chosen variant
+  std::vector<double> cand_ms;
+  int *d_ids = nullptr;       // device copy of ids
+  PassArgs *d_args[NPASS] = {};  // 2D: per instance and pass kind
+  int64_t items[NPASS] = {};
+};
+
+int ilog2(int64_t v) {
+  int l = 0;
+  while ((int64_t(1) << l) < v) l++;
+  return l;
+}
+int64_t wrapped(int64_t i, int64_t n) { return ((i + n / 2) % n) - n / 2; }
+double scale_fak(int dim, const double *s) {
+  if (dim == 1) return s[0] / sqrt(2.0 * M_PI);
+  return 0.5 * s[0] * s[1] / M_PI;
+}
+
+bool pow2(int64_t n) { return n >= 2 && (n & (n - 1)) == 0; }
+
+}  // namespace
+
+struct atus_batch {
+  int prec = 0;
+  double dt = 0;
+  std::vector<atus_batch_instance> inst;
+  std::vector<double> t;           // header times
+  std::vector<void *> psi[2];
+  std::vector<double2 *> kt[2][2]; // [half/full][axis] per instance
+  BInst1 *d_b1 = nullptr;          // per batch index (1D entries used)
+  Pulse *d_pulse = nullptr;
+  double *d_t0 = nullptr, *h_t0 = nullptr;
+  void *tw = nullptr;              // twiddles in the field precision
+  double2 *unit = nullptr;         // factor (1, 0) of the absent third axis
+  std::vector<Class> cls;
+  cudaStream_t st = nullptr;
+  std::vector<cudaStream_t> side;   // one per 1D class (concurrent persistent kernels)
+  std::vector<cudaEvent_t> joins;
+  cudaEvent_t ev_fork = nullptr, e0 = nullptr, e1 = nullptr;
+  std::map<const void *, int> resident;  // kernels with attributes set: CTAs per SM
+  std::map<int, cudaGraphExec_t> graphs;
+  std::string err;
+  int nsm = 148;
+};
+
+namespace {
+
+int fail(atus_batch *b, int code, const std::string &m) {
+  if (b) b->err = m;
+  return code;
+}
+#define BCK(call)                                                                                 \
+  do {                                                                                            \
+    cudaError_t _e = (call);                                                                      \
+    if (_e != cudaSuccess) return fail(b, ATUS_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(_e)); \
+  } while (0)
+
+size_t csize(const atus_batch *b) { return b->prec == ATUS_PREC_FP64 ? 16 : 8; }
+int64_t npts(const atus_batch_instance &in) {
+  return in.grid.dim == 1 ? in.grid.n[0] : in.grid.n[0] * in.grid.n[1];
+}
+
+bool info1d(const atus_batch *b, int N, const Variant &v, BKernel *k) {
+  return b->prec == ATUS_PREC_FP64 ? batch1d_info_d(N, v.a, v.b, k) : batch1d_info_f(N, v.a, v.b, k);
+}
+bool info2d(const atus_batch *b, int N, int variant, int mode, BKernel *k) {
+  if (variant == BV_P2)
+    return b->prec == ATUS_PREC_FP64 ? batch2d_p2_info_d(N, mode, k) : batch2d_p2_info_f(N, mode, k);
+  return b->prec == ATUS_PREC_FP64 ? batch2d_tile_info_d(N, mode, k) : batch2d_tile_info_f(N, mode, k);
+}
+
+NLArgs nl_of(const atus_batch *b, const atus_batch_instance &in) {
+  NLArgs a;
+  memset(&a, 0, sizeof(a));
+  a.kind = K_BRAGG;
+  a.ncomp = 2;
+  a.mdt = -b->dt;
+  a.dt = b->dt;
+  a.gs[0] = in.gs[0];
+  a.gs[1] = in.gs[1];
+  a.gs[MAXC] = in.gs[2];
+  a.gs[MAXC + 1] = in.gs[3];
+  a.L.beta0 = in.laser.beta[0];
+  for (int c = 0; c < MAXC; c++) a.L.DeltaL[c] = in.laser.DeltaL[c];
+  a.L.Amp0 = in.laser.Amp[0];
+  a.L.laser_k0 = in.laser.laser_k[0];
+  a.L.laser_dk0 = in.laser.laser_dk[0];
+  a.L.laser_domh0 = in.laser.laser_domh[0];
+  a.L.phase0 = in.laser.phase[0];
+  a.L.chirp_rate0 = in.laser.chirp_rate[0];
+  a.L.chirp = in.laser.chirp;
+  a.dx0 = in.grid.d[0];
+  a.shift0 = (int)(in.grid.n[0] / 2);
+  return a;
+}
+
+// Pass arguments of 2D instance i for pass kind p with B pencils per tile.
+PassArgs pass_of(const atus_batch *b, int i, int p, int B) {
+  const atus_batch_instance &in = b->inst[i];
+  const int64_t n0 = in.grid.n[0], n1 = in.grid.n[1];
+  PassArgs a;
+  memset(&a, 0, sizeof(a));
+  a.psi[0] = b->psi[0][i];
+  a.psi[1] = b->psi[1][i];
+  const int axis = (p == P_KH || p == P_KF) ? 0 : 1;
+  a.axis = axis;
+  a.x_along = (axis == 0);
+  a.per_comp = (p == P_POT) ? 0 : 1;
+  a.nc = (p == P_POT) ? 2 : 1;
+  a.ncomp_grid = 2;
+  a.t1 = (p == P_FWD || p == P_KH || p == P_KF) ? T_FWD : T_INV;
+  a.op = (p == P_POT) ? OP_NL : (p == P_KH || p == P_KF) ? OP_KIN : OP_NONE;
+  a.t2 = (p == P_POT) ? T_FWD : (p == P_KH || p == P_KF) ? T_INV : T_NONE;
+  for (int c = 0; c < 2; c++)
+    for (int ax = 0; ax < 2; ax++) a.kt[c][ax] = b->kt[p == P_KH ? 0 : 1][ax][i];
+  a.kt[0][2] = a.kt[1][2] = b->unit;  // read by the kinetic product at index 0
+  a.s_f = scale_fak(2, in.grid.d);
+  a.s_b = scale_fak(2, in.grid.dk);
+  a.tw = b->tw;
+  a.g.lg[0] = ilog2(n0);
+  a.g.lg[1] = ilog2(n1);
+  a.g.lg[2] = 0;
+  a.g.npts = n0 * n1;
+  a.nl = nl_of(b, in);
+  for (int ax = 0; ax < 3; ax++) {
+    a.dk[ax] = ax < 2 ? in.grid.dk[ax] : 0.0;
+    a.n[ax] = ax < 2 ? (int)in.grid.n[ax] : 1;
+  }
+  const int64_t N = axis == 0 ? n0 : n1;
+  const int64_t sa = axis == 0 ? n1 : 1;
+  a.sa = sa;
+  if (sa > 1) {
+    a.inner_tiles = (sa + B - 1) / B;
+    a.ntiles = (a.g.npts / (N * sa)) * a.inner_tiles;
+    a.npencils = 0;
+  } else {
+    a.inner_tiles = 1;
+    a.npencils = a.g.npts / N;
+    a.ntiles = (a.npencils + B - 1) / B;
+  }
+  return a;
+}
+
+const int PASS_MODE[NPASS] = {M2_FWD, M2_INV, M2_KIN, M2_KIN, M2_NL};
+
+// Device argument arrays of a 2D class for its variant.
+int build_2d_args(atus_batch *b, Class &c) {
+  const int m = (int)c.ids.size();
+  for (int p = 0; p < NPASS; p++) {
+    BKernel k;
+    if (!info2d(b, c.n, c.v.a, PASS_MODE[p], &k)) return fail(b, ATUS_E_UNSUPPORTED, "no 2D batch kernel for this size");
+    std::vector<PassArgs> h(m);
+    for (int q = 0; q < m; q++) h[q] = pass_of(b, c.ids[q], p, k.B);
+    if (!c.d_args[p]) BCK(cudaMalloc(&c.d_args[p], sizeof(PassArgs) * m));
+    BCK(cudaMemcpy(c.d_args[p], h.data(), sizeof(PassArgs) * m, cudaMemcpyHostToDevice));
+    c.items[p] = h[0].ntiles * (h[0].per_comp ? 2 : 1);
+  }
+  return ATUS_OK;
+}
+
+// Shared-memory attribute and occupancy of a kernel, set up once outside
+// any stream capture.
+int prepare(atus_batch *b, const BKernel &k) {
+  if (b->resident.count(k.fn)) return ATUS_OK;
+  BCK(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem));
+  int res = 0;
+  BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&res, k.fn, k.nt, k.smem));
+  if (res < 1) return fail(b, ATUS_E_UNSUPPORTED, "batch kernel does not fit on an SM");
+  b->resident[k.fn] = res;
+  return ATUS_OK;
+}
+
+int launch(atus_batch *b, const BKernel &k, int grid, void **args, cudaStream_t s) {
+  BCK(cudaLaunchKernel(k.fn, dim3(grid), dim3(k.nt), args, k.smem, s));
+  return ATUS_OK;
+}
+
+int grid_for(atus_batch *b, const BKernel &k, int64_t work) {
+  auto it = b->resident.find(k.fn);
+  const int res = it == b->resident.end() ? 1 : it->second;
+  const int64_t slots = (int64_t)b->nsm * res;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(work, slots));
+}
+
+// One Strang block of nk steps of class c on stream s.
+int enqueue_class(atus_batch *b, Class &c, int nk, cudaStream_t s) {
+  const int m = (int)c.ids.size();
+  if (c.dim == 1) {
+    BKernel k;
+    if (!info1d(b, c.n, c.v, &k)) return fail(b, ATUS_E_UNSUPPORTED, "no 1D batch kernel for this variant");
+    const BInst1 *insts = b->d_b1;
+    const int *order = c.d_ids;
+    const double *t0 = b->d_t0;
+    int ninst = m;
+    const void *tw = b->tw;
+    void *args[] = {(void *)&insts, (void *)&order, (void *)&t0, (void *)&ninst, (void *)&nk, (void *)&tw};
+    // one CTA per instance: the whole block of an instance runs in one CTA
+    return launch(b, k, grid_for(b, k, m), args, s);
+  }
+  auto pass = [&](int p, int step) -> int {
+    BKernel k;
+    if (!info2d(b, c.n, c.v.a, PASS_MODE[p], &k)) return fail(b, ATUS_E_UNSUPPORTED, "no 2D batch kernel");
+    BPass bp;
+    bp.args = c.d_args[p];
+    bp.ids = c.d_ids;
+    bp.pulse = b->d_pulse;
+    bp.t0 = b->d_t0;
+    bp.ninst = m;
+    bp.items = c.items[p];
+    bp.step = step;
+    bp.potential = (p == P_POT);
+    void *args[] = {(void *)&bp};
+    return launch(b, k, grid_for(b, k, bp.items * m), args, s);
+  };
+  int r = pass(P_FWD, 0);
+  if (r == ATUS_OK) r = pass(P_KH, 0);
+  for (int j = 0; j < nk && r == ATUS_OK; j++) {
+    r = pass(P_POT, j);
+    if (r == ATUS_OK) r = pass(j == nk - 1 ? P_KH : P_KF, 0);
+  }
+  if (r == ATUS_OK) r = pass(P_INV, 0);
+  return r;
+}
+
+void drop_graphs(atus_batch *b) {
+  for (auto &g : b->graphs) cudaGraphExecDestroy(g.second);
+  b->graphs.clear();
+}
+
+std::string variant_name(const Class &c, const Variant &v) {
+  char buf[64];
+  if (c.dim == 1) snprintf(buf, sizeof(buf), "%d threads, %d resident", v.a, v.b);
+  else snprintf(buf, sizeof(buf), "%s", v.a == BV_P2 ? "register-staged passes" : "shared-memory tile passes");
+  return buf;
+}
+
+}  // namespace
+
+extern "C" {
+
+int atus_batch_create(const atus_batch_instance *inst, int count, int precision, double dt, atus_batch **out) {
+  if (!inst || !out || count < 1 || !(dt > 0)) return ATUS_E_ARG;
+  if (precision != ATUS_PREC_FP64 && precision != ATUS_PREC_MIXED) return ATUS_E_ARG;
+  *out = nullptr;
+  atus_batch *b = new atus_batch();
+  b->prec = precision;
+  b->dt = dt;
+  b->inst.assign(inst, inst + count);
+  b->t.resize(count);
+  for (int i = 0; i < count; i++) {
+    const atus_grid &g = inst[i].grid;
+    bool ok = (g.dim == 1 && pow2(g.n[0]) && g.n[0] >= 1024 && g.n[0] <= 16384) ||
+              (g.dim == 2 && pow2(g.n[0]) && g.n[0] == g.n[1] && g.n[0] >= 64 && g.n[0] <= 512);
+    if (!ok) {
+      delete b;
+      return ATUS_E_UNSUPPORTED;
+    }
+    b->t[i] = g.t;
+  }
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, dev);
+  auto bail = [&](int code) {
+    atus_batch_destroy(b);
+    return code;
+  };
+  if (cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreate(&b->e0) != cudaSuccess || cudaEventCreate(&b->e1) != cudaSuccess)
+    return bail(ATUS_E_CUDA);
+  // twiddles exp(-2 pi i m / TWN): double2, or float4 (hi, lo) for complex64
+  {
+    const long double two_pi = 6.283185307179586476925286766559005768L;
+    std::vector<double2> t64(TWN);
+    for (int m = 0; m < TWN; m++) {
+      long double c, s;
+      if (m == 0) { c = 1; s = 0; }
+      else if (4 * m == TWN) { c = 0; s = 1; }
+      else if (2 * m == TWN) { c = -1; s = 0; }
+      else if (4 * m == 3 * TWN) { c = 0; s = -1; }
+      else { c = cosl(two_pi * m / TWN); s = sinl(two_pi * m / TWN); }
+      t64[m] = make_double2((double)c, (double)(-s));
+    }
+    if (precision == ATUS_PREC_FP64) {
+      if (cudaMalloc(&b->tw, 16 * TWN) != cudaSuccess) return bail(ATUS_E_NOMEM);
+      cudaMemcpy(b->tw, t64.data(), 16 * TWN, cudaMemcpyHostToDevice);
+    } else {
+      std::vector<float4> t4(TWN);
+      for (int m = 0; m < TWN; m++) {
+        t4[m].x = (float)t64[m].x;
+        t4[m].y = (float)t64[m].y;
+        t4[m].z = (float)(t64[m].x - (double)t4[m].x);
+        t4[m].w = (float)(t64[m].y - (double)t4[m].y);
+      }
+      if (cudaMalloc(&b->tw, sizeof(float4) * TWN) != cudaSuccess) return bail(ATUS_E_NOMEM);
+      cudaMemcpy(b->tw, t4.data(), sizeof(float4) * TWN, cudaMemcpyHostToDevice);
+    }
+  }
+  // fields and kinetic factors (the reference's double arithmetic,
+  // include/CRT_Base.h:257-271: phi = (-dt) ((k alpha) k) per axis)
+  for (int c = 0; c < 2; c++) b->psi[c].assign(count, nullptr);
+  for (int h = 0; h < 2; h++)
+    for (int ax = 0; ax < 2; ax++) b->kt[h][ax].assign(count, nullptr);
+  std::vector<BInst1> b1(count);
+  std::vector<Pulse> pulse(count);
+  for (int i = 0; i < count; i++) {
+    const atus_batch_instance &in = inst[i];
+    const int64_t np = npts(in);
+    for (int c = 0; c < 2; c++) {
+      if (cudaMalloc(&b->psi[c][i], csize(b) * np) != cudaSuccess) return bail(ATUS_E_NOMEM);
+      cudaMemset(b->psi[c][i], 0, csize(b) * np);
+    }
+    for (int ax = 0; ax < in.grid.dim; ax++) {
+      const int64_t n = in.grid.n[ax];
+      std::vector<double2> th(n), tf(n);
+      for (int64_t q = 0; q < n; q++) {
+        const double k = in.grid.dk[ax] * (double)wrapped(q, n);
+        const double phi = (-dt) * ((k * in.alpha) * k);
+        th[q] = make_double2(cos(0.5 * phi), sin(0.5 * phi));
+        tf[q] = make_double2(cos(phi), sin(phi));
+      }
+      if (cudaMalloc(&b->kt[0][ax][i], 16 * n) != cudaSuccess || cudaMalloc(&b->kt[1][ax][i], 16 * n) != cudaSuccess)
+        return bail(ATUS_E_NOMEM);
+      cudaMemcpy(b->kt[0][ax][i], th.data(), 16 * n, cudaMemcpyHostToDevice);
+      cudaMemcpy(b->kt[1][ax][i], tf.data(), 16 * n, cudaMemcpyHostToDevice);
+    }
+    pulse[i].tc = in.pulse_tc;
+    pulse[i].two_sigma2 = in.pulse_sigma > 0 ? 2.0 * in.pulse_sigma * in.pulse_sigma : 0.0;
+    memset(&b1[i], 0, sizeof(BInst1));
+    b1[i].psi[0] = b->psi[0][i];
+    b1[i].psi[1] = b->psi[1][i];
+    b1[i].kh = b->kt[0][0][i];
+    b1[i].kf = b->kt[1][0][i];
+    b1[i].s_f = scale_fak(1, in.grid.d);
+    b1[i].s_b = scale_fak(1, in.grid.dk);
+    b1[i].pulse = pulse[i];
+    b1[i].nl = nl_of(b, in);
+  }
+  {
+    const double2 one = make_double2(1.0, 0.0);
+    if (cudaMalloc(&b->unit, sizeof(double2)) != cudaSuccess) return bail(ATUS_E_NOMEM);
+    cudaMemcpy(b->unit, &one, sizeof(double2), cudaMemcpyHostToDevice);
+  }
+  if (cudaMalloc(&b->d_b1, sizeof(BInst1) * count) != cudaSuccess ||
+      cudaMalloc(&b->d_pulse, sizeof(Pulse) * count) != cudaSuccess ||
+      cudaMalloc(&b->d_t0, sizeof(double) * count) != cudaSuccess ||
+      cudaMallocHost(&b->h_t0, sizeof(double) * count) != cudaSuccess)
+    return bail(ATUS_E_NOMEM);
+  cudaMemcpy(b->d_b1, b1.data(), sizeof(BInst1) * count, cudaMemcpyHostToDevice);
+  cudaMemcpy(b->d_pulse, pulse.data(), sizeof(Pulse) * count, cudaMemcpyHostToDevice);
+  // size classes, instances longest run first (equal here) in batch order
+  std::map<std::pair<int, int>, int> key;
+  for (int i = 0; i < count; i++) {
+    const std::pair<int, int> kk(inst[i].grid.dim, (int)inst[i].grid.n[0]);
+    if (!key.count(kk)) {
+      key[kk] = (int)b->cls.size();
+      Class c;
+      c.dim = kk.first;
+      c.n = kk.second;
+      b->cls.push_back(c);
+    }
+    b->cls[key[kk]].ids.push_back(i);
+  }
+  for (Class &c : b->cls) {
+    if (cudaMalloc(&c.d_ids, sizeof(int) * c.ids.size()) != cudaSuccess) return bail(ATUS_E_NOMEM);
+    cudaMemcpy(c.d_ids, c.ids.data(), sizeof(int) * c.ids.size(), cudaMemcpyHostToDevice);
+    BKernel k;
+    if (c.dim == 1) {
+      for (int res : {2, 1})
+        for (int nt : {256, 512}) {
+          Variant v;
+          v.a = nt;
+          v.b = res;
+          if (info1d(b, c.n, v, &k)) c.cands.push_back(v);
+        }
+    } else {
+      for (int var : {BV_P2, BV_TILE}) {
+        Variant v;
+        v.a = var;
+        if (info2d(b, c.n, var, M2_NL, &k)) c.cands.push_back(v);
+      }
+    }
+    if (c.cands.empty()) return bail(fail(b, ATUS_E_UNSUPPORTED, "no batch kernel for a size class"));
+    for (const Variant &v : c.cands) {
+      if (c.dim == 1) {
+        if (info1d(b, c.n, v, &k) && prepare(b, k) != ATUS_OK) return bail(ATUS_E_CUDA);
+      } else {
+        for (int mode : {M2_FWD, M2_INV, M2_KIN, M2_NL})
+          if (info2d(b, c.n, v.a, mode, &k) && prepare(b, k) != ATUS_OK) return bail(ATUS_E_CUDA);
+      }
+    }
+    if (c.dim == 1) {
+      cudaStream_t s = nullptr;
+      cudaEvent_t e = nullptr;
+      if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return bail(ATUS_E_CUDA);
+      b->side.push_back(s);
+      if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return bail(ATUS_E_CUDA);
+      b->joins.push_back(e);
+    }
+    // before tuning: candidate ATUS_BATCH_VARIANT (default 0, clamped) -- lets
+    // tests run every variant
+    const char *ev = getenv("ATUS_BATCH_VARIANT");
+    const int vi = ev ? atoi(ev) : 0;
+    c.v = c.cands[std::min<size_t>((size_t)std::max(vi, 0), c.cands.size() - 1)];
+    if (c.dim == 2) {
+      const int r = build_2d_args(b, c);
+      if (r != ATUS_OK) return bail(r);
+    }
+  }
+  if (cudaDeviceSynchronize() != cudaSuccess) return bail(ATUS_E_CUDA);
+  *out = b;
+  return ATUS_OK;
+}
+
+void atus_batch_destroy(atus_batch *b) {
+  if (!b) return;
+  if (b->st) cudaStreamSynchronize(b->st);
+  for (cudaStream_t s : b->side) cudaStreamSynchronize(s);
+  drop_graphs(b);
+  for (int c = 0; c < 2; c++)
+    for (void *p : b->psi[c]) cudaFree(p);
+  for (int h = 0; h < 2; h++)
+    for (int ax = 0; ax < 2; ax++)
+      for (double2 *p : b->kt[h][ax]) cudaFree(p);
+  for (Class &c : b->cls) {
+    cudaFree(c.d_ids);
+    for (int p = 0; p < NPASS; p++) cudaFree(c.d_args[p]);
+  }
+  cudaFree(b->d_b1);
+  cudaFree(b->d_pulse);
+  cudaFree(b->d_t0);
+  if (b->h_t0) cudaFreeHost(b->h_t0);
+  cudaFree(b->tw);
+  cudaFree(b->unit);
+  if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+  for (cudaEvent_t e : b->joins) cudaEventDestroy(e);
+  if (b->e0) cudaEventDestroy(b->e0);
+  if (b->e1) cudaEventDestroy(b->e1);
+  if (b->st) cudaStreamDestroy(b->st);
+  for (cudaStream_t s : b->side) cudaStreamDestroy(s);
+  delete b;
+}
+
+const char *atus_batch_last_error(const atus_batch *b) { return b ? b->err.c_str() : "null batch"; }
+
+int atus_batch_upload_psi(atus_batch *b, int i, int comp, const double *psi) {
+  if (!b || !psi || i < 0 || i >= (int)b->inst.size() || comp < 0 || comp > 1) return ATUS_E_ARG;
+  const int64_t np = npts(b->inst[i]);
+  BCK(cudaStreamSynchronize(b->st));
+  if (b->prec == ATUS_PREC_FP64) {
+    BCK(cudaMemcpy(b->psi[comp][i], psi, 16 * np, cudaMemcpyHostToDevice));
+  } else {
+    std::vector<float2> f(np);
+    for (int64_t l = 0; l < np; l++) f[l] = make_float2((float)psi[2 * l], (float)psi[2 * l + 1]);
+    BCK(cudaMemcpy(b->psi[comp][i], f.data(), 8 * np, cudaMemcpyHostToDevice));
+  }
+  return ATUS_OK;
+}
+
+int atus_batch_download_psi(atus_batch *b, int i, int comp, double *psi) {
+  if (!b || !psi || i < 0 || i >= (int)b->inst.size() || comp < 0 || comp > 1) return ATUS_E_ARG;
+  const int64_t np = npts(b->inst[i]);
+  BCK(cudaStreamSynchronize(b->st));
+  if (b->prec == ATUS_PREC_FP64) {
+    BCK(cudaMemcpy(psi, b->psi[comp][i], 16 * np, cudaMemcpyDeviceToHost));
+  } else {
+    std::vector<float2> f(np);
+    BCK(cudaMemcpy(f.data(), b->psi[comp][i], 8 * np, cudaMemcpyDeviceToHost));
+    for (int64_t l = 0; l < np; l++) {
+      psi[2 * l] = f[l].x;
+      psi[2 * l + 1] = f[l].y;
+    }
+  }
+  return ATUS_OK;
+}
+
+int atus_batch_get_time(const atus_batch *b, int i, double *t) {
+  if (!b || !t || i < 0 || i >= (int)b->inst.size()) return ATUS_E_ARG;
+  *t = b->t[i];
+  return ATUS_OK;
+}
+
+int atus_batch_tune(atus_batch *b, int probe_steps) {
+  if (!b || probe_steps < 1) return ATUS_E_ARG;
+  BCK(cudaStreamSynchronize(b->st));
+  for (int i = 0; i < (int)b->inst.size(); i++) b->h_t0[i] = b->t[i];
+  BCK(cudaMemcpy(b->d_t0, b->h_t0, sizeof(double) * b->inst.size(), cudaMemcpyHostToDevice));
+  for (Class &c : b->cls) {
+    // probe on the real fields, restored from a copy afterwards
+    std::vector<void *> keep[2];
+    for (int comp = 0; comp < 2; comp++)
+      for (int i : c.ids) {
+        void *p = nullptr;
+        const size_t bytes = csize(b) * npts(b->inst[i]);
+        BCK(cudaMalloc(&p, bytes));
+        BCK(cudaMemcpy(p, b->psi[comp][i], bytes, cudaMemcpyDeviceToDevice));
+        keep[comp].push_back(p);
+      }
+    c.cand_ms.assign(c.cands.size(), -1.0);
+    int best = -1;
+    for (size_t q = 0; q < c.cands.size(); q++) {
+      c.v = c.cands[q];
+      if (c.dim == 2) {
+        const int r = build_2d_args(b, c);
+        if (r != ATUS_OK) return r;
+      }
+      int r = enqueue_class(b, c, probe_steps, b->st);  // warm-up (attributes, module load)
+      if (r != ATUS_OK) return r;
+      BCK(cudaEventRecord(b->e0, b->st));
+      r = enqueue_class(b, c, probe_steps, b->st);
+      if (r != ATUS_OK) return r;
+      BCK(cudaEventRecord(b->e1, b->st));
+      BCK(cudaEventSynchronize(b->e1));
+      float ms = 0;
+      BCK(cudaEventElapsedTime(&ms, b->e0, b->e1));
+      c.cand_ms[q] = ms;
+      if (best < 0 || ms < c.cand_ms[best]) best = (int)q;
+      for (int comp = 0; comp < 2; comp++)
+        for (size_t m = 0; m < c.ids.size(); m++)
+          BCK(cudaMemcpy(b->psi[comp][c.ids[m]], keep[comp][m], csize(b) * npts(b->inst[c.ids[m]]),
+                         cudaMemcpyDeviceToDevice));
+    }
+    for (int comp = 0; comp < 2; comp++)
+      for (void *p : keep[comp]) cudaFree(p);
+    c.v = c.cands[best];
+    c.probe_ms = c.cand_ms[best];
+    if (c.dim == 2) {
+      const int r = build_2d_args(b, c);
+      if (r != ATUS_OK) return r;
+    }
+  }
+  drop_graphs(b);
+  return ATUS_OK;
+}
+
+int atus_batch_run(atus_batch *b, int nk, double *ms) {
+  if (!b || nk < 1) return ATUS_E_ARG;
+  const int n = (int)b->inst.size();
+  BCK(cudaStreamSynchronize(b->st));
+  for (int i = 0; i < n; i++) b->h_t0[i] = b->t[i];
+  auto it = b->graphs.find(nk);
+  if (it == b->graphs.end()) {
+    cudaGraph_t g = nullptr;
+    BCK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+    int r = ATUS_OK;
+    cudaError_t e = cudaMemcpyAsync(b->d_t0, b->h_t0, sizeof(double) * n, cudaMemcpyHostToDevice, b->st);
+    if (e == cudaSuccess) e = cudaEventRecord(b->ev_fork, b->st);
+    // every 1D class on its own stream (its persistent kernel runs beside the
+    // 2D passes), the 2D classes in sequence on the main stream
+    size_t q = 0;
+    for (Class &c : b->cls) {
+      if (c.dim != 1) continue;
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(b->side[q], b->ev_fork, 0);
+      if (r == ATUS_OK && e == cudaSuccess) r = enqueue_class(b, c, nk, b->side[q]);
+      if (e == cudaSuccess) e = cudaEventRecord(b->joins[q], b->side[q]);
+      q++;
+    }
+    for (Class &c : b->cls)
+      if (r == ATUS_OK && e == cudaSuccess && c.dim == 2) r = enqueue_class(b, c, nk, b->st);
+    for (size_t w = 0; w < q && e == cudaSuccess; w++) e = cudaStreamWaitEvent(b->st, b->joins[w], 0);
+    const cudaError_t ee = cudaStreamEndCapture(b->st, &g);
+    if (r != ATUS_OK) {
+      if (g) cudaGraphDestroy(g);
+      return r;
+    }
+    if (e != cudaSuccess || ee != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      return fail(b, ATUS_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e != cudaSuccess ? e : ee));
+    }
+    cudaGraphExec_t x = nullptr;
+    const cudaError_t ie = cudaGraphInstantiate(&x, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) return fail(b, ATUS_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+    it = b->graphs.emplace(nk, x).first;
+  }
+  BCK(cudaEventRecord(b->e0, b->st));
+  BCK(cudaGraphLaunch(it->second, b->st));
+  BCK(cudaEventRecord(b->e1, b->st));
+  BCK(cudaEventSynchronize(b->e1));
+  if (ms) {
+    float f = 0;
+    BCK(cudaEventElapsedTime(&f, b->e0, b->e1));
+    *ms = f;
+  }
+  // header times with the reference's additions (half, full..., half)
+  const double dt = b->dt;
+  for (int i = 0; i < n; i++) {
+    double t = b->t[i] + 0.5 * dt;
+    for (int j = 0; j < nk; j++) t += (j == nk - 1) ? 0.5 * dt : dt;
+    b->t[i] = t;
+  }
+  return ATUS_OK;
+}
+
+int atus_batch_schedule(const atus_batch *b, char *buf, int len) {
+  if (!b || !buf || len < 1) return ATUS_E_ARG;
+  std::string s;
+  for (const Class &c : b->cls) {
+    char line[256];
+    if (c.dim == 1) snprintf(line, sizeof(line), "1D %d: %zu instances, %s", c.n, c.ids.size(), variant_name(c, c.v).c_str());
+    else snprintf(line, sizeof(line), "2D %dx%d: %zu instances, %s", c.n, c.n, c.ids.size(), variant_name(c, c.v).c_str());
+    s += line;
+    if (!c.cand_ms.empty()) {
+      s += " [probe ms:";
+      for (size_t q = 0; q < c.cands.size(); q++) {
+        snprintf(line, sizeof(line), " %s=%.3f;", variant_name(c, c.cands[q]).c_str(), c.cand_ms[q]);
+        s += line;
+      }
+      s += "]";
+    }
+    s += "\n";
+  }
+  snprintf(buf, (size_t)len, "%s", s.c_str());
+  return ATUS_OK;
+}
+
+}  // extern "C"

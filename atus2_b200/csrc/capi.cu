@@ -402,7 +402,7 @@ int atus_create(const atus_grid *grid, int ncomp, int precision, atus_ctx **out)
     ctx->n[a] = (a < grid->dim) ? grid->n[a] : 1;
     ctx->d[a] = (a < grid->dim) ? grid->d[a] : 0.0;
     ctx->dk[a] = (a < grid->dim) ? grid->dk[a] : 0.0;
-    if (ctx->n[a] < 1 || (ctx->n[a] & (ctx->n[a] - 1)) != 0 || ctx->n[a] > TWN) {
+    if (ctx->n[a] < 1 || (ctx->n[a] & (ctx->n[a] - 1)) != 0 || ctx->n[a] > 8192) {  // longest pass instantiation
       delete ctx;
       return ATUS_E_UNSUPPORTED;
     }

@@ -22,7 +22,7 @@
 namespace atus {
 
 constexpr int MAXC = 4;
-constexpr int TWN = 8192;  // twiddle table length (largest supported pencil)
+constexpr int TWN = 16384;  // twiddle table length (largest supported pencil)
 
 // Per-CTA tile budget in complex elements and threads per CTA.
 template <typename R> struct Tile;

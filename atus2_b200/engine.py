@@ -75,6 +75,13 @@ class Laser(C.Structure):
         return L
 
 
+class BatchInstance(C.Structure):
+    """atus_batch_instance: one bragg_ad run of a batched sweep."""
+
+    _fields_ = [("grid", Grid), ("alpha", C.c_double), ("gs", C.c_double * 4), ("laser", Laser),
+                ("pulse_tc", C.c_double), ("pulse_sigma", C.c_double)]
+
+
 # Every entry point of include/atus_gpu.h with its ctypes signature.
 _vp, _dp, _i, _d = C.c_void_p, C.POINTER(C.c_double), C.c_int, C.c_double
 SIGNATURES = {
@@ -101,6 +108,15 @@ SIGNATURES = {
     "atus_profile_passes": (_i, [_vp, _i, _i, _dp, _dp, _dp, C.POINTER(C.c_int)]),
     "atus_particle_number": (_i, [_vp, _i, _dp]),
     "atus_particle_number_noalloc": (_i, [_vp, C.c_int64, _i, C.c_double, _vp, _vp]),
+    "atus_batch_create": (_i, [C.POINTER(BatchInstance), _i, _i, _d, C.POINTER(C.c_void_p)]),
+    "atus_batch_destroy": (None, [_vp]),
+    "atus_batch_last_error": (C.c_char_p, [_vp]),
+    "atus_batch_upload_psi": (_i, [_vp, _i, _i, _dp]),
+    "atus_batch_download_psi": (_i, [_vp, _i, _i, _dp]),
+    "atus_batch_get_time": (_i, [_vp, _i, _dp]),
+    "atus_batch_tune": (_i, [_vp, _i]),
+    "atus_batch_run": (_i, [_vp, _i, _dp]),
+    "atus_batch_schedule": (_i, [_vp, C.c_char_p, _i]),
     "atus_expval_position": (_i, [_vp, _i, _dp]),
     "atus_expval_momentum": (_i, [_vp, _i, _dp]),
     "atus_setup_momentum": (_i, [_vp, _i, _dp]),
@@ -339,3 +355,74 @@ class Solver:
         mu = np.zeros(MAX_COMP)
         self._ok(self._L.atus_sob_mu(self._c, _dptr(mu)), "sob_mu")
         return mu[: self.ncomp]
+
+
+class Batch:
+    """Many independent two-component bragg_ad runs advanced together
+    (atus_batch_*): ``instances`` is a list of dicts with ``header`` (1D or
+    square 2D .bin header), ``alpha``, ``gs`` (4 values), ``laser`` (a
+    ``Laser``) and ``pulse`` = (tc, sigma) of AMP_T."""
+
+    def __init__(self, instances, precision: int = PREC_MIXED, dt: float = 1e-3):
+        self._L = load_library()
+        arr = (BatchInstance * len(instances))()
+        self.shapes = []
+        for i, d in enumerate(instances):
+            h = d["header"]
+            arr[i].grid = grid_from_header(h)
+            arr[i].alpha = float(d.get("alpha", 0.5))
+            for q, g in enumerate(d["gs"]):
+                arr[i].gs[q] = float(g)
+            arr[i].laser = d["laser"]
+            arr[i].pulse_tc, arr[i].pulse_sigma = (float(x) for x in d.get("pulse", (0.0, 0.0)))
+            dim = int(h["nDims"])
+            self.shapes.append(tuple(int(h[f"nDim{a}"]) for a in "XYZ"[:dim]))
+        self._b = C.c_void_p()
+        r = self._L.atus_batch_create(arr, len(instances), int(precision), float(dt), C.byref(self._b))
+        if r != ATUS_OK:
+            raise AtusError(f"atus_batch_create failed: {_ERRORS.get(r, r)}")
+        self.count = len(instances)
+
+    def close(self):
+        if getattr(self, "_b", None) and self._b.value:
+            self._L.atus_batch_destroy(self._b)
+            self._b = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ok(self, r: int, what: str):
+        if r != ATUS_OK:
+            msg = self._L.atus_batch_last_error(self._b)
+            raise AtusError(f"{what}: {_ERRORS.get(r, r)}: {msg.decode() if msg else ''}")
+
+    def set_psi(self, i: int, comp: int, data) -> None:
+        a = np.ascontiguousarray(np.asarray(data, dtype=np.complex128).reshape(self.shapes[i]))
+        self._ok(self._L.atus_batch_upload_psi(self._b, i, comp, _dptr(a.view(np.float64))), "batch_upload_psi")
+
+    def psi(self, i: int, comp: int) -> np.ndarray:
+        out = np.empty(self.shapes[i], dtype=np.complex128)
+        self._ok(self._L.atus_batch_download_psi(self._b, i, comp, _dptr(out.view(np.float64))), "batch_download_psi")
+        return out
+
+    def time(self, i: int) -> float:
+        t = C.c_double()
+        self._ok(self._L.atus_batch_get_time(self._b, i, C.byref(t)), "batch_get_time")
+        return t.value
+
+    def tune(self, probe_steps: int = 20) -> None:
+        self._ok(self._L.atus_batch_tune(self._b, int(probe_steps)), "batch_tune")
+
+    def run(self, nk: int) -> float:
+        """One Strang block of nk steps for every instance; device ms of the graph launch."""
+        ms = C.c_double()
+        self._ok(self._L.atus_batch_run(self._b, int(nk), C.byref(ms)), "batch_run")
+        return ms.value
+
+    def schedule(self) -> str:
+        buf = C.create_string_buffer(8192)
+        self._ok(self._L.atus_batch_schedule(self._b, buf, len(buf)), "batch_schedule")
+        return buf.value.decode()

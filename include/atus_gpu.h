@@ -42,6 +42,11 @@
  *   atus_sob_*                      CSOB_Base (include/CSOB_Base.h:96-543)
  *   atus_particle_number_noalloc    no counterpart in the reference (see its
  *                                   declaration below)
+ *   atus_batch_*                    many bragg runs at once: per instance the
+ *                                   Strang loop of CRT_Base_IF::run_sequence
+ *                                   (CRT_Base_IF.h:779-789) with the bragg_ad
+ *                                   step (bragg.cpp:185-304) and the AMP_T
+ *                                   pulse (CRT_Base_IF.h:170-198)
  */
 #ifndef ATUS_GPU_H
 #define ATUS_GPU_H
@@ -199,6 +204,42 @@ ATUS_API int atus_sob_iterate(atus_ctx *ctx, int n_iter, double *res, double *N)
 ATUS_API int atus_sob_run(atus_ctx *ctx, double epsilon, int max_iter, int *iters, double *res);
 /* mu_i = m_ar * sum[-Re(psi* Lap psi) + (V + sum_j g_ij |psi_j|^2) |psi_i|^2] */
 ATUS_API int atus_sob_mu(atus_ctx *ctx, double *mu /* ncomp */);
+
+/* ------------------------------------------------------------ batched sweep
+ * Independent two-component bragg_ad instances (1D lengths 1024..16384, square
+ * 2D grids 64^2..512^2; powers of two), all advanced by one CUDA-graph launch
+ * per Strang block: 1D instances by one persistent kernel per length with the
+ * instance resident in shared memory, 2D instances by batched passes over all
+ * instances of a size.  atus_batch_tune picks, per size class, the kernel
+ * variant (threads per CTA and resident components for 1D; register-staged or
+ * shared-memory tile passes for 2D) from timed probe runs on copies of the
+ * fields.  Each instance computes what a context with the same parameters
+ * computes with atus_strang_block(ATUS_STEP_BRAGG_AD) and F[j] =
+ * AMP_T(t1_j) = exp(-(t1_j - tc)^2 / (2 sigma^2)), t1_j = t0 + dt (j + 1). */
+typedef struct atus_batch atus_batch;
+typedef struct {
+  atus_grid grid;      /* dim 1 or 2, n, d, dk, t (2D: n[0] == n[1]) */
+  double alpha;        /* kinetic coefficient on every axis */
+  double gs[4];        /* g11, g12, g21, g22 */
+  atus_laser laser;    /* bragg_ad laser members */
+  double pulse_tc;     /* AMP_T centre */
+  double pulse_sigma;  /* AMP_T width; <= 0: AMP_T = 1 */
+} atus_batch_instance;
+ATUS_API int atus_batch_create(const atus_batch_instance *inst, int count, int precision, double dt,
+                               atus_batch **out);
+ATUS_API void atus_batch_destroy(atus_batch *b);
+ATUS_API const char *atus_batch_last_error(const atus_batch *b);
+/* Interleaved complex128 host buffers of the instance's grid size. */
+ATUS_API int atus_batch_upload_psi(atus_batch *b, int inst, int comp, const double *psi);
+ATUS_API int atus_batch_download_psi(atus_batch *b, int inst, int comp, double *psi);
+ATUS_API int atus_batch_get_time(const atus_batch *b, int inst, double *t);
+/* Autotuner: probe_steps Strang steps per candidate and size class. */
+ATUS_API int atus_batch_tune(atus_batch *b, int probe_steps);
+/* One Strang block of nk steps for every instance (one graph launch); *ms
+ * (may be NULL) receives its device time. */
+ATUS_API int atus_batch_run(atus_batch *b, int nk, double *ms);
+/* Human-readable schedule (size classes, chosen variants, probe times). */
+ATUS_API int atus_batch_schedule(const atus_batch *b, char *buf, int len);
 
 #ifdef __cplusplus
 }
