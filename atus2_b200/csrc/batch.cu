@@ -136,6 +136,7 @@ NLArgs nl_of(const atus_batch *b, const atus_batch_instance &in) {
   a.L.chirp = in.laser.chirp;
   a.dx0 = in.grid.d[0];
   a.shift0 = (int)(in.grid.n[0] / 2);
+  a.stable = in.bragg_stable ? 1 : 0;
   return a;
 }
 

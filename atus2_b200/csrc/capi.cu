@@ -117,6 +117,7 @@ static NLArgs nl_args(const atus_ctx *ctx, int kind, double t1, double F) {
   a.F = F;
   a.dx0 = ctx->d[0];
   a.shift0 = (int)(ctx->n[0] / 2);
+  a.stable = ctx->bragg_stable;
   return a;
 }
 
@@ -539,6 +540,12 @@ int atus_set_dt(atus_ctx *ctx, double dt) {
 int atus_get_dt(const atus_ctx *ctx, double *dt) {
   if (!ctx || !dt) return ATUS_E_ARG;
   *dt = ctx->dt;
+  return ATUS_OK;
+}
+
+int atus_set_bragg_stable(atus_ctx *ctx, int on) {
+  if (!ctx || (on != 0 && on != 1)) return ATUS_E_ARG;
+  ctx->bragg_stable = on;
   return ATUS_OK;
 }
 

@@ -37,6 +37,7 @@ struct atus_ctx {
   PipeQueue *pipe = nullptr;    // its device-resident work queue
   unsigned pipe_epoch = 0;      // pipeline launches since the queue was zeroed
   bool pipe_pending = false;    // a launch whose error flag is not read yet
+  int bragg_stable = 0;         // FP64 Bragg step in the eigenvalue-free form
   std::string err;
   // Sobolev state
   bool sob_ready = false;

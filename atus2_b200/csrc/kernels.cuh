@@ -57,6 +57,7 @@ struct NLArgs {
   double F;                 // pulse amplitude
   double dx0;               // grid step of axis 0
   int shift0;               // n0 / 2
+  int stable;               // FP64 Bragg step in the eigenvalue-free form (1) or the reference's (0)
 };
 
 struct Geo {
@@ -200,6 +201,7 @@ __device__ __forceinline__ void nl_point(const NLArgs &a, cplx<R> *v, int64_t l,
   const double V22 = a.gs[MAXC] * rho[0] + a.gs[MAXC + 1] * rho[1] - a.L.DeltaL[1] + a.L.beta0 * x0;
   const double dt = a.dt;
   if constexpr (sizeof(R) == 8) {
+   if (!a.stable) {
     double re1, im1;
     if (Omega == 0.0) {
       sincos_step(-dt * V11, &im1, &re1);
@@ -229,15 +231,20 @@ __device__ __forceinline__ void nl_point(const NLArgs &a, cplx<R> *v, int64_t l,
     const double2 p1 = v[0], p2 = v[1];
     v[0] = cadd(cmul(O11, p1), cmul(O12, p2));
     v[1] = cadd(cmul(O21, p1), cmul(O22, p2));
-  } else {
+    return;
+   }
+  }
+  {
     // U = e^{-i dt m} [cos(r dt) I - i sin(r dt)/r [[d, W], [W, -d]]], m = (V11+V22)/2,
     // d = (V11-V22)/2, W = Omega, r = sqrt(d^2 + W^2); off-diagonals times eta / conj(eta).
-    // The matrix is built in FP64 from renormalised (cos, sin) pairs, so it is
-    // unitary to FP64 accuracy; only the fields are complex64.
+    // The matrix is built in FP64 from unit (cos, sin) pairs, so it is unitary
+    // to FP64 accuracy for every Omega (the reference's eigen-form divides by
+    // (V11 - E)^2 + Omega^2, which loses unitarity once Omega is below the
+    // spacing of V and divides by zero once Omega^2 underflows).
     const double m = 0.5 * (V11 + V22), d = 0.5 * (V11 - V22);
     const double r = sqrt(d * d + Omega * Omega);
-    const double2 e = expi<float>(-dt * m);   // e^{-i dt m}
-    const double2 rr = expi<float>(dt * r);   // (cos r dt, sin r dt)
+    const double2 e = expi<R>(-dt * m);   // e^{-i dt m}
+    const double2 rr = expi<R>(dt * r);   // (cos r dt, sin r dt)
     const double sor = (r > 0.0) ? rr.y / r : dt;
     const double fd = sor * d, fw = sor * Omega;
     // U11 = e(cos - i fd), U22 = e(cos + i fd), Uoff = e(-i fw)

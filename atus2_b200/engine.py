@@ -79,7 +79,7 @@ class BatchInstance(C.Structure):
     """atus_batch_instance: one bragg_ad run of a batched sweep."""
 
     _fields_ = [("grid", Grid), ("alpha", C.c_double), ("gs", C.c_double * 4), ("laser", Laser),
-                ("pulse_tc", C.c_double), ("pulse_sigma", C.c_double)]
+                ("pulse_tc", C.c_double), ("pulse_sigma", C.c_double), ("bragg_stable", C.c_int)]
 
 
 # Every entry point of include/atus_gpu.h with its ctypes signature.
@@ -107,6 +107,7 @@ SIGNATURES = {
     "atus_strang_block": (_i, [_vp, _i, _i, _dp]),
     "atus_profile_passes": (_i, [_vp, _i, _i, _dp, _dp, _dp, C.POINTER(C.c_int)]),
     "atus_particle_number": (_i, [_vp, _i, _dp]),
+    "atus_set_bragg_stable": (_i, [_vp, _i]),
     "atus_particle_number_noalloc": (_i, [_vp, C.c_int64, _i, C.c_double, _vp, _vp]),
     "atus_batch_create": (_i, [C.POINTER(BatchInstance), _i, _i, _d, C.POINTER(C.c_void_p)]),
     "atus_batch_destroy": (None, [_vp]),
@@ -262,6 +263,10 @@ class Solver:
             raise ValueError("potential size does not match the grid")
         self._ok(self._L.atus_set_potential(self._c, comp, _dptr(a)), "set_potential")
 
+    def set_bragg_stable(self, on: bool = True) -> None:
+        """FP64 bragg_ad in the eigenvalue-free form instead of the reference's eigen-form."""
+        self._ok(self._L.atus_set_bragg_stable(self._c, int(bool(on))), "set_bragg_stable")
+
     def set_laser(self, laser: Laser) -> None:
         self._ok(self._L.atus_set_laser(self._c, C.byref(laser)), "set_laser")
 
@@ -375,6 +380,7 @@ class Batch:
                 arr[i].gs[q] = float(g)
             arr[i].laser = d["laser"]
             arr[i].pulse_tc, arr[i].pulse_sigma = (float(x) for x in d.get("pulse", (0.0, 0.0)))
+            arr[i].bragg_stable = int(bool(d.get("bragg_stable", False)))
             dim = int(h["nDims"])
             self.shapes.append(tuple(int(h[f"nDim{a}"]) for a in "XYZ"[:dim]))
         self._b = C.c_void_p()

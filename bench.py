@@ -381,11 +381,136 @@ def atus_arm(args, rank, ws, local, dist):
     out["e2e"] = {"value": ws * npts * E2E_NK * e2e_steps / (ms_e * 1e-3), "unit": UNIT,
                   "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo,
                   "step": f"upload 2 components, {E2E_NK} Strang steps, download 2 components", "steps": e2e_steps}
+    if not args.no_batch:
+        barrier(dist)
+        out["variants"]["batch"] = run_batch()
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = run_cpu_baseline()
     barrier(dist)
     if rank == 0:
         print(json.dumps(out))
+
+
+# ------------------------------------------------------------------ batched sweep
+BATCH_COUNT, BATCH_STEPS, BATCH_SEED = 768, 4000, 1
+
+
+def run_batch(stream_unused=None):
+    """The batched Bragg sweep: BATCH_COUNT instances drawn from seed 1
+    (atus2_b200.sweep), complex64 fields with FP64 phase arguments, autotuned,
+    BATCH_STEPS steps as one graph launch.  Against it: the same instances one
+    by one in plain FP64, timed on one representative instance per size class
+    over the full BATCH_STEPS -- a context where one exists, a single-instance
+    FP64 batch for 1D 8192 (no FP64 context fits one SM), and for 1D 16384
+    (no FP64 kernel at all) the 8192 time scaled by 2 * 14/13, the FFT work
+    ratio -- which also gives the accuracy of each class after BATCH_STEPS
+    steps."""
+    import torch
+
+    from atus2_b200 import PREC_FP64, PREC_MIXED, STEP_BRAGG_AD, Batch, Solver, sweep
+
+    insts = sweep.draw(BATCH_COUNT, BATCH_SEED)
+    b = Batch(insts, PREC_MIXED, DT)
+    for i, d in enumerate(insts):
+        p = sweep.initial_state(d["header"])
+        b.set_psi(i, 0, p)
+        b.set_psi(i, 1, np.zeros_like(p))
+    t_tune = time.perf_counter()
+    b.tune(20)
+    t_tune = time.perf_counter() - t_tune
+    ms = b.run(BATCH_STEPS)
+    classes = {}
+    for i, d in enumerate(insts):
+        h = d["header"]
+        key = (int(h["nDims"]), int(h["nDimX"]))
+        classes.setdefault(key, []).append(i)
+    seq_ms = {}
+    errs = {}
+    for key, ids in sorted(classes.items()):
+        if key == (1, 16384):
+            continue
+        i = ids[0]
+        d = insts[i]
+        h = d["header"]
+        if key == (1, 8192):
+            # two complex128 components of 8192 points exceed one SM's shared
+            # memory for a context: a single-instance FP64 batch (one component
+            # resident) is the plain FP64 run of this instance
+            one = Batch([dict(d, bragg_stable=True)], PREC_FP64, DT)
+            p = sweep.initial_state(h)
+            one.set_psi(0, 0, p)
+            one.set_psi(0, 1, np.zeros_like(p))
+            seq_ms[key] = one.run(BATCH_STEPS)
+            ref = np.stack([one.psi(0, 0), one.psi(0, 1)])
+            got = np.stack([b.psi(i, 0), b.psi(i, 1)])
+            errs[f"{key[0]}D-{key[1]}"] = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+            one.close()
+            continue
+        s = Solver(h, 2, PREC_FP64)
+        s.set_bragg_stable(True)  # the reference's eigen-form diverges in this sweep's pulse tails
+        p = sweep.initial_state(h)
+        s.set_psi(0, p)
+        s.set_psi(1, np.zeros_like(p))
+        for c in range(2):
+            s.set_alpha(c, [0.5] * key[0])
+        s.set_gs(d["gs"])
+        s.set_dt(DT)
+        F = sweep.pulse_values(0.0, BATCH_STEPS, *d["pulse"], DT)
+        s.synchronize()
+        t0 = time.perf_counter()
+        s.block(BATCH_STEPS, STEP_BRAGG_AD, d["laser"], F)
+        s.synchronize()
+        seq_ms[key] = (time.perf_counter() - t0) * 1e3
+        ref = np.stack([s.psi(0), s.psi(1)])
+        got = np.stack([b.psi(i, 0), b.psi(i, 1)])
+        errs[f"{key[0]}D-{key[1]}"] = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+        s.close()
+    # the reference's own FP64 form on the same instances (what the drop-in
+    # computes): its norm after the run, per class
+    ref_norms = {}
+    for key, ids in sorted(classes.items()):
+        if key[0] != 1 or key[1] > 4096:
+            continue
+        d = insts[ids[0]]
+        h = d["header"]
+        s = Solver(h, 2, PREC_FP64)
+        p = sweep.initial_state(h)
+        s.set_psi(0, p)
+        s.set_psi(1, np.zeros_like(p))
+        for c in range(2):
+            s.set_alpha(c, [0.5])
+        s.set_gs(d["gs"])
+        s.set_dt(DT)
+        s.block(BATCH_STEPS, STEP_BRAGG_AD, d["laser"], sweep.pulse_values(0.0, BATCH_STEPS, *d["pulse"], DT))
+        ref_norms[f"1D-{key[1]}"] = s.particle_number(0) + s.particle_number(1)
+        s.close()
+    if (1, 16384) in classes and (1, 8192) in classes:
+        seq_ms[(1, 16384)] = seq_ms[(1, 8192)] * 2 * 14 / 13
+    seq_total = sum(seq_ms[k] * len(v) for k, v in classes.items())
+    work = BATCH_COUNT * BATCH_STEPS
+    sched = b.schedule()
+    b.close()
+    return {
+        "metric": "instance-steps/s (batched Bragg sweep)",
+        "value": work / (ms * 1e-3),
+        "unit": "instance-steps/s",
+        "ms": ms,
+        "instances": BATCH_COUNT,
+        "steps": BATCH_STEPS,
+        "dtype": "c64 fields, f64 phase arguments",
+        "sequential_fp64": {"value": work / (seq_total * 1e-3), "unit": "instance-steps/s",
+                            "ms": seq_total, "method": "one FP64 context per instance, one block of "
+                            f"{BATCH_STEPS} steps; per size class one instance timed (wall clock around the "
+                            "synchronised call), times summed over the instances"},
+        "speedup_vs_sequential_fp64": seq_total / ms,
+        "rel_l2_vs_fp64_after_run": errs,
+        "fp64_reference": "eigenvalue-free 2x2 exponential (atus_set_bragg_stable); the reference's eigen-form "
+                          "loses unitarity in the pulse tails of this sweep",
+        "reference_form_norm_after_run": ref_norms,
+        "tune_s": t_tune,
+        "schedule": sched.strip().split("\n"),
+        "classes": {f"{k[0]}D-{k[1]}": len(v) for k, v in sorted(classes.items())},
+    }
 
 
 # ------------------------------------------------------------------ reference arm
@@ -427,6 +552,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="atus", choices=["atus", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-sweep variant")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, ws, local, dist = dist_init()

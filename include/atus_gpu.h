@@ -129,6 +129,13 @@ ATUS_API int atus_set_gs(atus_ctx *ctx, const double *gs /* ncomp*ncomp, row i =
 /* V: N doubles in grid order, or NULL to drop the potential of comp. */
 ATUS_API int atus_set_potential(atus_ctx *ctx, int comp, const double *V);
 ATUS_API int atus_set_laser(atus_ctx *ctx, const atus_laser *laser);
+/* on = 1: FP64 contexts take the bragg_ad step in the eigenvalue-free form
+ * U = e^{-i dt m}[cos(r dt) - i sin(r dt)/r (H - m)] (complex64 contexts always
+ * do).  No counterpart in the reference: its eigen-form (bragg.cpp:254-277)
+ * divides by (V11 - E)^2 + Omega^2, loses unitarity once |Omega| is below the
+ * spacing of V11 and divides by zero once Omega^2 underflows -- the tails of a
+ * Gaussian pulse reach both.  Default 0: the reference's form, bit for bit. */
+ATUS_API int atus_set_bragg_stable(atus_ctx *ctx, int on);
 
 /* ------------------------------------------------------------ fields */
 /* Interleaved complex128, N values, grid order (the .bin payload). */
@@ -224,6 +231,7 @@ typedef struct {
   atus_laser laser;    /* bragg_ad laser members */
   double pulse_tc;     /* AMP_T centre */
   double pulse_sigma;  /* AMP_T width; <= 0: AMP_T = 1 */
+  int bragg_stable;    /* FP64 batches: the eigenvalue-free form (atus_set_bragg_stable) */
 } atus_batch_instance;
 ATUS_API int atus_batch_create(const atus_batch_instance *inst, int count, int precision, double dt,
                                atus_batch **out);
