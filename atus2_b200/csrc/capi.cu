@@ -356,6 +356,23 @@ static int reduce(atus_ctx *ctx, RedArgs &a, double *out) {
   return ATUS_OK;
 }
 
+// The same reduction, result left in device memory (no host round trip).
+static int reduce_dev(atus_ctx *ctx, RedArgs &a, double *dst) {
+  a.g = geo(ctx);
+  a.dim = ctx->dim;
+  for (int ax = 0; ax < 3; ax++) {
+    a.d[ax] = ctx->d[ax];
+    a.dk[ax] = ctx->dk[ax];
+    a.n[ax] = (int)ctx->n[ax];
+    a.shift[ax] = (int)(ctx->n[ax] / 2);
+  }
+  reduce_kernel<double><<<RED_BLOCKS, RED_THREADS, 0, ctx->stream>>>(a, ctx->red_partial);
+  LAUNCHED(ctx);
+  reduce_final<<<1, 32, 0, ctx->stream>>>(ctx->red_partial, RED_BLOCKS, a.nq, dst);
+  LAUNCHED(ctx);
+  return ATUS_OK;
+}
+
 static int grid_blocks(int64_t n, int threads) {
   int64_t b = (n + threads - 1) / threads;
   return (int)(b < 148 * 16 ? b : 148 * 16);
@@ -444,6 +461,7 @@ int atus_create(const atus_grid *grid, int ncomp, int precision, atus_ctx **out)
   if (ok) ok = cudaMalloc(&ctx->red_partial, sizeof(double) * RED_BLOCKS * RED_MAXQ) == cudaSuccess;
   if (ok) ok = cudaMalloc(&ctx->red_out, sizeof(double) * RED_MAXQ) == cudaSuccess;
   if (ok) ok = cudaMallocHost(&ctx->h_red, sizeof(double) * RED_MAXQ) == cudaSuccess;
+  if (ok) ok = cudaMallocHost(&ctx->h_sob, sizeof(SobDev)) == cudaSuccess;
   if (ok) {
     ok = cudaMalloc(&ctx->tw64, 16 * TWN) == cudaSuccess;
     if (ok) {
@@ -495,6 +513,9 @@ void atus_destroy(atus_ctx *ctx) {
   }
   cudaFree(ctx->scratch);
   cudaFree(ctx->pipe);
+  cudaFree(ctx->sob_dev);
+  if (ctx->sob_graph) cudaGraphExecDestroy(ctx->sob_graph);
+  if (ctx->h_sob) cudaFreeHost(ctx->h_sob);
   if (ctx->tw != ctx->tw64) cudaFree(ctx->tw);
   cudaFree(ctx->tw64);
   cudaFree(ctx->red_partial);
@@ -894,7 +915,7 @@ static int sob_filter(atus_ctx *ctx, void *buf, int mode, double alpha) {
     a.filt_scale = round_trip_scale(ctx);
     const int saved_nc = ctx->ncomp;
     ctx->ncomp = 1;
-    r = launch_pass_d1(ctx, a, 0);
+    r = dispatch_pass(ctx, a, 0, 1);
     ctx->ncomp = saved_nc;
   }
   for (int ax = 1; ax < ctx->dim && r == ATUS_OK; ax++) r = run_pass(ctx, ax, T_INV, OP_NONE, T_NONE, nullptr, 0, f, 1);
@@ -993,6 +1014,74 @@ static int sob_iterate_once(atus_ctx *ctx, double *res_out, double *N_out) {
   return ATUS_OK;
 }
 
+// One iteration of sob_iterate_once with every scalar in device memory:
+// the same kernels and reductions in the same order; psi changes only in an
+// active iteration (not yet converged, below max_iter).
+static int sob_iterate_dev(atus_ctx *ctx) {
+  const int n = ctx->ncomp;
+  const int blocks = grid_blocks(ctx->npts, 256);
+  SobDev *d = (SobDev *)ctx->sob_dev;
+  for (int i = 0; i < n; i++) {
+    CK(cudaMemcpyAsync(ctx->sob_psi[i], ctx->psi[i], 16 * ctx->npts, cudaMemcpyDeviceToDevice, ctx->stream));
+    RUN(sob_filter(ctx, ctx->sob_psi[i], FILT_SOBOLEV, ctx->sob_alpha[i]));
+  }
+  RUN(sob_laplace(ctx));
+  for (int i = 0; i < n; i++) {
+    SobArgs a;
+    memset(&a, 0, sizeof(a));
+    for (int j = 0; j < MAXC; j++) a.psi[j] = (const double2 *)ctx->psi[j];
+    a.lap = (const double2 *)ctx->sob_lap[i];
+    a.V = ctx->V[i];
+    a.grad = (double2 *)ctx->sob_grad[i];
+    a.comp = i;
+    a.ncomp = n;
+    for (int k = 0; k < MAXC * MAXC; k++) a.gs[k] = ctx->gs[k];
+    a.npts = ctx->npts;
+    sob_assemble_kernel<<<blocks, 256, 0, ctx->stream>>>(a);
+    LAUNCHED(ctx);
+    RUN(sob_filter(ctx, ctx->sob_grad[i], FILT_SOBOLEV, ctx->sob_alpha[i]));
+  }
+  for (int i = 0; i < n; i++) {
+    RedArgs r;
+    memset(&r, 0, sizeof(r));
+    r.mode = RED_DOT2;
+    r.nq = 2;
+    r.a = ctx->psi[i];
+    r.b = ctx->sob_grad[i];
+    r.c = ctx->sob_psi[i];
+    RUN(reduce_dev(ctx, r, d->q[i]));
+    sob_proj_kernel<<<blocks, 256, 0, ctx->stream>>>((double2 *)ctx->sob_grad[i], (const double2 *)ctx->sob_psi[i], d,
+                                                    i, ctx->npts);
+    LAUNCHED(ctx);
+  }
+  for (int i = 0; i < n; i++) {
+    RedArgs r;
+    memset(&r, 0, sizeof(r));
+    r.mode = RED_NORM;
+    r.nq = 1;
+    r.a = ctx->sob_grad[i];
+    RUN(reduce_dev(ctx, r, &d->g2[i]));
+  }
+  for (int i = 0; i < n; i++) {
+    RedArgs r;
+    memset(&r, 0, sizeof(r));
+    r.mode = RED_NORM;
+    r.nq = 1;
+    r.a = ctx->psi[i];
+    RUN(reduce_dev(ctx, r, &d->n[i]));
+  }
+  sob_scalars_kernel<<<1, 1, 0, ctx->stream>>>(d, ctx->ar, n);
+  LAUNCHED(ctx);
+  for (int i = 0; i < n; i++) {
+    sob_update_kernel<<<blocks, 256, 0, ctx->stream>>>((double2 *)ctx->psi[i], (const double2 *)ctx->sob_grad[i],
+                                                      ctx->stepsize, d, i, ctx->npts);
+    LAUNCHED(ctx);
+  }
+  sob_commit_kernel<<<1, 1, 0, ctx->stream>>>(d);
+  LAUNCHED(ctx);
+  return ATUS_OK;
+}
+
 int atus_sob_init(atus_ctx *ctx, const double *alpha, double stepsize) {
   if (!ctx || !alpha) return ATUS_E_ARG;
   if (ctx->prec != ATUS_PREC_FP64) return fail(ctx, ATUS_E_UNSUPPORTED, "the Sobolev descent runs in FP64");
@@ -1021,17 +1110,51 @@ int atus_sob_iterate(atus_ctx *ctx, int n_iter, double *res, double *N) {
   return ATUS_OK;
 }
 
+// Iterations until the residual is <= epsilon (the reference's run loop, the
+// update of the converging iteration included) or max_iter.  The first
+// iteration runs directly, the rest as a CUDA graph of SOB_CHUNK device-side
+// iterations; the host reads the device scalars once per chunk.
+constexpr int SOB_CHUNK = 64;
+
 int atus_sob_run(atus_ctx *ctx, double epsilon, int max_iter, int *iters, double *res) {
   if (!ctx || !ctx->sob_ready) return ctx ? fail(ctx, ATUS_E_STATE, "atus_sob_init first") : ATUS_E_ARG;
+  if (max_iter < 1) return fail(ctx, ATUS_E_ARG, "max_iter < 1");
   RUN(sob_renorm(ctx));
-  int it = 0;
-  double r = 0;
-  do {
-    RUN(sob_iterate_once(ctx, &r, nullptr));
-    it++;
-  } while (r > epsilon && it < max_iter);
-  if (iters) *iters = it;
-  if (res) *res = r;
+  if (!ctx->sob_dev) CK(cudaMalloc(&ctx->sob_dev, sizeof(SobDev)));
+  SobDev h;
+  memset(&h, 0, sizeof(h));
+  h.eps = epsilon;
+  h.max_iter = max_iter;
+  CK(cudaMemcpyAsync(ctx->sob_dev, &h, sizeof(SobDev), cudaMemcpyHostToDevice, ctx->stream));
+  RUN(sob_iterate_dev(ctx));  // eager: kernel attributes are set outside any capture
+  if (ctx->sob_graph && ctx->sob_graph_step != ctx->stepsize) {
+    cudaGraphExecDestroy(ctx->sob_graph);
+    ctx->sob_graph = nullptr;
+  }
+  if (!ctx->sob_graph) {
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    int r = ATUS_OK;
+    for (int k = 0; k < SOB_CHUNK && r == ATUS_OK; k++) r = sob_iterate_dev(ctx);
+    const cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    if (r != ATUS_OK || e != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      return r != ATUS_OK ? r : cuda_check(ctx, e, "Sobolev graph capture");
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&ctx->sob_graph, g, 0);
+    cudaGraphDestroy(g);
+    CK(ie);
+    ctx->sob_graph_step = ctx->stepsize;
+  }
+  SobDev *hd = reinterpret_cast<SobDev *>(ctx->h_sob);
+  for (;;) {
+    CK(cudaMemcpyAsync(hd, ctx->sob_dev, sizeof(SobDev), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (hd->done || hd->iters >= max_iter) break;
+    CK(cudaGraphLaunch(ctx->sob_graph, ctx->stream));
+  }
+  if (iters) *iters = hd->iters;
+  if (res) *res = hd->res;
   return ATUS_OK;
 }
 

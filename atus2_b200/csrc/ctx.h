@@ -44,6 +44,10 @@ struct atus_ctx {
   void *sob_lap[MAXC] = {}, *sob_psi[MAXC] = {}, *sob_grad[MAXC] = {};
   double sob_alpha[MAXC] = {};
   double stepsize = 0;
+  void *sob_dev = nullptr;              // SobDev in device memory
+  cudaGraphExec_t sob_graph = nullptr;  // a chunk of device-side iterations
+  double sob_graph_step = 0;            // stepsize the graph was captured with
+  void *h_sob = nullptr;                // pinned host copy of the SobDev
 };
 
 // ------------------------------------------------------------------ errors

@@ -384,3 +384,37 @@ def test_stable_bragg_form():
     s.block(50, KIND_BRAGG_AD, Laser.make(**kw), np.full(50, 1e-200))
     n1 = s.particle_number(0) + s.particle_number(1)
     assert np.isfinite(n1) and abs(n1 - n0) < 1e-12
+
+
+def test_sob_run_on_device_matches_host_loop():
+    """atus_sob_run (device-side scalars, graph chunks) stops at the same
+    iteration with the same state as the host loop over atus_sob_iterate."""
+    h = _grid(3, [32, 32, 16], 12.0)
+    x, y, z = _coords(h)
+    V = 0.5 * (x * x + 4 * y * y + 2.25 * z * z)
+    guess = np.sqrt(np.maximum(0.0, 3.0 - V)).astype(np.complex128) + 1e-3
+    eps = 2e-4
+    runs = []
+    for mode in ("host", "device"):
+        s = Solver(h, 1, PREC_FP64)
+        s.set_psi(0, guess)
+        s.set_potential(0, V)
+        s.set_gs([50.0])
+        s.sob_init([0.5], 0.01)
+        if mode == "host":
+            s.sob_renormalize()
+            it = 0
+            while True:
+                r, _ = s.sob_iterate()
+                it += 1
+                if r <= eps or it >= 5000:
+                    break
+        else:
+            it, r = s.sob_run(eps, 5000)
+        runs.append((it, r, s.psi(0)))
+    assert runs[0][0] == runs[1][0] and runs[0][0] > 70  # more than one graph chunk
+    # rounding-level differences (the fused renormalise-and-update kernel and
+    # the device-side sum of squares contract multiply-adds differently); the
+    # residual, a squared norm of a small gradient, amplifies them
+    assert abs(runs[0][1] - runs[1][1]) <= 1e-12 * runs[0][1]
+    assert rel_l2(runs[1][2], runs[0][2]) < 1e-13
