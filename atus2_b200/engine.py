@@ -109,6 +109,11 @@ SIGNATURES = {
     "atus_particle_number": (_i, [_vp, _i, _dp]),
     "atus_set_bragg_stable": (_i, [_vp, _i]),
     "atus_particle_number_noalloc": (_i, [_vp, C.c_int64, _i, C.c_double, _vp, _vp]),
+    "atus_guess_init": (_i, [C.c_uint64, _dp]),
+    "atus_guess_grad": (_i, [_dp, _dp, _dp, _i, _dp, _dp]),
+    "atus_guess_train": (_i, [_dp, _dp, _dp, _i, _i, _d, _dp]),
+    "atus_guess_predict": (_i, [_dp, _dp, _i, _dp]),
+    "atus_guess_decode": (_i, [_vp, _i, _dp, _dp]),
     "atus_batch_create": (_i, [C.POINTER(BatchInstance), _i, _i, _d, C.POINTER(C.c_void_p)]),
     "atus_batch_destroy": (None, [_vp]),
     "atus_batch_last_error": (C.c_char_p, [_vp]),
@@ -355,6 +360,12 @@ class Solver:
         res = C.c_double()
         self._ok(self._L.atus_sob_run(self._c, float(epsilon), int(max_iter), C.byref(it), C.byref(res)), "sob_run")
         return it.value, res.value
+
+    def guess_decode(self, comp: int, coef, scale) -> None:
+        """Fill component comp with the Hermite expansion coef (64) at basis lengths scale (3)."""
+        c = np.ascontiguousarray(coef, dtype=np.float64)
+        sc = np.ascontiguousarray(scale, dtype=np.float64)
+        self._ok(self._L.atus_guess_decode(self._c, comp, _dptr(c), _dptr(sc)), "guess_decode")
 
     def sob_mu(self) -> np.ndarray:
         mu = np.zeros(MAX_COMP)

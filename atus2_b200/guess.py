@@ -1,0 +1,235 @@
+"""Learned initial guess for the Sobolev ground-state solver (sobmin).
+
+Problem family: 3D grid on [-16, 16)^3, V = (x^2 + w_y^2 y^2 + w_z^2 z^2) / 2,
+one component, N = 1, alpha = 1/2, interaction g; draws w_y, w_z ~ U[0.5, 4],
+g ~ log-uniform on [10, 2000].
+
+The guess of a draw is the Hermite expansion
+
+    psi(x, y, z) = sum_{a,b,c in {0,2,4,6}} C[a/2, b/2, c/2] phi_a(x/lx) phi_b(y/ly) phi_c(z/lz)
+
+(phi_n the orthonormal Hermite functions, divided by sqrt(l)), with basis
+lengths l from the draw itself -- l^2 = 1/w + (R/3)^2, the oscillator length
+and a third of the Thomas-Fermi radius R = sqrt(2 mu_TF)/w -- and the 64
+coefficients C predicted by an MLP from (w_y, w_z, log g) scaled to O(1).
+The network trains (atus_guess_train, hand-written CUDA kernels) on the
+coefficients of ground states that plain sobmin itself computed: the
+projections of each converged state on the basis.  Plain sobmin from the
+Thomas-Fermi guess stays the fallback; the converged residual and chemical
+potential judge the learned guess.
+
+    python -m atus2_b200.guess generate --count 256 --out atus2_b200/data/sob_train_64.npz
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import concurrent.futures as cf
+import math
+import os
+import time
+
+import numpy as np
+
+from . import binfmt
+from .engine import PREC_FP64, Solver, load_library
+
+NIN, NOUT, NPARAM = 3, 64, 8576
+L_BOX = 32.0
+STEP = 4e-4       # fixed Sobolev step: stable for the largest corner potential of the family
+EPS = 1e-10       # residual target (the reference's squared-norm residual)
+ALPHA = 0.5
+HERE = os.path.dirname(os.path.abspath(__file__))
+TRAIN_FILE = os.path.join(HERE, "data", "sob_train_64.npz")
+
+
+def header(n: int):
+    return binfmt.make_header(3, [n] * 3, [-L_BOX / 2] * 3, [L_BOX / 2] * 3)
+
+
+def draw(count: int, seed: int):
+    rng = np.random.default_rng(seed)
+    wy = rng.uniform(0.5, 4.0, count)
+    wz = rng.uniform(0.5, 4.0, count)
+    g = np.exp(rng.uniform(math.log(10.0), math.log(2000.0), count))
+    return np.stack([wy, wz, g], axis=1)
+
+
+def features(p) -> np.ndarray:
+    p = np.atleast_2d(np.asarray(p, dtype=np.float64))
+    c = 0.5 * (math.log(10.0) + math.log(2000.0))
+    h = 0.5 * (math.log(2000.0) - math.log(10.0))
+    return np.stack([(p[:, 0] - 2.25) / 1.75, (p[:, 1] - 2.25) / 1.75, (np.log(p[:, 2]) - c) / h], axis=1)
+
+
+def mu_tf(wy: float, wz: float, g: float) -> float:
+    """Thomas-Fermi chemical potential of N = 1 in the trap (1, wy, wz):
+    N = (8 pi / 15) (2 mu)^{3/2} mu / (g wx wy wz)."""
+    return (15.0 * g * wy * wz / (8.0 * math.pi * 2.0 * math.sqrt(2.0))) ** 0.4
+
+
+def scales(wy: float, wz: float, g: float) -> np.ndarray:
+    mu = mu_tf(wy, wz, g)
+    w = np.array([1.0, wy, wz])
+    R = np.sqrt(2.0 * mu) / w
+    return np.sqrt(1.0 / w + (R / 3.0) ** 2)
+
+
+def hermite_rows(n: int, dx: float, l: float) -> np.ndarray:
+    """phi_n(x/l)/sqrt(l), n = 0, 2, 4, 6, at x_i = (i - n/2) dx: shape (4, n)."""
+    x = (np.arange(n) - n // 2) * dx
+    u = x / l
+    out = np.zeros((4, n))
+    pm, pc = np.zeros(n), math.pi ** -0.25 / math.sqrt(l) * np.exp(-0.5 * u * u)
+    for q in range(7):
+        if q % 2 == 0:
+            out[q // 2] = pc
+        pn = math.sqrt(2.0 / (q + 1)) * u * pc - math.sqrt(q / (q + 1)) * pm
+        pm, pc = pc, pn
+    return out
+
+
+def project(psi: np.ndarray, h, sc) -> np.ndarray:
+    """Least-squares coefficients of psi (real part) on the basis sampled on
+    the grid: the separable normal equations, one 4 x 4 Gram matrix per axis
+    (the sampled functions are orthonormal only on fine grids)."""
+    n = psi.shape
+    B = [hermite_rows(n[a], float(h[f"d{'xyz'[a]}"]), sc[a]) for a in range(3)]
+    r = np.einsum("ijk,ai,bj,ck->abc", psi.real, B[0], B[1], B[2])
+    Gi = [np.linalg.inv(b @ b.T) for b in B]
+    return np.einsum("abc,pa,qb,rc->pqr", r, Gi[0], Gi[1], Gi[2]).ravel()
+
+
+def decode(coef, h, sc) -> np.ndarray:
+    n = [int(h[f"nDim{a}"]) for a in "XYZ"]
+    B = [hermite_rows(n[a], float(h[f"d{'xyz'[a]}"]), sc[a]) for a in range(3)]
+    return np.einsum("abc,ai,bj,ck->ijk", np.asarray(coef).reshape(4, 4, 4), B[0], B[1], B[2])
+
+
+def potential(h, wy, wz):
+    x, y, z = np.meshgrid(*[binfmt.x_coords(h, a) for a in range(3)], indexing="ij")
+    return 0.5 * (x * x + wy * wy * y * y + wz * wz * z * z)
+
+
+def tf_guess(h, V, g):
+    """sqrt(max(0, (mu - V)/g)) with mu set by N = 1 on the grid (bisection)."""
+    dv = float(h["dx"] * h["dy"] * h["dz"])
+    lo, hi = 0.0, float(V.max()) + 1e3 * g
+    for _ in range(200):
+        mu = 0.5 * (lo + hi)
+        if np.sum(np.maximum(0.0, mu - V)) / g * dv > 1.0:
+            hi = mu
+        else:
+            lo = mu
+    return np.sqrt(np.maximum(0.0, (mu - V) / g)).astype(np.complex128)
+
+
+def solve(n, wy, wz, g, coef=None, eps=EPS, max_iter=200000):
+    """Plain sobmin from the Thomas-Fermi guess (coef None) or from the
+    learned guess; returns (psi, iterations, residual, seconds, mu)."""
+    h = header(n)
+    V = potential(h, wy, wz)
+    s = Solver(h, 1, PREC_FP64)
+    if coef is None:
+        s.set_psi(0, tf_guess(h, V, g))
+    else:
+        s.guess_decode(0, coef, scales(wy, wz, g))
+    s.set_potential(0, V)
+    s.set_gs([g])
+    s.sob_init([ALPHA], STEP)
+    s.synchronize()
+    t0 = time.perf_counter()
+    it, res = s.sob_run(eps, max_iter)
+    s.synchronize()
+    dt = time.perf_counter() - t0
+    mu = float(s.sob_mu()[0])
+    psi = s.psi(0)
+    s.close()
+    return psi, it, res, dt, mu
+
+
+def generate(count: int, seed: int, n: int = 64, workers: int = 8):
+    """Training set: plain-sobmin ground states of `count` draws at n^3,
+    projected on their bases."""
+    P = draw(count, seed)
+
+    def one(k):
+        wy, wz, g = P[k]
+        psi, it, res, dt, mu = solve(n, wy, wz, g)
+        return project(psi, header(n), scales(wy, wz, g)), it, res, mu
+
+    with cf.ThreadPoolExecutor(workers) as ex:
+        out = list(ex.map(one, range(count)))
+    coef = np.stack([o[0] for o in out])
+    return dict(params=P, coef=coef, iters=np.array([o[1] for o in out]), res=np.array([o[2] for o in out]),
+                mu=np.array([o[3] for o in out]), n=n, seed=seed, step=STEP, eps=EPS)
+
+
+# ------------------------------------------------------------------ network (C ABI)
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def init_params(seed: int) -> np.ndarray:
+    p = np.zeros(NPARAM)
+    _check(load_library().atus_guess_init(C.c_uint64(seed), _dp(p)), "guess_init")
+    return p
+
+
+def _check(r, what):
+    if r != 0:
+        raise RuntimeError(f"{what} failed: {r}")
+
+
+def grad(params, X, Y):
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    Y = np.ascontiguousarray(Y, dtype=np.float64)
+    p = np.ascontiguousarray(params, dtype=np.float64)
+    g = np.zeros(NPARAM)
+    loss = np.zeros(1)
+    _check(load_library().atus_guess_grad(_dp(p), _dp(X), _dp(Y), len(X), _dp(loss), _dp(g)), "guess_grad")
+    return float(loss[0]), g
+
+
+def train(X, Y, epochs=20000, lr=2e-3, seed=0, params=None):
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    Y = np.ascontiguousarray(Y, dtype=np.float64)
+    p = init_params(seed) if params is None else np.array(params, dtype=np.float64)
+    hist = np.zeros(epochs)
+    _check(load_library().atus_guess_train(_dp(p), _dp(X), _dp(Y), len(X), int(epochs), float(lr), _dp(hist)),
+           "guess_train")
+    return p, hist
+
+
+def predict(params, X):
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    p = np.ascontiguousarray(params, dtype=np.float64)
+    out = np.zeros((len(X), NOUT))
+    _check(load_library().atus_guess_predict(_dp(p), _dp(X), len(X), _dp(out)), "guess_predict")
+    return out
+
+
+# Coefficients are trained in units of their spread over the training set.
+def coef_stats(coef):
+    return coef.mean(axis=0), coef.std(axis=0) + 1e-12
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("cmd", choices=["generate"])
+    ap.add_argument("--count", type=int, default=256)
+    ap.add_argument("--seed", type=int, default=7)
+    ap.add_argument("--n", type=int, default=64)
+    ap.add_argument("--workers", type=int, default=8)
+    ap.add_argument("--out", default=TRAIN_FILE)
+    a = ap.parse_args()
+    t0 = time.perf_counter()
+    d = generate(a.count, a.seed, a.n, a.workers)
+    os.makedirs(os.path.dirname(a.out), exist_ok=True)
+    np.savez_compressed(a.out, **d)
+    print(f"{a.count} ground states at {a.n}^3 in {time.perf_counter() - t0:.1f} s; "
+          f"iterations {d['iters'].min()}..{d['iters'].max()}; residuals <= {d['res'].max():.2e}")
+
+
+if __name__ == "__main__":
+    main()

@@ -384,6 +384,9 @@ def atus_arm(args, rank, ws, local, dist):
     if not args.no_batch:
         barrier(dist)
         out["variants"]["batch"] = run_batch()
+    if not args.no_sobmin:
+        barrier(dist)
+        out["variants"]["sobmin"] = run_sobmin(no_cpu=args.no_cpu_baseline or rank != 0)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = run_cpu_baseline()
     barrier(dist)
@@ -513,6 +516,81 @@ def run_batch(stream_unused=None):
     }
 
 
+# ------------------------------------------------------------------ sobmin (ground state)
+SOB_N, SOB_HELD_OUT, SOB_SEED = 128, 6, 2
+
+
+def run_sobmin(no_cpu=False):
+    """Ground states by the Sobolev descent at 128^3 on [-16,16)^3 (trap
+    (1, w_y, w_z), w ~ U[0.5, 4], g ~ logU[10, 2000], N = 1, alpha = 1/2,
+    fixed step 4e-4), residual 1e-10: plain sobmin from the Thomas-Fermi guess
+    against the learned guess, on SOB_HELD_OUT draws from seed 2.  The network
+    is trained here, on the GPU with the project's kernels, from the committed
+    training set (plain-sobmin ground states at 64^3, atus2_b200/data).  The
+    best 64-mode start (the converged state projected on the basis) bounds
+    what this decoder can gain."""
+    from atus2_b200 import guess
+
+    if not os.path.exists(guess.TRAIN_FILE):
+        return {"unavailable": "training set atus2_b200/data/sob_train_64.npz not generated"}
+    d = np.load(guess.TRAIN_FILE)
+    m, sd = guess.coef_stats(d["coef"])
+    t0 = time.perf_counter()
+    params, hist = guess.train(guess.features(d["params"]), (d["coef"] - m) / sd, epochs=20000, lr=2e-3)
+    t_train = time.perf_counter() - t0
+    H = guess.draw(SOB_HELD_OUT, SOB_SEED)
+    pred = guess.predict(params, guess.features(H)) * sd + m
+    rows = []
+    for k, (wy, wz, g) in enumerate(H):
+        psi, it_tf, res_tf, t_tf, mu_tf = guess.solve(SOB_N, wy, wz, g)
+        best = guess.project(psi, guess.header(SOB_N), guess.scales(wy, wz, g))
+        _, it_nn, res_nn, t_nn, mu_nn = guess.solve(SOB_N, wy, wz, g, coef=pred[k])
+        _, it_bs, _, t_bs, mu_bs = guess.solve(SOB_N, wy, wz, g, coef=best)
+        rows.append(dict(w_y=float(wy), w_z=float(wz), g=float(g), iters_tf=int(it_tf), s_tf=t_tf, mu_tf=mu_tf,
+                         iters_learned=int(it_nn), s_learned=t_nn, mu_learned=mu_nn, dmu=abs(mu_nn - mu_tf),
+                         res_learned=res_nn, iters_best64=int(it_bs), s_best64=t_bs))
+    t_tf = float(np.mean([r["s_tf"] for r in rows]))
+    t_nn = float(np.mean([r["s_learned"] for r in rows]))
+    out = {
+        "metric": "sobmin time-to-1e-10 (128^3, FP64)",
+        "value": t_tf,
+        "unit": "s",
+        "iterations_mean": float(np.mean([r["iters_tf"] for r in rows])),
+        "learned_guess": {"value": t_nn, "unit": "s", "speedup": t_tf / t_nn,
+                          "iterations_mean": float(np.mean([r["iters_learned"] for r in rows])),
+                          "max_abs_dmu": float(max(r["dmu"] for r in rows))},
+        "best_64_mode_start": {"s": float(np.mean([r["s_best64"] for r in rows])),
+                               "iterations_mean": float(np.mean([r["iters_best64"] for r in rows]))},
+        "training": {"draws": int(len(d["params"])), "grid": int(d["n"]), "seconds": t_train,
+                     "loss_first_last": [float(hist[0]), float(hist[-1])], "epochs": len(hist)},
+        "held_out": rows,
+        "step": guess.STEP,
+    }
+    if not no_cpu:
+        # the oracle port's iteration at 128^3 on all host cores, times the GPU's iteration count
+        from oracle.oracle import Oracle
+
+        wy, wz, g = H[0]
+        h = guess.header(SOB_N)
+        V = guess.potential(h, wy, wz)
+        cores = os.cpu_count() or 1
+        o = Oracle(h, 1, threads=cores)
+        o.set_psi(0, guess.tf_guess(h, V, g))
+        o.set_potential(0, V)
+        o.set_gs([g])
+        o.sob_init([guess.ALPHA], guess.STEP)
+        o.sob_renormalize()
+        o.sob_iterate()
+        t0 = time.perf_counter()
+        for _ in range(5):
+            o.sob_iterate()
+        per_it = (time.perf_counter() - t0) / 5
+        out["cpu_baseline"] = {"value": per_it * out["iterations_mean"], "unit": "s", "cores": cores, "kind": "port",
+                               "sample": f"5 Sobolev iterations of the oracle restatement at 128^3 on {cores} threads, "
+                                         "times the mean plain iteration count"}
+    return out
+
+
 # ------------------------------------------------------------------ reference arm
 def reference_arm(args, rank, ws, dist):
     if rank != 0:
@@ -553,6 +631,7 @@ def main():
     ap.add_argument("--impl", default="atus", choices=["atus", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-sweep variant")
+    ap.add_argument("--no-sobmin", action="store_true", help="skip the ground-state variant")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, ws, local, dist = dist_init()

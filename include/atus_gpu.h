@@ -42,6 +42,10 @@
  *   atus_sob_*                      CSOB_Base (include/CSOB_Base.h:96-543)
  *   atus_particle_number_noalloc    no counterpart in the reference (see its
  *                                   declaration below)
+ *   atus_guess_*                    no counterpart in the reference: a learned
+ *                                   initial state for CSOB_Base::run (the
+ *                                   reference starts from a muParser guess,
+ *                                   sob_solver.cpp:117-137)
  *   atus_batch_*                    many bragg runs at once: per instance the
  *                                   Strang loop of CRT_Base_IF::run_sequence
  *                                   (CRT_Base_IF.h:779-789) with the bragg_ad
@@ -211,6 +215,31 @@ ATUS_API int atus_sob_iterate(atus_ctx *ctx, int n_iter, double *res, double *N)
 ATUS_API int atus_sob_run(atus_ctx *ctx, double epsilon, int max_iter, int *iters, double *res);
 /* mu_i = m_ar * sum[-Re(psi* Lap psi) + (V + sum_j g_ij |psi_j|^2) |psi_i|^2] */
 ATUS_API int atus_sob_mu(atus_ctx *ctx, double *mu /* ncomp */);
+
+/* ------------------------------------------------------------ learned guess
+ * A small MLP (3 inputs, two tanh layers of 64, 64 linear outputs) maps the
+ * scaled parameters of a ground-state problem to the coefficients of the
+ * state in the 64 products phi_a(x/lx) phi_b(y/ly) phi_c(z/lz) of even
+ * Hermite functions (a, b, c in {0, 2, 4, 6}; coefficient 16 a' + 4 b' + c'
+ * with a' = a/2 ...).  Training and inference run in hand-written FP64
+ * kernels.  Parameter vector: W1[64][3], b1[64], W2[64][64], b2[64],
+ * W3[64][64], b3[64]. */
+#define ATUS_GUESS_NIN 3
+#define ATUS_GUESS_NOUT 64
+#define ATUS_GUESS_NPARAM 8576
+/* Glorot-uniform weights, zero biases, from a seeded splitmix64 stream. */
+ATUS_API int atus_guess_init(uint64_t seed, double *params);
+/* Mean squared error over B samples (X: B x 3, Y: B x 64) and its gradient. */
+ATUS_API int atus_guess_grad(const double *params, const double *X, const double *Y, int B, double *loss,
+                             double *grad);
+/* Full-batch Adam (beta 0.9 / 0.999) for `epochs` steps; params updated in
+ * place; loss_history (may be NULL) gets the loss before each step. */
+ATUS_API int atus_guess_train(double *params, const double *X, const double *Y, int B, int epochs, double lr,
+                              double *loss_history);
+ATUS_API int atus_guess_predict(const double *params, const double *X, int B, double *coef /* B x 64 */);
+/* Writes sum coef * phi phi phi (real) into component comp of a 3D FP64
+ * context; scale = the three basis lengths (lx, ly, lz). */
+ATUS_API int atus_guess_decode(atus_ctx *ctx, int comp, const double *coef, const double *scale);
 
 /* ------------------------------------------------------------ batched sweep
  * Independent two-component bragg_ad instances (1D lengths 1024..16384, square
