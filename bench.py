@@ -302,12 +302,24 @@ def run_cpu_baseline(n_steps_sample=(1, 3)):
     }
 
 
-def roofline(s, kind, peak, peak_kind):
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
+# FP64 kernels, from one ncu capture each (profiles/pipe_kernel_fp64_bragg256.md,
+# profiles/pass2_kinetic_fp64_bragg256.md).
+NCU_TRAFFIC_FP64 = {"pipe_kernel": 1.0204e9, "pass2_kernel M2_KIN": 1.0142e9}
+
+
+def roofline(s, kind, peak, peak_kind, fp64=True):
     prof = s.profile_passes(kind, reps=5)
+    # pass names in atus_profile_passes order: x kinetic pass, then the
+    # real-space half step (one plane-pipeline launch, or three axis passes)
+    names = (["pass2_kernel M2_KIN", "pipe_kernel"] if len(prof) == 2 else
+             ["pass2_kernel M2_KIN", "pass2_kernel M2_INV (y)", "pass2_kernel M2_NL (z)", "pass2_kernel M2_FWD (y)"])
     # dominant pass: largest device time per Strang step
-    best = max(prof, key=lambda p: p[0] * p[1])
-    ms, lps, by = best
+    bi = max(range(len(prof)), key=lambda q: prof[q][0] * prof[q][1])
+    ms, lps, by = prof[bi]
     achieved = by / (ms * 1e-3) / 1e9
+    name = names[bi] if bi < len(names) else f"pass {bi}"
+    traffic = NCU_TRAFFIC_FP64.get(name) if fp64 else None
     return {
         "bound": "hbm",
         "achieved": achieved,
@@ -315,9 +327,11 @@ def roofline(s, kind, peak, peak_kind):
         "unit": "GB/s",
         "frac": achieved / peak,
         "peak_source": peak_kind,
-        "traffic": None,
-        "kernel": "pass_kernel (see profiles/)",
-        "passes": [{"ms": p[0], "launches_per_step": p[1], "bytes": p[2], "GBps": p[2] / (p[0] * 1e-3) / 1e9} for p in prof],
+        "traffic": traffic,
+        "kernel": name,
+        "algorithmic_bytes_per_launch": by,
+        "passes": [{"kernel": names[q] if q < len(names) else f"pass {q}", "ms": p[0], "launches_per_step": p[1],
+                    "bytes": p[2], "GBps": p[2] / (p[0] * 1e-3) / 1e9} for q, p in enumerate(prof)],
     }
 
 
@@ -371,7 +385,7 @@ def atus_arm(args, rank, ws, local, dist):
     out["variants"] = {"mixed": {"value": ws * npts * args.steps / (msm * 1e-3), "ms_per_step": msm / args.steps,
                                  "dtype": "c64 fields, f64 phase arguments", "speedup_vs_fp64": ms / msm}}
     if rank == 0:
-        out["variants"]["mixed"]["roofline"] = roofline(sm, STEP_BRAGG_AD, peak, peak_kind)
+        out["variants"]["mixed"]["roofline"] = roofline(sm, STEP_BRAGG_AD, peak, peak_kind, fp64=False)
     sm.close()
     # end-to-end through the C ABI with host buffers
     barrier(dist)
