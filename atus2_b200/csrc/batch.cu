@@ -29,6 +29,7 @@ bool batch2d_p2_info_f(int N, int mode, BKernel *k);
 bool batch2d_p2_info_d(int N, int mode, BKernel *k);
 bool batch2d_tile_info_f(int N, int mode, BKernel *k);
 bool batch2d_tile_info_d(int N, int mode, BKernel *k);
+bool batch2d_p5_info_f(int N, int mode, BKernel *k);
 
 namespace {
 
@@ -111,6 +112,7 @@ bool info1d(const atus_batch *b, int N, const Variant &v, BKernel *k) {
 bool info2d(const atus_batch *b, int N, int variant, int mode, BKernel *k) {
   if (variant == BV_P2)
     return b->prec == ATUS_PREC_FP64 ? batch2d_p2_info_d(N, mode, k) : batch2d_p2_info_f(N, mode, k);
+  if (variant == BV_P5) return b->prec == ATUS_PREC_FP64 ? false : batch2d_p5_info_f(N, mode, k);
   return b->prec == ATUS_PREC_FP64 ? batch2d_tile_info_d(N, mode, k) : batch2d_tile_info_f(N, mode, k);
 }
 
@@ -276,7 +278,7 @@ void drop_graphs(atus_batch *b) {
 std::string variant_name(const Class &c, const Variant &v) {
   char buf[64];
   if (c.dim == 1) snprintf(buf, sizeof(buf), "%d threads, %d resident", v.a, v.b);
-  else snprintf(buf, sizeof(buf), "%s", v.a == BV_P2 ? "register-staged passes" : "shared-memory tile passes");
+  else snprintf(buf, sizeof(buf), "%s", v.a == BV_P2 ? "register-staged passes" : v.a == BV_P5 ? "register-staged 512-point passes" : "shared-memory tile passes");
   return buf;
 }
 
@@ -420,7 +422,7 @@ int atus_batch_create(const atus_batch_instance *inst, int count, int precision,
           if (info1d(b, c.n, v, &k)) c.cands.push_back(v);
         }
     } else {
-      for (int var : {BV_P2, BV_TILE}) {
+      for (int var : {BV_P2, BV_P5, BV_TILE}) {
         Variant v;
         v.a = var;
         if (info2d(b, c.n, var, M2_NL, &k)) c.cands.push_back(v);

@@ -15,6 +15,7 @@
 //   size class; the tile of work item w belongs to instance w / tiles.
 #pragma once
 #include "pass2.cuh"
+#include "pass512.cuh"
 
 namespace atus {
 
@@ -239,6 +240,27 @@ __global__ void __launch_bounds__(Tile2<R>::NT, Tile2<R>::MINB) batch_pass2_kern
   }
 }
 
+// 512-point register-staged variant (complex64 fields).
+template <typename R, int TC, int MODE, bool STRIDED>
+__global__ void __launch_bounds__(P5Cfg<R, TC>::NT, 4) batch_pass512_kernel(BPass bp) {
+  using Cfg = P5Cfg<R, TC>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double s_om[Cfg::B], s_ec[Cfg::B], s_es[Cfg::B];
+  __shared__ __align__(16) PassArgs sa;
+  bool setup = false;
+  const int64_t W = bp.items * bp.ninst;
+  for (int64_t w = blockIdx.x; w < W; w += gridDim.x) {
+    const int inst = (int)(w / bp.items);
+    bpass_args(bp, inst, &sa);
+    if (!setup) {
+      p5_setup<R, TC>(sa, smem_raw);
+      setup = true;
+    }
+    p5_item<R, TC, MODE, STRIDED, false>(sa, tile_geo<Cfg::B, 512>(sa, w % bp.items), smem_raw, s_om, s_ec, s_es);
+    __syncthreads();
+  }
+}
+
 // Tile variant (any pencil length): the whole tile is loaded into shared
 // memory and transformed with fft_tile (radix-16 Stockham passes), then the
 // operator and the second transform, as pass_kernel without the prefetch.
@@ -377,6 +399,8 @@ struct BKernel {
   size_t smem;
   int B;
 };
-enum { BV_P2 = 0, BV_TILE = 1 };  // 2D variants: register-staged passes, shared-memory tile passes
+// 2D variants: register-staged passes (32..256 points), shared-memory tile
+// passes, register-staged 512-point passes (complex64)
+enum { BV_P2 = 0, BV_TILE = 1, BV_P5 = 2 };
 
 }  // namespace atus

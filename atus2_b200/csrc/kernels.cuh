@@ -152,6 +152,11 @@ template <> __device__ __forceinline__ double2 expi<double>(double phi) {
   return make_double2(c, s);
 }
 template <> __device__ __forceinline__ double2 expi<float>(double phi) {
+  if (fabs(phi) <= 0.03125) {  // the usual phase of one time step: FP64 Taylor, |e| = 1 to FP64
+    double sd, cd;
+    sincos_step(phi, &sd, &cd);
+    return make_double2(cd, sd);
+  }
   float s, c;
   sincosf((float)reduce_2pi(phi), &s, &c);
   const double cd = c, sd = s;
@@ -245,7 +250,18 @@ __device__ __forceinline__ void nl_point(const NLArgs &a, cplx<R> *v, int64_t l,
     const double r = sqrt(d * d + Omega * Omega);
     const double2 e = expi<R>(-dt * m);   // e^{-i dt m}
     const double2 rr = expi<R>(dt * r);   // (cos r dt, sin r dt)
-    const double sor = (r > 0.0) ? rr.y / r : dt;
+    // sin(r dt) / r: Taylor series of sinc (truncation below 2^-72 for r dt <= 1/32)
+    const double xr = dt * r;
+    double sor;
+    if (xr <= 0.03125) {
+      const double x2 = xr * xr;
+      double p = fma(x2, 1.0 / 362880.0, -1.0 / 5040.0);
+      p = fma(p, x2, 1.0 / 120.0);
+      p = fma(p, x2, -1.0 / 6.0);
+      sor = dt * fma(p, x2, 1.0);
+    } else {
+      sor = rr.y / r;
+    }
     const double fd = sor * d, fw = sor * Omega;
     // U11 = e(cos - i fd), U22 = e(cos + i fd), Uoff = e(-i fw)
     const double2 U11 = cmul(e, make_double2(rr.x, -fd));

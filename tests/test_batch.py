@@ -112,3 +112,18 @@ def test_batch_mixed_tuned_matches_oracle():
     assert "probe ms" in sched
     b.run(30)
     _check(b, insts, _oracle_runs(insts, [30, 30]), MIXED_TOL)
+
+
+@pytest.mark.parametrize("variant", ["0", "1"])
+def test_batch_mixed_variants_match_oracle(variant, monkeypatch):
+    """Mixed batch with each 2D variant forced: 512^2 register-staged or tile
+    passes, 256^2 register-staged or tile passes."""
+    monkeypatch.setenv("ATUS_BATCH_VARIANT", variant)
+    sizes = [(2, 512), (2, 256), (1, 2048)]
+    insts = _instances(13, sizes)
+    b = Batch(insts, PREC_MIXED, DT)
+    for i, d in enumerate(insts):
+        b.set_psi(i, 0, _psi0(d["header"]))
+        b.set_psi(i, 1, np.zeros_like(_psi0(d["header"])))
+    b.run(40)
+    _check(b, insts, _oracle_runs(insts, [40]), MIXED_TOL)
