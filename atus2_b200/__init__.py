@@ -9,6 +9,7 @@ from .engine import (  # noqa: F401
     PREC_FP64,
     PREC_MIXED,
     STEP_BRAGG_AD,
+    STEP_DOUBLE_BRAGG_AD,
     STEP_NL,
     STEP_NL_IF,
     AtusError,

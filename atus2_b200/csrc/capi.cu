@@ -118,6 +118,14 @@ static NLArgs nl_args(const atus_ctx *ctx, int kind, double t1, double F) {
   a.dx0 = ctx->d[0];
   a.shift0 = (int)(ctx->n[0] / 2);
   a.stable = ctx->bragg_stable;
+  a.beta1 = ctx->laser.beta[1];
+  a.beta2 = ctx->laser.beta[2];
+  a.dx1 = ctx->d[1];
+  a.dx2 = ctx->d[2];
+  a.shift1 = (int)(ctx->n[1] / 2);
+  a.shift2 = (int)(ctx->n[2] / 2);
+  a.lg1 = ctx->lg[1];
+  a.lg2 = ctx->lg[2];
   return a;
 }
 
@@ -653,8 +661,10 @@ int atus_ft_step(atus_ctx *ctx, int half) {
 }
 
 static int check_kind(atus_ctx *ctx, int kind) {
-  if (kind != K_NL && kind != K_NL_IF && kind != K_BRAGG) return fail(ctx, ATUS_E_ARG, "unknown step kind");
+  if (kind != K_NL && kind != K_NL_IF && kind != K_BRAGG && kind != K_DBRAGG)
+    return fail(ctx, ATUS_E_ARG, "unknown step kind");
   if (kind == K_BRAGG && ctx->ncomp != 2) return fail(ctx, ATUS_E_ARG, "bragg_ad needs two components");
+  if (kind == K_DBRAGG && ctx->ncomp != 3) return fail(ctx, ATUS_E_ARG, "the three-level bragg_ad needs three components");
   return ATUS_OK;
 }
 
@@ -678,6 +688,29 @@ int atus_strang_block(atus_ctx *ctx, int nk, int kind, const double *F) {
   if (!ctx || nk < 1) return ATUS_E_ARG;
   RUN(check_kind(ctx, kind));
   const double dt = ctx->dt;
+  if (ctx->dim == 1 && ctx->ncomp > 2) {
+    // more components than the resident 1D kernel holds: per step one
+    // kinetic pass (FFT, phase, IFFT per component) and one point-wise
+    // potential step
+    RUN(kinetic_pass(ctx, 1));
+    ctx->t += 0.5 * dt;
+    for (int j = 0; j < nk; j++) {
+      NLKArgs a;
+      memset(&a, 0, sizeof(a));
+      for (int c = 0; c < MAXC; c++) a.psi[c] = ctx->psi[c];
+      a.nl = nl_args(ctx, kind, ctx->t + 0.5 * dt, F ? F[j] : 1.0);
+      a.g = geo(ctx);
+      if (ctx->prec == ATUS_PREC_FP64)
+        nl_kernel<double><<<grid_blocks(ctx->npts, 256), 256, 0, ctx->stream>>>(a);
+      else
+        nl_kernel<float><<<grid_blocks(ctx->npts, 256), 256, 0, ctx->stream>>>(a);
+      LAUNCHED(ctx);
+      const bool last = (j == nk - 1);
+      RUN(kinetic_pass(ctx, last ? 1 : 0));
+      ctx->t += last ? 0.5 * dt : dt;
+    }
+    return ATUS_OK;
+  }
   if (ctx->dim == 1) {
     Block1DArgs a;
     memset(&a, 0, sizeof(a));

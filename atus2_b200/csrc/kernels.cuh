@@ -36,7 +36,7 @@ constexpr int BLOCK1D_NT = 256;  // threads of the resident 1D Strang-block kern
 enum { T_NONE = 0, T_FWD = -1, T_INV = 1 };
 enum { OP_NONE = 0, OP_KIN = 1, OP_NL = 2, OP_FILT = 3 };
 enum { FILT_SOBOLEV = 0, FILT_LAPLACE = 1 };
-enum { K_NL = 0, K_NL_IF = 1, K_BRAGG = 2 };
+enum { K_NL = 0, K_NL_IF = 1, K_BRAGG = 2, K_DBRAGG = 3 };
 // modes of the register-staged pass kernel (pass2.cuh)
 enum { M2_FWD = 0, M2_INV = 1, M2_KIN = 2, M2_NL = 3 };
 
@@ -58,6 +58,10 @@ struct NLArgs {
   double dx0;               // grid step of axis 0
   int shift0;               // n0 / 2
   int stable;               // FP64 Bragg step in the eigenvalue-free form (1) or the reference's (0)
+  // three-level Bragg step: beta . x over every axis (grid steps, centres and
+  // log2 lengths of axes 1 and 2 to recover y and z from the grid index)
+  double beta1, beta2, dx1, dx2;
+  int shift1, shift2, lg1, lg2;
 };
 
 struct Geo {
@@ -164,6 +168,88 @@ template <> __device__ __forceinline__ double2 expi<float>(double phi) {
   return make_double2(cd * inv, sd * inv);
 }
 
+// ------------------------------------------------------------ three-level Bragg step
+// Bragg_double::Do_Double_Bragg_ad (source/interferometry/src/double_bragg.cpp:
+// 123-256) at grid index l: state 1 (component 0) couples to states 2 and 3
+// with Omega_+ = F Amp cos(k x - (domh + rate t1) t1 - phase/2) and Omega_- =
+// F Amp cos(-k x - (domh - rate t1) t1 - phase/2); states 2 and 3 share V22;
+// V includes beta . x over all axes.  The reference's operation order,
+// including its O32 update that reads the already-updated O23 imaginary part
+// (double_bragg.cpp:233).  FP64 arithmetic for both field precisions.
+template <typename R>
+__device__ __forceinline__ void dbragg_point(const NLArgs &a, cplx<R> *v, int64_t l, double x0) {
+  double bx = a.L.beta0 * x0;
+  if (a.lg1 > 0) {
+    const int iy = (int)((l >> a.lg2) & ((1 << a.lg1) - 1));
+    bx += a.beta1 * ((double)(iy - a.shift1) * a.dx1);
+  }
+  if (a.lg2 > 0) {
+    const int iz = (int)(l & ((1 << a.lg2) - 1));
+    bx += a.beta2 * ((double)(iz - a.shift2) * a.dx2);
+  }
+  const double2 p1 = to_d<R>(v[0]), p2 = to_d<R>(v[1]), p3 = to_d<R>(v[2]);
+  double tmp1 = p1.x * p1.x + p1.y * p1.y;
+  double tmp2 = p2.x * p2.x + p2.y * p2.y;
+  const double tmp3 = p3.x * p3.x + p3.y * p3.y;
+  const double *gs = a.gs;  // padded rows: g_ij at i * MAXC + j
+  const double V11 = gs[0] * tmp1 + gs[1] * tmp2 + gs[2] * tmp3 + bx;
+  const double V22 = gs[MAXC] * tmp1 + gs[MAXC + 1] * tmp2 + gs[MAXC + 2] * tmp3 - a.L.DeltaL[1] + bx;
+  const double t1 = a.t1, dt = a.dt;
+  const double F = a.F < 0 ? 0.0 : a.F;
+  double dw = a.L.laser_domh0 + a.L.chirp_rate0 * t1;
+  const double Op = F * a.L.Amp0 * cos(a.L.laser_k0 * x0 - dw * t1 - a.L.phase0 / 2);
+  dw = a.L.laser_domh0 - a.L.chirp_rate0 * t1;
+  const double Om = F * a.L.Amp0 * cos(-a.L.laser_k0 * x0 - dw * t1 - a.L.phase0 / 2);
+  double re1, im1;
+  if (Om == 0.0 && Op == 0.0) {
+    sincos_step(-dt * V11, &im1, &re1);
+    v[0] = from_d<R>(cmul(p1, make_double2(re1, im1)));
+    sincos_step(-dt * V22, &im1, &re1);
+    v[1] = from_d<R>(cmul(p2, make_double2(re1, im1)));
+    v[2] = from_d<R>(cmul(p3, make_double2(re1, im1)));
+    return;
+  }
+  double e0, e1;
+  sincos(-0.5 * a.L.laser_dk0 * x0, &e1, &e0);
+  const double OO = Op * Op + Om * Om;
+  tmp1 = sqrt((V11 - V22) * (V11 - V22) + 4.0 * OO);
+  const double E1 = 0.5 * (V11 + V22 + tmp1);
+  const double E2 = 0.5 * (V11 + V22 - tmp1);
+  double2 g1, g2, g3;
+  sincos_step(-dt * E1, &im1, &re1);
+  tmp1 = 1.0 / fabs((V22 - E1) * (V22 - E1) + Op * Op + Om * Om);
+  g1 = make_double2(tmp1 * re1, tmp1 * im1);
+  sincos_step(-dt * E2, &im1, &re1);
+  tmp1 = 1.0 / fabs((V22 - E2) * (V22 - E2) + Op * Op + Om * Om);
+  g2 = make_double2(tmp1 * re1, tmp1 * im1);
+  sincos_step(-dt * V22, &im1, &re1);
+  tmp1 = 1.0 / fabs(OO);
+  g3 = make_double2(tmp1 * re1, tmp1 * im1);
+  tmp1 = (V22 - E2) * (V22 - E2);
+  tmp2 = (V22 - E1) * (V22 - E1);
+  const double2 O11 = make_double2(tmp1 * g2.x + tmp2 * g1.x, tmp1 * g2.y + tmp2 * g1.y);
+  tmp1 = (V22 - E2) * g2.x + (V22 - E1) * g1.x;
+  tmp2 = (V22 - E2) * g2.y + (V22 - E1) * g1.y;
+  const double2 A12 = make_double2(-Op * tmp1, -Op * tmp2);  // O12 = O21 before eta
+  const double2 A13 = make_double2(-Om * tmp1, -Om * tmp2);  // O13 = O31 before eta
+  const double2 O12 = make_double2(e0 * A12.x - e1 * A12.y, e1 * A12.x + e0 * A12.y);
+  const double2 O21 = make_double2(e0 * A12.x + e1 * A12.y, e0 * A12.y - e1 * A12.x);
+  const double2 O31 = make_double2(e0 * A13.x - e1 * A13.y, e1 * A13.x + e0 * A13.y);
+  const double2 O13 = make_double2(e0 * A13.x + e1 * A13.y, e0 * A13.y - e1 * A13.x);
+  tmp1 = Op * Op;
+  tmp2 = Om * Om;
+  const double2 O22 = make_double2(tmp1 * (g2.x + g1.x) + tmp2 * g3.x, tmp1 * (g2.y + g1.y) + tmp2 * g3.y);
+  const double2 O33 = make_double2(tmp2 * (g2.x + g1.x) + tmp1 * g3.x, tmp2 * (g2.y + g1.y) + tmp1 * g3.y);
+  tmp1 = Om * Op;
+  const double2 A23 = make_double2(tmp1 * (g1.x + g2.x - g3.x), tmp1 * (g1.y + g2.y - g3.y));
+  const double ep = e0 * e0 + e1 * e1, em = e0 * e0 - e1 * e1, e2 = 2 * e0 * e1;
+  const double2 O23 = make_double2(ep * A23.x + e2 * A23.y, ep * A23.y - e2 * A23.x);
+  const double2 O32 = make_double2(em * A23.x - e2 * A23.y, em * O23.y + e2 * A23.x);
+  v[0] = from_d<R>(cadd(cadd(cmul(O11, p1), cmul(O12, p2)), cmul(O13, p3)));
+  v[1] = from_d<R>(cadd(cadd(cmul(O21, p1), cmul(O22, p2)), cmul(O23, p3)));
+  v[2] = from_d<R>(cadd(cadd(cmul(O31, p1), cmul(O32, p2)), cmul(O33, p3)));
+}
+
 // ------------------------------------------------------------ potential step
 // Point-wise potential step on the ncomp values v[] at grid index l.
 // FP64: the reference's formulas (include/CRT_Base.h:410-439,
@@ -173,6 +259,10 @@ template <typename R>
 __device__ __forceinline__ void nl_point(const NLArgs &a, cplx<R> *v, int64_t l, double x0, double Omega,
                                          double eta_c, double eta_s) {
   using C = cplx<R>;
+  if (a.kind == K_DBRAGG) {
+    dbragg_point<R>(a, v, l, x0);
+    return;
+  }
   const int n = a.ncomp;
   double rho[MAXC];
   #pragma unroll

@@ -117,7 +117,7 @@ static inline int launch_block1d_n(atus_ctx *ctx, Block1DArgs &a) {
 template <typename R, int N, int TC, int MODE, bool STRIDED>
 static inline int launch_pass2_t(atus_ctx *ctx, PassArgs &a, int axis) {
   using Cfg = P2Cfg<R, N, TC>;
-  constexpr size_t smem = (MODE == M2_KIN) ? Cfg::smem_kin : Cfg::smem;
+  constexpr size_t smem = (MODE == M2_KIN && Cfg::kin_smem) ? Cfg::smem_kin : Cfg::smem;
   static int resident = 0;
   static int nsm = 0;
   if (!resident) {

@@ -45,6 +45,8 @@ struct P2Cfg {
   // k-space passes also keep the along-axis kinetic factors of up to two
   // components in shared memory (FP64)
   static constexpr size_t smem_kin = smem + 2 * N * sizeof(double2);
+  // the kinetic factors go to shared memory only if that keeps MINB CTAs per SM
+  static constexpr bool kin_smem = (smem_kin + 1024) * Tile2<R>::MINB <= 228 * 1024;
 };
 
 // Exchange layout of one pencil-component: row-major R2 x 16 with row pitch
@@ -108,7 +110,7 @@ __device__ __forceinline__ bool p2_setup(const PassArgs &a, unsigned char *smem_
   }
   // k-space passes: along-axis kinetic factors of components 0 and 1
   double2 *const s_kt = reinterpret_cast<double2 *>(smem_raw + Cfg::smem);
-  const bool kt_shared = (MODE == M2_KIN) && a.op == OP_KIN && a.ncomp_grid <= 2;
+  const bool kt_shared = (MODE == M2_KIN) && Cfg::kin_smem && a.op == OP_KIN && a.ncomp_grid <= 2;
   if (kt_shared) {
     for (int e = tid; e < a.ncomp_grid * N; e += NT) {
       const int cc = e / N, i = e % N;

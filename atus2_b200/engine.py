@@ -30,7 +30,7 @@ LIB_PATH = os.path.join(HERE, "libatus_gpu.so")
 ATUS_OK = 0
 PREC_FP64 = 0
 PREC_MIXED = 1
-STEP_NL, STEP_NL_IF, STEP_BRAGG_AD = 0, 1, 2
+STEP_NL, STEP_NL_IF, STEP_BRAGG_AD, STEP_DOUBLE_BRAGG_AD = 0, 1, 2, 3
 MAX_COMP = 4
 
 _ERRORS = {-1: "invalid argument", -2: "unsupported", -3: "CUDA error", -4: "bad state", -5: "out of device memory"}

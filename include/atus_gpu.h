@@ -83,6 +83,8 @@ extern "C" {
 #define ATUS_STEP_NL 0       /* "freeprop" of CRT_Base: V + g|psi|^2 */
 #define ATUS_STEP_NL_IF 1    /* "freeprop" of CRT_Base_IF: g|psi|^2 + beta.x - DeltaL */
 #define ATUS_STEP_BRAGG_AD 2 /* "bragg_ad": analytic 2x2 Bragg exponential */
+#define ATUS_STEP_DOUBLE_BRAGG_AD 3 /* "bragg_ad" of double_bragg: three-level exponential,
+                                       Bragg_double::Do_Double_Bragg_ad (double_bragg.cpp:100-258) */
 
 #define ATUS_MAX_COMP 4
 

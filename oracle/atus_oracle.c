@@ -20,6 +20,8 @@
  *   orc_nl_step               include/CRT_Base.h:396-441 (Do_NL_Step)
  *   orc_nl_if_step            include/CRT_Base_IF.h:380-419 (freeprop of the IF programs)
  *   orc_bragg_ad              source/interferometry/src/bragg.cpp:185-304 (Do_Bragg_ad)
+ *   orc_double_bragg_ad       source/interferometry/src/double_bragg.cpp:100-258
+ *                             (Bragg_double::Do_Double_Bragg_ad)
  *   orc_block                 include/CRT_Base.h:776-786 / CRT_Base_IF.h:779-789
  *   orc_particle_number       include/CRT_Base.h:586-599
  *   orc_expval_position/momentum include/CRT_Base.h:480-580
@@ -363,11 +365,132 @@ void orc_bragg_ad(orc_ctx *c, const orc_laser *L, double F) {
   }
 }
 
-/* Step kinds: 0 = CRT_Base freeprop, 1 = CRT_Base_IF freeprop, 2 = bragg_ad. */
+/* Three-level Bragg step: state 1 (component 0) couples to states 2 and 3
+ * (components 1, 2) with Omega_+ and Omega_-; states 2 and 3 share the
+ * diagonal V22.  The operation order follows double_bragg.cpp:123-256,
+ * including beta . x over all axes (CPoint product), F clipped at 0, and the
+ * O32 update that reads the already-updated O23[1] (double_bragg.cpp:233). */
+void orc_double_bragg_ad(orc_ctx *c, const orc_laser *L, double F) {
+  const double dt = c->dt;
+  const double t1 = c->t + 0.5 * dt;
+  if (F < 0) F = 0;
+  double *P1 = c->psi[0], *P2 = c->psi[1], *P3 = c->psi[2];
+  const double *gs = c->gs;
+  #pragma omp parallel for schedule(static)
+  for (long l = 0; l < c->npts; l++) {
+    double x[3];
+    orc_get_x(c, l, x);
+    double bx = 0;
+    for (int a = 0; a < c->dim; a++) bx += L->beta[a] * x[a];
+    double tmp1 = P1[2 * l] * P1[2 * l] + P1[2 * l + 1] * P1[2 * l + 1];
+    double tmp2 = P2[2 * l] * P2[2 * l] + P2[2 * l + 1] * P2[2 * l + 1];
+    double tmp3 = P3[2 * l] * P3[2 * l] + P3[2 * l + 1] * P3[2 * l + 1];
+    const double V11 = gs[0] * tmp1 + gs[1] * tmp2 + gs[2] * tmp3 + bx;
+    const double V22 = gs[3] * tmp1 + gs[4] * tmp2 + gs[5] * tmp3 - L->DeltaL[1] + bx;
+    double dw = L->laser_domh[0] + (L->chirp_rate[0]) * t1;
+    const double Op = F * L->Amp[0] * cos(L->laser_k[0] * x[0] - dw * t1 - L->phase[0] / 2);
+    dw = L->laser_domh[0] - (L->chirp_rate[0]) * t1;
+    const double Om = F * L->Amp[0] * cos(-L->laser_k[0] * x[0] - dw * t1 - L->phase[0] / 2);
+    double re1, im1;
+    if ((Om == 0.0) && (Op == 0.0)) {
+      sincos(-dt * V11, &im1, &re1);
+      tmp1 = P1[2 * l];
+      P1[2 * l] = tmp1 * re1 - P1[2 * l + 1] * im1;
+      P1[2 * l + 1] = tmp1 * im1 + P1[2 * l + 1] * re1;
+      sincos(-dt * V22, &im1, &re1);
+      tmp1 = P2[2 * l];
+      P2[2 * l] = tmp1 * re1 - P2[2 * l + 1] * im1;
+      P2[2 * l + 1] = tmp1 * im1 + P2[2 * l + 1] * re1;
+      tmp1 = P3[2 * l];
+      P3[2 * l] = tmp1 * re1 - P3[2 * l + 1] * im1;
+      P3[2 * l + 1] = tmp1 * im1 + P3[2 * l + 1] * re1;
+      continue;
+    }
+    double eta[2], g1[2], g2[2], g3[2];
+    double O11[2], O12[2], O13[2], O21[2], O22[2], O23[2], O31[2], O32[2], O33[2];
+    sincos(-0.5 * L->laser_dk[0] * x[0], &im1, &re1);
+    eta[0] = re1;
+    eta[1] = im1;
+    tmp1 = sqrt((V11 - V22) * (V11 - V22) + 4.0 * (Op * Op + Om * Om));
+    const double E1 = 0.5 * (V11 + V22 + tmp1);
+    const double E2 = 0.5 * (V11 + V22 - tmp1);
+    sincos(-dt * E1, &im1, &re1);
+    tmp1 = 1.0 / fabs((V22 - E1) * (V22 - E1) + Op * Op + Om * Om);
+    g1[0] = tmp1 * re1;
+    g1[1] = tmp1 * im1;
+    sincos(-dt * E2, &im1, &re1);
+    tmp1 = 1.0 / fabs((V22 - E2) * (V22 - E2) + Op * Op + Om * Om);
+    g2[0] = tmp1 * re1;
+    g2[1] = tmp1 * im1;
+    sincos(-dt * V22, &im1, &re1);
+    tmp1 = 1.0 / fabs(Op * Op + Om * Om);
+    g3[0] = tmp1 * re1;
+    g3[1] = tmp1 * im1;
+    tmp1 = (V22 - E2) * (V22 - E2);
+    tmp2 = (V22 - E1) * (V22 - E1);
+    O11[0] = tmp1 * g2[0] + tmp2 * g1[0];
+    O11[1] = tmp1 * g2[1] + tmp2 * g1[1];
+    tmp1 = (V22 - E2) * g2[0] + (V22 - E1) * g1[0];
+    tmp2 = (V22 - E2) * g2[1] + (V22 - E1) * g1[1];
+    O12[0] = -Op * tmp1;
+    O12[1] = -Op * tmp2;
+    O13[0] = -Om * tmp1;
+    O13[1] = -Om * tmp2;
+    O21[0] = O12[0];
+    O21[1] = O12[1];
+    O31[0] = O13[0];
+    O31[1] = O13[1];
+    tmp1 = O12[0];
+    O12[0] = eta[0] * tmp1 - eta[1] * O12[1];
+    O12[1] = eta[1] * tmp1 + eta[0] * O12[1];
+    tmp1 = O21[0];
+    O21[0] = eta[0] * tmp1 + eta[1] * O21[1];
+    O21[1] = eta[0] * O21[1] - eta[1] * tmp1;
+    tmp1 = O31[0];
+    O31[0] = eta[0] * tmp1 - eta[1] * O31[1];
+    O31[1] = eta[1] * tmp1 + eta[0] * O31[1];
+    tmp1 = O13[0];
+    O13[0] = eta[0] * tmp1 + eta[1] * O13[1];
+    O13[1] = eta[0] * O13[1] - eta[1] * tmp1;
+    tmp1 = Op * Op;
+    tmp2 = Om * Om;
+    O22[0] = tmp1 * (g2[0] + g1[0]) + tmp2 * g3[0];
+    O22[1] = tmp1 * (g2[1] + g1[1]) + tmp2 * g3[1];
+    O33[0] = tmp2 * (g2[0] + g1[0]) + tmp1 * g3[0];
+    O33[1] = tmp2 * (g2[1] + g1[1]) + tmp1 * g3[1];
+    tmp1 = Om * Op;
+    O23[0] = tmp1 * (g1[0] + g2[0] - g3[0]);
+    O23[1] = tmp1 * (g1[1] + g2[1] - g3[1]);
+    O32[0] = O23[0];
+    O32[1] = O23[1];
+    tmp1 = O23[0];
+    O23[0] = (eta[0] * eta[0] + eta[1] * eta[1]) * tmp1 + 2 * eta[0] * eta[1] * O23[1];
+    O23[1] = (eta[0] * eta[0] + eta[1] * eta[1]) * O23[1] - 2 * eta[0] * eta[1] * tmp1;
+    tmp1 = O32[0];
+    O32[0] = (eta[0] * eta[0] - eta[1] * eta[1]) * tmp1 - 2 * eta[0] * eta[1] * O32[1];
+    O32[1] = (eta[0] * eta[0] - eta[1] * eta[1]) * O23[1] + 2 * eta[0] * eta[1] * tmp1;
+    g1[0] = P1[2 * l];
+    g1[1] = P1[2 * l + 1];
+    g2[0] = P2[2 * l];
+    g2[1] = P2[2 * l + 1];
+    g3[0] = P3[2 * l];
+    g3[1] = P3[2 * l + 1];
+    P1[2 * l] = (O11[0] * g1[0] - O11[1] * g1[1]) + (O12[0] * g2[0] - O12[1] * g2[1]) + (O13[0] * g3[0] - O13[1] * g3[1]);
+    P1[2 * l + 1] = (O11[0] * g1[1] + O11[1] * g1[0]) + (O12[0] * g2[1] + O12[1] * g2[0]) + (O13[0] * g3[1] + O13[1] * g3[0]);
+    P2[2 * l] = (O21[0] * g1[0] - O21[1] * g1[1]) + (O22[0] * g2[0] - O22[1] * g2[1]) + (O23[0] * g3[0] - O23[1] * g3[1]);
+    P2[2 * l + 1] = (O21[0] * g1[1] + O21[1] * g1[0]) + (O22[0] * g2[1] + O22[1] * g2[0]) + (O23[0] * g3[1] + O23[1] * g3[0]);
+    P3[2 * l] = (O31[0] * g1[0] - O31[1] * g1[1]) + (O32[0] * g2[0] - O32[1] * g2[1]) + (O33[0] * g3[0] - O33[1] * g3[1]);
+    P3[2 * l + 1] = (O31[0] * g1[1] + O31[1] * g1[0]) + (O32[0] * g2[1] + O32[1] * g2[0]) + (O33[0] * g3[1] + O33[1] * g3[0]);
+  }
+}
+
+/* Step kinds: 0 = CRT_Base freeprop, 1 = CRT_Base_IF freeprop, 2 = bragg_ad,
+ * 3 = bragg_ad of the three-level double_bragg program. */
 static void nl_dispatch(orc_ctx *c, int kind, const orc_laser *L, double F) {
   if (kind == 0) orc_nl_step(c);
   else if (kind == 1) orc_nl_if_step(c, L);
-  else orc_bragg_ad(c, L, F);
+  else if (kind == 2) orc_bragg_ad(c, L, F);
+  else orc_double_bragg_ad(c, L, F);
 }
 
 /* One outer iteration of run_sequence: half, (V, full)^(Nk-1), V, half.

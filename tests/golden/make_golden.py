@@ -99,6 +99,17 @@ BRAGG_CASES = [
          Delta_L=[0.0, 0.0], Beta=[0.0, 0.0, 0.0]),
 ]
 
+DBRAGG_CASES = [
+    dict(name="dbragg1d", dim=1, n=[256], lo=[-32.0], hi=[32.0], laser_k=2.0, laser_domh=8.0, Amp=4.0,
+         tc=0.03, two_sigma2=2 * 0.01 ** 2, g=[100.0, 90.0, 90.0, 90.0, 100.0, 95.0, 90.0, 95.0, 100.0],
+         Delta_L=[0.0, 0.0, 0.0], Beta=[0.05]),
+    dict(name="dbragg2d", dim=2, n=[64, 32], lo=[-16.0, -8.0], hi=[16.0, 8.0], laser_k=2.0, laser_domh=8.0,
+         Amp=4.0, tc=0.03, two_sigma2=2 * 0.01 ** 2, g=[100.0] * 9, Delta_L=[0.0, 0.5, 0.5], Beta=[0.1, 0.05]),
+    dict(name="dbragg3d", dim=3, n=[16, 8, 16], lo=[-8.0, -4.0, -8.0], hi=[8.0, 4.0, 8.0], laser_k=1.5,
+         laser_domh=4.0, Amp=4.0, tc=0.03, two_sigma2=2 * 0.01 ** 2, g=[100.0] * 9, Delta_L=[0.0, 0.0, 0.0],
+         Beta=[0.0, 0.02, 0.03]),
+]
+
 SOB_CASES = [
     dict(name="sob1d", dim=1, n=[64], lo=[-8.0], hi=[8.0], g=50.0, Nparticles=1.0, alpha=0.5, stepsize=0.01,
          epsilon=1e-7, V_expr="0.5*x*x", guess_expr="exp(-0.5*x*x)"),
@@ -240,6 +251,63 @@ def make_bragg(case, tmp):
                 params=json.dumps(params), xml=xml)
 
 
+def make_dbragg(case, tmp):
+    """The three-level program (double_bragg): state 1 a Thomas-Fermi-like
+    profile with noise, states 2 and 3 empty."""
+    rng = np.random.default_rng(2)
+    dim = case["dim"]
+    h = binfmt.make_header(dim, case["n"], case["lo"], case["hi"], dt=0.001)
+    X = grid(h)
+    r2 = sum(x * x for x in X)
+    psi1 = np.sqrt(np.maximum(0.0, 1.0 - 0.1 * r2)) * (1 + 0.01 * rng.standard_normal(r2.shape))
+    psi1 = psi1.astype(np.complex128)
+    psi2 = np.zeros_like(psi1)
+    for k, p in enumerate((psi1, psi2, psi2)):
+        binfmt.write_bin(os.path.join(tmp, f"inp_{k + 1}.bin"), h, p)
+    seq = [dict(name="bragg_ad", dt=0.001, Nk=20, duration=0.06, rabi=True),
+           dict(name="freeprop", dt=0.001, Nk=20, duration=0.04, rabi=True)]
+    g = case["g"]
+    xml = f"""<SIMULATION>
+  <DIM>{dim}</DIM>
+  <FILENAME>inp_1.bin</FILENAME>
+  <FILENAME_2>inp_2.bin</FILENAME_2>
+  <FILENAME_3>inp_3.bin</FILENAME_3>
+  <AMP_T>exp(-(t-{case['tc']!r})*(t-{case['tc']!r})/{case['two_sigma2']!r})</AMP_T>
+  <CONSTANTS>
+    <laser_k>{case['laser_k']!r}</laser_k><laser_dk>0</laser_dk><laser_domh>{case['laser_domh']!r}</laser_domh>
+    <rabi_threshold>1.0</rabi_threshold><chirp>0</chirp>
+  </CONSTANTS>
+  <VCONSTANTS>
+    <Amp_1>{case['Amp']!r},{case['Amp']!r}</Amp_1>
+    <Alpha_1>{xml_vec([0.5] * dim)}</Alpha_1>
+    <Delta_L>{xml_vec(case['Delta_L'])}</Delta_L>
+    <GS_1>{xml_vec(g[0:3])}</GS_1>
+    <GS_2>{xml_vec(g[3:6])}</GS_2>
+    <GS_3>{xml_vec(g[6:9])}</GS_3>
+    <Beta>{xml_vec(case['Beta'])}</Beta>
+  </VCONSTANTS>
+  <ALGORITHM><DT>1</DT></ALGORITHM>
+  <SEQUENCE>{seq_xml(seq, ' rabi_output_freq="each"')}</SEQUENCE>
+</SIMULATION>"""
+    open(os.path.join(tmp, "run.xml"), "w").write(xml)
+    run("double_bragg", tmp)
+    t, psi = collect_outputs(tmp, 3, seq)
+    rabi = []
+    for s in (1, 2):
+        rows = [ln.split() for ln in open(os.path.join(tmp, f"Rabi_{s}_0.txt")) if not ln.startswith("#")]
+        rabi += [[float(v) for v in r[1:]] for r in rows if r]
+    k0 = np.zeros((3, dim))
+    k0[1, 0] = 2 * case["laser_k"]
+    k0[2, 0] = -2 * case["laser_k"]
+    params = dict(program="double_bragg", dim=dim, ncomp=3, header_dt=0.001, algo_dt=1.0, Alpha_1=[0.5] * dim,
+                  gs=g, sequence=seq, AMP_T=dict(tc=case["tc"], two_sigma2=case["two_sigma2"]),
+                  laser_k=case["laser_k"], laser_domh=case["laser_domh"], laser_dk=0.0, chirp=0.0,
+                  Amp_1=[case["Amp"], case["Amp"]], Delta_L=case["Delta_L"], Beta=case["Beta"],
+                  rabi_threshold=1.0, rabi_k0=k0.tolist())
+    return dict(header=h.tobytes(), psi0=np.stack([psi1, psi2, psi2]), t=t, psi=psi, rabi=np.array(rabi),
+                params=json.dumps(params), xml=xml)
+
+
 def make_sob(case, tmp):
     dim = case["dim"]
     ax = "XYZ"[:dim]
@@ -266,8 +334,13 @@ def make_sob(case, tmp):
 
 
 def main():
-    if not os.path.exists(os.path.join(REF, "rt_solver")):
+    if not os.path.exists(os.path.join(REF, "double_bragg")):
         subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+    only = set(sys.argv[1:])
+    keep = (lambda c: not only or c["name"] in only)
+    global CASES, BRAGG_CASES, DBRAGG_CASES, SOB_CASES
+    CASES, BRAGG_CASES = [c for c in CASES if keep(c)], [c for c in BRAGG_CASES if keep(c)]
+    DBRAGG_CASES, SOB_CASES = [c for c in DBRAGG_CASES if keep(c)], [c for c in SOB_CASES if keep(c)]
     for case in CASES:
         with tempfile.TemporaryDirectory() as tmp:
             d = make_rt(case, tmp)
@@ -276,6 +349,11 @@ def main():
     for case in BRAGG_CASES:
         with tempfile.TemporaryDirectory() as tmp:
             d = make_bragg(case, tmp)
+        np.savez_compressed(os.path.join(HERE, case["name"] + ".npz"), **d)
+        print("wrote", case["name"], d["psi"].shape, d["rabi"].shape)
+    for case in DBRAGG_CASES:
+        with tempfile.TemporaryDirectory() as tmp:
+            d = make_dbragg(case, tmp)
         np.savez_compressed(os.path.join(HERE, case["name"] + ".npz"), **d)
         print("wrote", case["name"], d["psi"].shape, d["rabi"].shape)
     for case in SOB_CASES:

@@ -17,7 +17,7 @@ import math
 
 import numpy as np
 
-KIND_NL, KIND_NL_IF, KIND_BRAGG_AD = 0, 1, 2
+KIND_NL, KIND_NL_IF, KIND_BRAGG_AD, KIND_DOUBLE_BRAGG_AD = 0, 1, 2, 3
 
 
 def gaussian_pulse(tc: float, two_sigma2: float):
@@ -35,7 +35,7 @@ def laser_kwargs(p: dict) -> dict:
     beta = list(p.get("Beta", [0.0] * dim)) + [0.0] * (3 - dim)
     return dict(
         beta=beta,
-        DeltaL=list(p.get("Delta_L", [0.0, 0.0])) + [0.0, 0.0],
+        DeltaL=(list(p.get("Delta_L", [0.0, 0.0])) + [0.0] * 4)[:4],
         Amp=p.get("Amp_1", [0.0, 0.0]),
         laser_k=[p.get("laser_k", 0.0), 0.0],
         laser_dk=[p.get("laser_dk", 0.0), 0.0],
@@ -52,7 +52,7 @@ def run_rt(engine, p: dict, psi0, V=None, make_laser=None, on_block=None):
     p keys: dim, ncomp, header_dt (dt stored in the input file), algo_dt
     (ALGORITHM/DT), Alpha_1, gs (flat ncomp^2), sequence = list of dicts
     {name, dt, Nk, duration}, optional AMP_T pulse {tc, two_sigma2}, program
-    ('rt_solver' or 'bragg').  Returns the list of (t, [psi per comp]) after
+    ('rt_solver', 'bragg' or 'double_bragg').  Returns the list of (t, [psi per comp]) after
     every block, and the Rabi sums per block when the program is bragg.
     """
     ncomp = p["ncomp"]
@@ -68,7 +68,7 @@ def run_rt(engine, p: dict, psi0, V=None, make_laser=None, on_block=None):
     laser = make_laser(**laser_kwargs(p)) if make_laser is not None else None
     F = gaussian_pulse(p["AMP_T"]["tc"], p["AMP_T"]["two_sigma2"]) if p.get("AMP_T") else None
     outputs, rabi = [], []
-    is_if = p["program"] == "bragg"
+    is_if = p["program"] in ("bragg", "double_bragg")
     for seq in p["sequence"]:
         subN = int(seq["duration"] / seq["dt"])
         nk = seq["Nk"]
@@ -77,14 +77,14 @@ def run_rt(engine, p: dict, psi0, V=None, make_laser=None, on_block=None):
             engine.set_dt(seq["dt"])
             cur_dt = seq["dt"]
         if seq["name"] == "bragg_ad":
-            kind = KIND_BRAGG_AD
+            kind = KIND_DOUBLE_BRAGG_AD if p["program"] == "double_bragg" else KIND_BRAGG_AD
         elif is_if:
             kind = KIND_NL_IF
         else:
             kind = KIND_NL
         for _ in range(na):
             Fv = None
-            if kind == KIND_BRAGG_AD:
+            if kind in (KIND_BRAGG_AD, KIND_DOUBLE_BRAGG_AD):
                 t = engine.t + 0.5 * seq["dt"]
                 Fv = []
                 for j in range(nk):

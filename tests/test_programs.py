@@ -14,7 +14,7 @@ import numpy as np
 import pytest
 
 from atus2_b200 import binfmt
-from golden_io import BRAGG_CASES, RT_CASES, SOB_CASES, load
+from golden_io import BRAGG_CASES, DBRAGG_CASES, RT_CASES, SOB_CASES, load
 from gpu_util import rel_l2
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -84,19 +84,19 @@ def _outputs(tmp, ncomp):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", RT_CASES + BRAGG_CASES)
+@pytest.mark.parametrize("name", RT_CASES + BRAGG_CASES + DBRAGG_CASES)
 def test_realtime_program_matches_reference(name):
     from test_gpu_parity import FP64_TOL, state_close
 
     g = load(name)
     p = g["params"]
-    prog = "bragg" if p["program"] == "bragg" else "rt_solver"
+    prog = p["program"] if p["program"] in ("bragg", "double_bragg") else "rt_solver"
     with tempfile.TemporaryDirectory() as tmp:
         _write_inputs(g, tmp)
         run(prog, tmp)
         outs = _outputs(tmp, p["ncomp"])
         rabi = []
-        if prog == "bragg":
+        if prog != "rt_solver":
             for s in (1, 2):
                 rows = [ln.split() for ln in open(os.path.join(tmp, f"Rabi_{s}_0.txt")) if not ln.startswith("#")]
                 rabi += [[float(v) for v in r[1:]] for r in rows if r]
@@ -104,7 +104,7 @@ def test_realtime_program_matches_reference(name):
     for (t, psi), t_ref, psi_ref in zip(outs, g["t"], g["psi"]):
         assert t == t_ref
         state_close(list(psi), list(psi_ref), FP64_TOL)
-    if prog == "bragg":
+    if prog != "rt_solver":
         np.testing.assert_allclose(np.array(rabi), g["rabi"], rtol=5e-6, atol=1e-10)
 
 
