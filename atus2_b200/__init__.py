@@ -10,6 +10,8 @@ from .engine import (  # noqa: F401
     PREC_MIXED,
     STEP_BRAGG_AD,
     STEP_DOUBLE_BRAGG_AD,
+    STEP_NL_IF_2,
+    STEP_BRAGG_DS_AD,
     STEP_NL,
     STEP_NL_IF,
     AtusError,

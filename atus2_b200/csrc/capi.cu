@@ -126,6 +126,20 @@ static NLArgs nl_args(const atus_ctx *ctx, int kind, double t1, double F) {
   a.shift2 = (int)(ctx->n[2] / 2);
   a.lg1 = ctx->lg[1];
   a.lg2 = ctx->lg[2];
+  a.L2.beta0 = ctx->laser2.beta[0];
+  a.L2.Amp0 = ctx->laser2.Amp[0];
+  a.L2.laser_k0 = ctx->laser2.laser_k[0];
+  a.L2.laser_dk0 = ctx->laser2.laser_dk[0];
+  a.L2.laser_domh0 = ctx->laser2.laser_domh[0];
+  a.L2.phase0 = ctx->laser2.phase[0];
+  a.L2.chirp_rate0 = ctx->laser2.chirp_rate[0];
+  a.F2 = F;
+  if (kind == K_BRAGG_DS) {
+    // mode1 / mode2 of bragg_ds.cpp:117-127: time = t1 - seq.time
+    const double time = t1 - ctx->win_t0;
+    if (time > ctx->win_dur[0]) a.F = 0.0;
+    if (time > ctx->win_dur[1]) a.F2 = 0.0;
+  }
   return a;
 }
 
@@ -619,6 +633,20 @@ int atus_set_laser(atus_ctx *ctx, const atus_laser *laser) {
   return ATUS_OK;
 }
 
+int atus_set_laser2(atus_ctx *ctx, const atus_laser *laser2) {
+  if (!ctx || !laser2) return ATUS_E_ARG;
+  ctx->laser2 = *laser2;
+  return ATUS_OK;
+}
+
+int atus_set_pulse_windows(atus_ctx *ctx, double t_start, const double *duration) {
+  if (!ctx || !duration) return ATUS_E_ARG;
+  ctx->win_t0 = t_start;
+  ctx->win_dur[0] = duration[0];
+  ctx->win_dur[1] = duration[1];
+  return ATUS_OK;
+}
+
 int atus_upload_psi(atus_ctx *ctx, int comp, const double *psi) {
   if (!ctx || !psi || comp < 0 || comp >= ctx->ncomp) return ATUS_E_ARG;
   if (ctx->prec == ATUS_PREC_FP64) {
@@ -661,8 +689,10 @@ int atus_ft_step(atus_ctx *ctx, int half) {
 }
 
 static int check_kind(atus_ctx *ctx, int kind) {
-  if (kind != K_NL && kind != K_NL_IF && kind != K_BRAGG && kind != K_DBRAGG)
-    return fail(ctx, ATUS_E_ARG, "unknown step kind");
+  if (kind < K_NL || kind > K_BRAGG_DS) return fail(ctx, ATUS_E_ARG, "unknown step kind");
+  if (kind == K_NL_IF2 && (ctx->ncomp % 2) != 0)
+    return fail(ctx, ATUS_E_ARG, "the two-species freeprop needs an even number of components");
+  if (kind == K_BRAGG_DS && ctx->ncomp != 4) return fail(ctx, ATUS_E_ARG, "the two-species bragg_ad needs four components");
   if (kind == K_BRAGG && ctx->ncomp != 2) return fail(ctx, ATUS_E_ARG, "bragg_ad needs two components");
   if (kind == K_DBRAGG && ctx->ncomp != 3) return fail(ctx, ATUS_E_ARG, "the three-level bragg_ad needs three components");
   return ATUS_OK;
@@ -906,9 +936,14 @@ int atus_setup_momentum(atus_ctx *ctx, int comp, const double *p) {
 }
 
 int atus_rabi_integrals(atus_ctx *ctx, const double *k0, int n, double thr, double *out) {
+  return atus_rabi_integrals_comp(ctx, 0, k0, n, thr, out);
+}
+
+int atus_rabi_integrals_comp(atus_ctx *ctx, int comp, const double *k0, int n, double thr, double *out) {
   if (!ctx || !out || n < 0 || n > RED_MAXQ || (n > 0 && !k0)) return ATUS_E_ARG;
+  if (comp < 0 || comp >= ctx->ncomp) return ATUS_E_ARG;
   if (n == 0) return ATUS_OK;
-  RUN(to_scratch(ctx, 0));
+  RUN(to_scratch(ctx, comp));
   RUN(scratch_forward(ctx));
   RedArgs a;
   memset(&a, 0, sizeof(a));

@@ -1,5 +1,6 @@
 // ctx.h -- the engine context shared by the host translation units.
 #pragma once
+#include <cmath>
 #include <cuda_runtime.h>
 
 #include <string>
@@ -20,6 +21,9 @@ struct atus_ctx {
   double alpha[MAXC][3] = {};
   double gs[MAXC * MAXC] = {};  // padded [i*MAXC + j]
   atus_laser laser = {};
+  atus_laser laser2 = {};       // second species (two-species programs)
+  double win_t0 = 0;            // pulse windows of the two-species bragg_ad:
+  double win_dur[2] = {HUGE_VAL, HUGE_VAL};  // species s on while t1 - win_t0 <= win_dur[s]
   size_t csize = 16;            // bytes per complex value
   void *psi[MAXC] = {};
   double *V[MAXC] = {};

@@ -36,7 +36,10 @@ constexpr int BLOCK1D_NT = 256;  // threads of the resident 1D Strang-block kern
 enum { T_NONE = 0, T_FWD = -1, T_INV = 1 };
 enum { OP_NONE = 0, OP_KIN = 1, OP_NL = 2, OP_FILT = 3 };
 enum { FILT_SOBOLEV = 0, FILT_LAPLACE = 1 };
-enum { K_NL = 0, K_NL_IF = 1, K_BRAGG = 2, K_DBRAGG = 3 };
+// step kinds: CRT_Base freeprop, CRT_Base_IF freeprop, bragg_ad, the
+// three-level bragg_ad (double_bragg), CRT_Base_IF_2 freeprop (two species),
+// the two-species bragg_ad (bragg_ds)
+enum { K_NL = 0, K_NL_IF = 1, K_BRAGG = 2, K_DBRAGG = 3, K_NL_IF2 = 4, K_BRAGG_DS = 5 };
 // modes of the register-staged pass kernel (pass2.cuh)
 enum { M2_FWD = 0, M2_INV = 1, M2_KIN = 2, M2_NL = 3 };
 
@@ -62,6 +65,10 @@ struct NLArgs {
   // log2 lengths of axes 1 and 2 to recover y and z from the grid index)
   double beta1, beta2, dx1, dx2;
   int shift1, shift2, lg1, lg2;
+  // second species of the two-species programs (beta0, Amp0, laser_k0,
+  // laser_dk0, laser_domh0, phase0, chirp_rate0 used) and its pulse factor
+  LaserD L2;
+  double F2;
 };
 
 struct Geo {
@@ -250,6 +257,116 @@ __device__ __forceinline__ void dbragg_point(const NLArgs &a, cplx<R> *v, int64_
   v[2] = from_d<R>(cadd(cadd(cmul(O31, p1), cmul(O32, p2)), cmul(O33, p3)));
 }
 
+// ------------------------------------------------------------ two-level exponential
+// exp(-i dt [[V11, Omega eta], [Omega conj(eta), V22]]) applied to (p1, p2).
+// FP64 and not `stable`: the reference's eigenvalue form (bragg.cpp:226-302,
+// bragg_ds.cpp:215-248): E+- = (V11 + V22 +- sqrt((V11 - V22)^2 + 4 Omega^2))/2,
+// gamma+- = e^{-i dt E+-} / |(V11 - E+-)^2 + Omega^2|, pure phases when
+// Omega == 0.  Otherwise the eigenvalue-free form
+//   U = e^{-i dt m} [cos(r dt) I - i sin(r dt)/r [[d, W], [W, -d]]],
+// m = (V11+V22)/2, d = (V11-V22)/2, W = Omega, r = sqrt(d^2 + W^2), built in
+// FP64 from unit (cos, sin) pairs, so it is unitary to FP64 accuracy for every
+// Omega (the eigenvalue form divides by (V11 - E)^2 + Omega^2, which loses
+// unitarity once Omega is below the spacing of V and divides by zero once
+// Omega^2 underflows).
+template <typename R>
+__device__ __forceinline__ void bragg_pair(int stable, double dt, double V11, double V22, double Omega, double eta_c,
+                                           double eta_s, cplx<R> &q1, cplx<R> &q2) {
+  if constexpr (sizeof(R) == 8) {
+    if (!stable) {
+      double re1, im1;
+      if (Omega == 0.0) {
+        sincos_step(-dt * V11, &im1, &re1);
+        q1 = cmul(q1, make_double2(re1, im1));
+        sincos_step(-dt * V22, &im1, &re1);
+        q2 = cmul(q2, make_double2(re1, im1));
+        return;
+      }
+      double tmp1 = sqrt((V11 - V22) * (V11 - V22) + 4.0 * Omega * Omega);
+      const double Ep = 0.5 * (V11 + V22 + tmp1);
+      const double Em = 0.5 * (V11 + V22 - tmp1);
+      double2 gp, gm;
+      sincos_step(-dt * Ep, &im1, &re1);
+      tmp1 = 1.0 / fabs((V11 - Ep) * (V11 - Ep) + Omega * Omega);
+      gp = make_double2(tmp1 * re1, tmp1 * im1);
+      sincos_step(-dt * Em, &im1, &re1);
+      tmp1 = 1.0 / fabs((V11 - Em) * (V11 - Em) + Omega * Omega);
+      gm = make_double2(tmp1 * re1, tmp1 * im1);
+      const double O2 = Omega * Omega;
+      const double2 O11 = make_double2(O2 * (gp.x + gm.x), O2 * (gp.y + gm.y));
+      const double a1 = V11 - Ep, a2 = V11 - Em;
+      const double2 O22 = make_double2(a1 * a1 * gp.x + a2 * a2 * gm.x, a1 * a1 * gp.y + a2 * a2 * gm.y);
+      const double2 Os = make_double2(-Omega * (a1 * gp.x + a2 * gm.x), -Omega * (a1 * gp.y + a2 * gm.y));
+      const double2 eta = make_double2(eta_c, eta_s);
+      const double2 O12 = cmul(Os, eta);   // eta * O12
+      const double2 O21 = cmulc(Os, eta);  // conj(eta) * O21
+      const double2 p1 = q1, p2 = q2;
+      q1 = cadd(cmul(O11, p1), cmul(O12, p2));
+      q2 = cadd(cmul(O21, p1), cmul(O22, p2));
+      return;
+    }
+  }
+  const double m = 0.5 * (V11 + V22), d = 0.5 * (V11 - V22);
+  const double r = sqrt(d * d + Omega * Omega);
+  const double2 e = expi<R>(-dt * m);   // e^{-i dt m}
+  const double2 rr = expi<R>(dt * r);   // (cos r dt, sin r dt)
+  // sin(r dt) / r: Taylor series of sinc (truncation below 2^-72 for r dt <= 1/32)
+  const double xr = dt * r;
+  double sor;
+  if (xr <= 0.03125) {
+    const double x2 = xr * xr;
+    double p = fma(x2, 1.0 / 362880.0, -1.0 / 5040.0);
+    p = fma(p, x2, 1.0 / 120.0);
+    p = fma(p, x2, -1.0 / 6.0);
+    sor = dt * fma(p, x2, 1.0);
+  } else {
+    sor = rr.y / r;
+  }
+  const double fd = sor * d, fw = sor * Omega;
+  // U11 = e(cos - i fd), U22 = e(cos + i fd), Uoff = e(-i fw)
+  const double2 U11 = cmul(e, make_double2(rr.x, -fd));
+  const double2 U22 = cmul(e, make_double2(rr.x, fd));
+  const double2 Uo = cmul(e, make_double2(0.0, -fw));
+  const double2 et = make_double2(eta_c, eta_s);
+  const double2 U12 = cmul(Uo, et), U21 = cmulc(Uo, et);
+  const double2 p1 = to_d<R>(q1), p2 = to_d<R>(q2);
+  q1 = from_d<R>(cadd(cmul(U11, p1), cmul(U12, p2)));
+  q2 = from_d<R>(cadd(cmul(U21, p1), cmul(U22, p2)));
+}
+
+// ------------------------------------------------------------ two-species Bragg step
+// Bragg_single::Do_Bragg_ad of the two-species program (source/interferometry/
+// src/bragg_ds.cpp:111-322) at grid index l: components (0, 1) are species 1,
+// (2, 3) species 2; V_i = sum_j g_ij |psi_j|^2 + (beta_s x - DeltaL_i) with
+// beta_s of the component's species (x along axis 0 only); species s couples
+// with Omega_s = F_s Amp_s cos(k_s x - (domh_s + rate_s t1) t1 + phase_s/2),
+// eta_s = e^{-i (dk_s x + phase_s)/2}.  F_s is 0 outside the species' pulse
+// window (bragg_ds.cpp:117-127), set on the host.
+template <typename R>
+__device__ __forceinline__ void bragg_ds_point(const NLArgs &a, cplx<R> *v, double x0) {
+  double rho[MAXC];
+  #pragma unroll
+  for (int j = 0; j < MAXC; j++) rho[j] = (double)v[j].x * (double)v[j].x + (double)v[j].y * (double)v[j].y;
+  double phi[MAXC];
+  #pragma unroll
+  for (int i = 0; i < MAXC; i++) {
+    double p = a.gs[i * MAXC] * rho[0];
+    #pragma unroll
+    for (int j = 1; j < MAXC; j++) p += a.gs[i * MAXC + j] * rho[j];
+    phi[i] = p + (((i < 2) ? a.L.beta0 : a.L2.beta0) * x0 - a.L.DeltaL[i]);
+  }
+  const double t1 = a.t1, dt = a.dt;
+  #pragma unroll
+  for (int s = 0; s < 2; s++) {
+    const LaserD &L = s ? a.L2 : a.L;
+    const double Omega = (s ? a.F2 : a.F) * L.Amp0 *
+                         cos(L.laser_k0 * x0 - (L.laser_domh0 + L.chirp_rate0 * t1) * t1 + L.phase0 / 2);
+    double es, ec;
+    sincos(-0.5 * (L.laser_dk0 * x0 + L.phase0), &es, &ec);
+    bragg_pair<R>(a.stable, dt, phi[2 * s], phi[2 * s + 1], Omega, ec, es, v[2 * s], v[2 * s + 1]);
+  }
+}
+
 // ------------------------------------------------------------ potential step
 // Point-wise potential step on the ncomp values v[] at grid index l.
 // FP64: the reference's formulas (include/CRT_Base.h:410-439,
@@ -261,6 +378,10 @@ __device__ __forceinline__ void nl_point(const NLArgs &a, cplx<R> *v, int64_t l,
   using C = cplx<R>;
   if (a.kind == K_DBRAGG) {
     dbragg_point<R>(a, v, l, x0);
+    return;
+  }
+  if (a.kind == K_BRAGG_DS) {
+    bragg_ds_point<R>(a, v, x0);
     return;
   }
   const int n = a.ncomp;
@@ -283,7 +404,9 @@ __device__ __forceinline__ void nl_point(const NLArgs &a, cplx<R> *v, int64_t l,
         #pragma unroll
         for (int j = 0; j < MAXC; j++)
           if (j < n) phi += a.gs[i * MAXC + j] * rho[j];
-        phi += a.L.beta0 * x0 - a.L.DeltaL[i];
+        // CRT_Base_IF_2 (two species): beta of the component's species
+        const double b = (a.kind == K_NL_IF2 && 2 * i >= n) ? a.L2.beta0 : a.L.beta0;
+        phi += b * x0 - a.L.DeltaL[i];
       }
       phi *= a.mdt;
       const double2 e = expi<R>(phi);
@@ -294,75 +417,7 @@ __device__ __forceinline__ void nl_point(const NLArgs &a, cplx<R> *v, int64_t l,
   // Bragg 2x2 (components 0 and 1)
   const double V11 = a.gs[0] * rho[0] + a.gs[1] * rho[1] + a.L.beta0 * x0;
   const double V22 = a.gs[MAXC] * rho[0] + a.gs[MAXC + 1] * rho[1] - a.L.DeltaL[1] + a.L.beta0 * x0;
-  const double dt = a.dt;
-  if constexpr (sizeof(R) == 8) {
-   if (!a.stable) {
-    double re1, im1;
-    if (Omega == 0.0) {
-      sincos_step(-dt * V11, &im1, &re1);
-      v[0] = cmul(v[0], make_double2(re1, im1));
-      sincos_step(-dt * V22, &im1, &re1);
-      v[1] = cmul(v[1], make_double2(re1, im1));
-      return;
-    }
-    double tmp1 = sqrt((V11 - V22) * (V11 - V22) + 4.0 * Omega * Omega);
-    const double Ep = 0.5 * (V11 + V22 + tmp1);
-    const double Em = 0.5 * (V11 + V22 - tmp1);
-    double2 gp, gm;
-    sincos_step(-dt * Ep, &im1, &re1);
-    tmp1 = 1.0 / fabs((V11 - Ep) * (V11 - Ep) + Omega * Omega);
-    gp = make_double2(tmp1 * re1, tmp1 * im1);
-    sincos_step(-dt * Em, &im1, &re1);
-    tmp1 = 1.0 / fabs((V11 - Em) * (V11 - Em) + Omega * Omega);
-    gm = make_double2(tmp1 * re1, tmp1 * im1);
-    const double O2 = Omega * Omega;
-    const double2 O11 = make_double2(O2 * (gp.x + gm.x), O2 * (gp.y + gm.y));
-    const double a1 = V11 - Ep, a2 = V11 - Em;
-    const double2 O22 = make_double2(a1 * a1 * gp.x + a2 * a2 * gm.x, a1 * a1 * gp.y + a2 * a2 * gm.y);
-    const double2 Os = make_double2(-Omega * (a1 * gp.x + a2 * gm.x), -Omega * (a1 * gp.y + a2 * gm.y));
-    const double2 eta = make_double2(eta_c, eta_s);
-    const double2 O12 = cmul(Os, eta);   // eta * O12
-    const double2 O21 = cmulc(Os, eta);  // conj(eta) * O21
-    const double2 p1 = v[0], p2 = v[1];
-    v[0] = cadd(cmul(O11, p1), cmul(O12, p2));
-    v[1] = cadd(cmul(O21, p1), cmul(O22, p2));
-    return;
-   }
-  }
-  {
-    // U = e^{-i dt m} [cos(r dt) I - i sin(r dt)/r [[d, W], [W, -d]]], m = (V11+V22)/2,
-    // d = (V11-V22)/2, W = Omega, r = sqrt(d^2 + W^2); off-diagonals times eta / conj(eta).
-    // The matrix is built in FP64 from unit (cos, sin) pairs, so it is unitary
-    // to FP64 accuracy for every Omega (the reference's eigen-form divides by
-    // (V11 - E)^2 + Omega^2, which loses unitarity once Omega is below the
-    // spacing of V and divides by zero once Omega^2 underflows).
-    const double m = 0.5 * (V11 + V22), d = 0.5 * (V11 - V22);
-    const double r = sqrt(d * d + Omega * Omega);
-    const double2 e = expi<R>(-dt * m);   // e^{-i dt m}
-    const double2 rr = expi<R>(dt * r);   // (cos r dt, sin r dt)
-    // sin(r dt) / r: Taylor series of sinc (truncation below 2^-72 for r dt <= 1/32)
-    const double xr = dt * r;
-    double sor;
-    if (xr <= 0.03125) {
-      const double x2 = xr * xr;
-      double p = fma(x2, 1.0 / 362880.0, -1.0 / 5040.0);
-      p = fma(p, x2, 1.0 / 120.0);
-      p = fma(p, x2, -1.0 / 6.0);
-      sor = dt * fma(p, x2, 1.0);
-    } else {
-      sor = rr.y / r;
-    }
-    const double fd = sor * d, fw = sor * Omega;
-    // U11 = e(cos - i fd), U22 = e(cos + i fd), Uoff = e(-i fw)
-    const double2 U11 = cmul(e, make_double2(rr.x, -fd));
-    const double2 U22 = cmul(e, make_double2(rr.x, fd));
-    const double2 Uo = cmul(e, make_double2(0.0, -fw));
-    const double2 et = make_double2(eta_c, eta_s);
-    const double2 U12 = cmul(Uo, et), U21 = cmulc(Uo, et);
-    const double2 p1 = to_d<R>(v[0]), p2 = to_d<R>(v[1]);
-    v[0] = from_d<R>(cadd(cmul(U11, p1), cmul(U12, p2)));
-    v[1] = from_d<R>(cadd(cmul(U21, p1), cmul(U22, p2)));
-  }
+  bragg_pair<R>(a.stable, a.dt, V11, V22, Omega, eta_c, eta_s, v[0], v[1]);
 }
 
 // Omega(x0) and eta(x0) of the Bragg step (bragg.cpp:224, 243).

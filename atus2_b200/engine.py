@@ -20,6 +20,7 @@ constructor raises.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 
 import numpy as np
@@ -30,7 +31,7 @@ LIB_PATH = os.path.join(HERE, "libatus_gpu.so")
 ATUS_OK = 0
 PREC_FP64 = 0
 PREC_MIXED = 1
-STEP_NL, STEP_NL_IF, STEP_BRAGG_AD, STEP_DOUBLE_BRAGG_AD = 0, 1, 2, 3
+STEP_NL, STEP_NL_IF, STEP_BRAGG_AD, STEP_DOUBLE_BRAGG_AD, STEP_NL_IF_2, STEP_BRAGG_DS_AD = 0, 1, 2, 3, 4, 5
 MAX_COMP = 4
 
 _ERRORS = {-1: "invalid argument", -2: "unsupported", -3: "CUDA error", -4: "bad state", -5: "out of device memory"}
@@ -99,6 +100,8 @@ SIGNATURES = {
     "atus_set_gs": (_i, [_vp, _dp]),
     "atus_set_potential": (_i, [_vp, _i, _dp]),
     "atus_set_laser": (_i, [_vp, C.POINTER(Laser)]),
+    "atus_set_laser2": (_i, [_vp, C.POINTER(Laser)]),
+    "atus_set_pulse_windows": (_i, [_vp, _d, _dp]),
     "atus_upload_psi": (_i, [_vp, _i, _dp]),
     "atus_download_psi": (_i, [_vp, _i, _dp]),
     "atus_device_psi": (_i, [_vp, _i, C.POINTER(C.c_void_p)]),
@@ -127,6 +130,7 @@ SIGNATURES = {
     "atus_expval_momentum": (_i, [_vp, _i, _dp]),
     "atus_setup_momentum": (_i, [_vp, _i, _dp]),
     "atus_rabi_integrals": (_i, [_vp, _dp, _i, _d, _dp]),
+    "atus_rabi_integrals_comp": (_i, [_vp, _i, _dp, _i, _d, _dp]),
     "atus_sob_init": (_i, [_vp, _dp, _d]),
     "atus_sob_renormalize": (_i, [_vp]),
     "atus_sob_iterate": (_i, [_vp, _i, _dp, _dp]),
@@ -275,6 +279,14 @@ class Solver:
     def set_laser(self, laser: Laser) -> None:
         self._ok(self._L.atus_set_laser(self._c, C.byref(laser)), "set_laser")
 
+    def set_species2(self, laser2: Laser, t_start: float = 0.0, durations=(math.inf, math.inf)) -> None:
+        """Second species of the two-species programs (laser parameters
+        Beta_2, Amp_2, laser_k_2, ...) and the pulse windows of their bragg_ad
+        (species s couples while t + dt/2 - t_start <= durations[s])."""
+        self._ok(self._L.atus_set_laser2(self._c, C.byref(laser2)), "set_laser2")
+        d = np.ascontiguousarray(durations, dtype=np.float64)
+        self._ok(self._L.atus_set_pulse_windows(self._c, float(t_start), _dptr(d)), "set_pulse_windows")
+
     def set_stream(self, stream_handle: int | None) -> None:
         self._ok(self._L.atus_set_stream(self._c, C.c_void_p(stream_handle or 0)), "set_stream")
 
@@ -334,11 +346,11 @@ class Solver:
         a[: len(p)] = p
         self._ok(self._L.atus_setup_momentum(self._c, comp, _dptr(a)), "setup_momentum")
 
-    def rabi_integrals(self, k0, thr: float) -> np.ndarray:
+    def rabi_integrals(self, k0, thr: float, comp: int = 0) -> np.ndarray:
         k = np.ascontiguousarray(k0, dtype=np.float64).reshape(-1, self.dim)
         out = np.zeros(k.shape[0])
-        self._ok(self._L.atus_rabi_integrals(self._c, _dptr(k), k.shape[0], float(thr), _dptr(out)),
-                 "rabi_integrals")
+        self._ok(self._L.atus_rabi_integrals_comp(self._c, int(comp), _dptr(k), k.shape[0], float(thr),
+                                                  _dptr(out)), "rabi_integrals")
         return out
 
     # ------------------------------------------------------------ Sobolev gradient

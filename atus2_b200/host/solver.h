@@ -2,7 +2,8 @@
 //
 // CRT_Base, CRT_Base_IF and CSOB_Base keep the public interface, the XML
 // semantics, the console output and the files of the reference's class
-// templates (include/CRT_Base.h, include/CRT_Base_IF.h, include/CSOB_Base.h),
+// templates (include/CRT_Base.h, include/CRT_Base_IF.h, include/CRT_Base_IF_2.h,
+// include/CSOB_Base.h),
 // while the fields live on the GPU: the step functions and the Strang block of
 // run_sequence go through the C ABI (include/atus_gpu.h).  A host copy of the
 // fields (Getp2In) is refreshed only when a file is written or a host-side step
@@ -640,6 +641,269 @@ class CRT_Base_IF : public CRT_Base<dim, no_int_states> {
   double m_rabi_threshold = 0;
   std::vector<CPoint<dim>> m_rabi_momentum_list;
   std::list<std::list<double>> m_rabi_freq_list, m_chirps_list;
+};
+
+// ============================================================== CRT_Base_IF_2
+// Two species of two internal states each (include/CRT_Base_2.h,
+// include/CRT_Base_IF_2.h): components [0, n/2) are species 1 with Alpha_1,
+// Beta and the laser constants, [n/2, n) species 2 with Alpha_2, Beta_2 and the
+// *_2 constants.  "freeprop" is CRT_Base_IF_2::Do_NL_Step (GPU kind
+// ATUS_STEP_NL_IF_2); "freeprop_lin" only takes the kinetic steps
+// (CRT_Base_2.h:283-286 is empty).
+template <int dim, int no_int_states>
+class CRT_Base_IF_2 : public CRT_Base<dim, no_int_states> {
+  using Base = CRT_Base<dim, no_int_states>;
+
+ public:
+  explicit CRT_Base_IF_2(ParameterHandler *params, int precision = ATUS_PREC_FP64) : Base(params, precision) {
+    // CRT_Base_2's constructor reads Alpha_2 after Init() as it reads Alpha_1
+    // (include/CRT_Base_2.h:125-129): the tables follow at the next Set_dt
+    for (int i = 0; i < dim; i++) m_alpha2[i] = this->m_params->Get_VConstant("Alpha_2", i);
+    for (int c = no_int_states / 2; c < no_int_states; c++)
+      gpu_check(this->m_gpu, atus_set_alpha(this->m_gpu, c, m_alpha2.data()), "set_alpha");
+    this->m_gpu_steps["freeprop"] = ATUS_STEP_NL_IF_2;
+    this->m_map_stepfcts["freeprop_lin"] = &Do_Nothing;
+    UpdateParams();
+  }
+
+  // CRT_Base_IF_2::run_sequence (include/CRT_Base_IF_2.h:420-593).
+  void run_sequence() override {
+    char filename[1024], filename2[1024];
+    std::cout << "FYI: Found " << this->m_params->m_sequence.size() << " sequences." << std::endl;
+    const int nrm = (int)m_rabi_momentum_list.size();
+    if (nrm == 0) std::cerr << "WARNING: Rabi momentum list is empty. Cannot compute rabi frquencies." << std::endl;
+    int seq_counter = 1;
+    for (auto seq : this->m_params->m_sequence) {
+      if (this->run_custom_sequence(seq)) continue;
+      if (seq.name == "set_momentum") {
+        this->set_momentum(seq);
+        continue;
+      }
+      double max_duration = 0;
+      for (double d : seq.duration)
+        if (d > max_duration) max_duration = d;
+      const int subN = int(max_duration / seq.dt);
+      const int Nk = seq.Nk;
+      const int Na = subN / seq.Nk;
+      seq.time = this->Get_t();
+      std::cout << "FYI: started new sequence " << seq.name << "\n";
+      std::cout << "FYI: sequence no : " << seq_counter << "\n";
+      std::cout << "FYI: duration    : " << max_duration << "\n";
+      std::cout << "FYI: dt          : " << seq.dt << "\n";
+      std::cout << "FYI: Na          : " << Na << "\n";
+      std::cout << "FYI: Nk          : " << Nk << "\n";
+      std::cout << "FYI: Na*Nk*dt    : " << double(Na * Nk) * seq.dt << "\n";
+      if (double(Na * Nk) * seq.dt != max_duration) std::cout << "FYI: double(Na*Nk)*seq.dt != max_duration\n";
+      if (this->Get_dt() != seq.dt) this->Set_dt(seq.dt);
+      if (!this->m_gpu_steps.count(seq.name) && !this->m_map_stepfcts.count(seq.name)) {
+        std::cerr << "Critical Error: Invalid squence name " << seq.name << "\n";
+        exit(EXIT_FAILURE);
+      }
+      if (seq.name == "freeprop") seq.no_of_chirps = 1;
+      const double backup_t = this->m_grid.h.t;
+      m_chirps_list.clear();
+      for (int s = 0; s < seq.no_of_chirps; ++s) {
+        m_rabi_freq_list.clear();
+        m_rabi_freq_list2.clear();
+        chirp_rate[0] = 0.0;
+        for (int i = 1; i <= Na; i++) {
+          this->strang_block(seq, Nk);
+          std::cout << "t = " << std::to_string(this->m_grid.h.t) << std::endl;
+          if (seq.output_freq == each) save_all();
+          if (seq.compute_pn_freq == each)
+            for (int c = 0; c < no_int_states; c++)
+              std::cout << "N[" << c << "] = " << this->Get_Particle_Number(c) << std::endl;
+          if (seq.rabi_output_freq == each) compute_rabi_integrals();
+          if (seq.custom_freq == each && this->m_custom_fct != nullptr) this->call_host(this->m_custom_fct, seq);
+        }
+        if (seq.output_freq == last) save_all();
+        if (seq.compute_pn_freq == last)
+          for (int c = 0; c < no_int_states; c++)
+            std::cout << "N[" << c << "] = " << this->Get_Particle_Number(c) << std::endl;
+        if (seq.custom_freq == last && this->m_custom_fct != nullptr) this->call_host(this->m_custom_fct, seq);
+        if (seq.rabi_output_freq == last) {
+          compute_rabi_integrals();
+          std::cout << "Spezie 1" << std::endl;
+          std::cout << "Rabi output for timestep ";
+          for (auto &row : m_rabi_freq_list) {
+            std::cout << this->Get_t() << "\n";
+            for (double v : row) std::cout << v << "\t";
+            std::cout << std::endl;
+          }
+          std::cout << "Spezie 2" << std::endl;
+          for (auto &row : m_rabi_freq_list2) {
+            std::cout << this->Get_t() << "\n";
+            for (double v : row) std::cout << v << "\t";
+            std::cout << std::endl;
+          }
+        }
+        if (seq.rabi_output_freq == each) {
+          snprintf(filename, sizeof filename, "Spezie_%d_Rabi_%d_%d.txt", 1, seq_counter, s);
+          snprintf(filename2, sizeof filename2, "Spezie_%d_Rabi_%d_%d.txt", 2, seq_counter, s);
+          Output_rabi_freq_list(filename, filename2, seq.Nk);
+        }
+        if (seq.no_of_chirps > 1 && nrm > 0) {
+          compute_rabi_integrals();
+          std::list<double> tmp = m_rabi_freq_list.back();
+          tmp.push_front(chirp_rate[0]);
+          tmp.push_front(s);
+          m_chirps_list.push_back(tmp);
+        }
+        // the scan restarts from the files of the sequence's start time; a
+        // file that does not open leaves the fields as they are
+        if (seq.no_of_chirps > 1 && s < seq.no_of_chirps - 1) {
+          this->sync_to_host();
+          for (int k = 0; k < no_int_states; k++) {
+            snprintf(filename, sizeof filename, "%.3f_%d.bin", backup_t, k + 1);
+            std::ifstream f(filename, std::ifstream::binary);
+            if (!f.is_open()) continue;
+            f.seekg(sizeof(generic_header), std::ifstream::beg);
+            f.read((char *)this->m_fields[k].data(), this->m_grid.npts * 16);
+          }
+          this->m_grid.h.t = backup_t;
+          this->sync_to_device();
+        }
+      }
+      if (seq.no_of_chirps > 1) {
+        snprintf(filename, sizeof filename, "Chirp_%d.txt", seq_counter);
+        Output_chirps_list(filename);
+      }
+      seq_counter++;
+    }
+  }
+
+ protected:
+  static void Do_Nothing(void *, sequence_item &) {}
+
+  // UpdateParams (include/CRT_Base_IF_2.h:80-113); phase, phase2 and
+  // chirp_rate2 are never set by the reference and stay 0.
+  void UpdateParams() {
+    for (int i = 0; i < dim; i++) {
+      beta[i] = this->m_params->Get_VConstant("Beta", i);
+      beta2[i] = this->m_params->Get_VConstant("Beta_2", i);
+    }
+    for (int i = 0; i < no_int_states; i++) DeltaL[i] = this->m_params->Get_VConstant("Delta_L", i);
+    try {
+      Amp[0] = this->m_params->Get_VConstant("Amp_1", 0);
+      Amp[1] = this->m_params->Get_VConstant("Amp_1", 1);
+      Amp2[0] = this->m_params->Get_VConstant("Amp_2", 0);
+      Amp2[1] = this->m_params->Get_VConstant("Amp_2", 1);
+      laser_k[0] = this->m_params->Get_Constant("laser_k");
+      laser_k2[0] = this->m_params->Get_Constant("laser_k_2");
+      laser_dk[0] = this->m_params->Get_Constant("laser_dk");
+      laser_dk2[0] = this->m_params->Get_Constant("laser_dk_2");
+      laser_domh[0] = this->m_params->Get_Constant("laser_domh");
+      laser_domh2[0] = this->m_params->Get_Constant("laser_domh_2");
+      m_rabi_threshold = this->m_params->Get_Constant("rabi_threshold");
+    } catch (std::string &str) {
+      std::cout << str << std::endl;
+    }
+  }
+
+  // Both species' lasers and the pulse windows of the sequence.  bragg_ds
+  // reads seq.duration[0] and [1] (bragg_ds.cpp:122-125); a sequence with a
+  // single duration uses it for both species.
+  void upload_step_parameters(const sequence_item &seq) override {
+    atus_laser L{}, L2{};
+    for (int i = 0; i < dim; i++) {
+      L.beta[i] = beta[i];
+      L2.beta[i] = beta2[i];
+    }
+    for (int i = 0; i < no_int_states; i++) L.DeltaL[i] = DeltaL[i];
+    for (int i = 0; i < 2; i++) {
+      L.Amp[i] = Amp[i];
+      L.laser_k[i] = laser_k[i];
+      L.laser_dk[i] = laser_dk[i];
+      L.laser_domh[i] = laser_domh[i];
+      L.phase[i] = phase[i];
+      L.chirp_rate[i] = chirp_rate[i];
+      L2.Amp[i] = Amp2[i];
+      L2.laser_k[i] = laser_k2[i];
+      L2.laser_dk[i] = laser_dk2[i];
+      L2.laser_domh[i] = laser_domh2[i];
+      L2.phase[i] = phase2[i];
+      L2.chirp_rate[i] = chirp_rate2[i];
+    }
+    gpu_check(this->m_gpu, atus_set_laser(this->m_gpu, &L), "set_laser");
+    gpu_check(this->m_gpu, atus_set_laser2(this->m_gpu, &L2), "set_laser2");
+    double dur[2] = {HUGE_VAL, HUGE_VAL};
+    if (!seq.duration.empty()) dur[0] = dur[1] = seq.duration[0];
+    if (seq.duration.size() > 1) dur[1] = seq.duration[1];
+    gpu_check(this->m_gpu, atus_set_pulse_windows(this->m_gpu, seq.time, dur), "set_pulse_windows");
+  }
+
+  void save_all() {
+    char filename[1024];
+    for (int k = 0; k < no_int_states; k++) {
+      snprintf(filename, sizeof filename, "%.3f_%d.bin", this->Get_t(), k + 1);
+      this->Save_Phi(filename, k);
+    }
+  }
+
+  // CRT_Base_IF_2::compute_rabi_integrals (include/CRT_Base_IF_2.h:115-210):
+  // species 1 on component 0, species 2 on component no_int_states/2.
+  void compute_rabi_integrals() {
+    const int n = (int)m_rabi_momentum_list.size(), m = (int)m_rabi_momentum_list2.size();
+    if (n == 0 || m == 0) {
+      std::cerr << "WARNING: Rabi momentum list is empty. Cannot compute rabi frquencies." << std::endl;
+      return;
+    }
+    std::vector<double> k0, k02, res(n), res2(m);
+    for (auto &p : m_rabi_momentum_list)
+      for (int a = 0; a < dim; a++) k0.push_back(p[a]);
+    for (auto &p : m_rabi_momentum_list2)
+      for (int a = 0; a < dim; a++) k02.push_back(p[a]);
+    gpu_check(this->m_gpu, atus_rabi_integrals_comp(this->m_gpu, 0, k0.data(), n, m_rabi_threshold, res.data()),
+              "rabi");
+    gpu_check(this->m_gpu,
+              atus_rabi_integrals_comp(this->m_gpu, no_int_states / 2, k02.data(), m, m_rabi_threshold, res2.data()),
+              "rabi");
+    m_rabi_freq_list.push_back(std::list<double>(res.begin(), res.end()));
+    m_rabi_freq_list2.push_back(std::list<double>(res2.begin(), res2.end()));
+  }
+
+  static void write_rabi(const std::string &filename, const std::vector<CPoint<dim>> &pts,
+                         const std::list<std::list<double>> &rows, double dt_out) {
+    std::ofstream txt(filename);
+    double t = 0;
+    txt << "# time \t";
+    for (auto &p : pts) {
+      for (int a = 0; a < dim; a++) txt << p[a] << ((a == dim - 1) ? "" : ",");
+      txt << "\t";
+    }
+    txt << std::endl;
+    for (auto &row : rows) {
+      txt << t << "\t";
+      for (double v : row) txt << v << "\t";
+      txt << std::endl;
+      t += dt_out;
+    }
+  }
+  void Output_rabi_freq_list(const std::string &filename, const std::string &filename2, long long Nk) {
+    write_rabi(filename, m_rabi_momentum_list, m_rabi_freq_list, this->m_grid.h.dt * double(Nk));
+    write_rabi(filename2, m_rabi_momentum_list2, m_rabi_freq_list2, this->m_grid.h.dt * double(Nk));
+  }
+  void Output_chirps_list(const std::string &filename) {
+    std::ofstream txt(filename);
+    txt << "# Step \t Chirp \t ";
+    for (auto &p : m_rabi_momentum_list) {
+      for (int a = 0; a < dim; a++) txt << p[a] << ((a == dim - 1) ? "" : ",");
+      txt << "\t";
+    }
+    txt << std::endl;
+    for (auto &row : m_chirps_list) {
+      for (double v : row) txt << v << "\t";
+      txt << std::endl;
+    }
+  }
+
+  CPoint<dim> m_alpha2{}, beta{}, beta2{};
+  std::array<double, no_int_states> DeltaL{};
+  std::array<double, 2> Amp{}, Amp2{}, laser_k{}, laser_k2{}, laser_dk{}, laser_dk2{}, laser_domh{}, laser_domh2{},
+      phase{}, phase2{}, chirp_rate{}, chirp_rate2{};
+  double m_rabi_threshold = 0;
+  std::vector<CPoint<dim>> m_rabi_momentum_list, m_rabi_momentum_list2;
+  std::list<std::list<double>> m_rabi_freq_list, m_rabi_freq_list2, m_chirps_list;
 };
 
 // ============================================================== CSOB_Base

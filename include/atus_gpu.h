@@ -85,6 +85,12 @@ extern "C" {
 #define ATUS_STEP_BRAGG_AD 2 /* "bragg_ad": analytic 2x2 Bragg exponential */
 #define ATUS_STEP_DOUBLE_BRAGG_AD 3 /* "bragg_ad" of double_bragg: three-level exponential,
                                        Bragg_double::Do_Double_Bragg_ad (double_bragg.cpp:100-258) */
+#define ATUS_STEP_NL_IF_2 4  /* "freeprop" of CRT_Base_IF_2 (two species, include/CRT_Base_IF_2.h:
+                                378-416): g|psi|^2 + beta_s x - DeltaL, beta_s of the component's
+                                species (atus_set_laser / atus_set_laser2) */
+#define ATUS_STEP_BRAGG_DS_AD 5 /* "bragg_ad" of bragg_ds: a 2x2 Bragg exponential per species,
+                                   components (0,1) and (2,3), Bragg_single::Do_Bragg_ad
+                                   (bragg_ds.cpp:111-322) */
 
 #define ATUS_MAX_COMP 4
 
@@ -135,6 +141,17 @@ ATUS_API int atus_set_gs(atus_ctx *ctx, const double *gs /* ncomp*ncomp, row i =
 /* V: N doubles in grid order, or NULL to drop the potential of comp. */
 ATUS_API int atus_set_potential(atus_ctx *ctx, int comp, const double *V);
 ATUS_API int atus_set_laser(atus_ctx *ctx, const atus_laser *laser);
+/* The second species of the two-species programs (CRT_Base_IF_2::UpdateParams,
+ * include/CRT_Base_IF_2.h:80-113: Beta_2, Amp_2, laser_k_2, laser_dk_2,
+ * laser_domh_2 and the members phase2, chirp_rate2); element 0 of each array is
+ * used.  DeltaL of all four components stays with atus_set_laser. */
+ATUS_API int atus_set_laser2(atus_ctx *ctx, const atus_laser *laser2);
+/* Pulse windows of ATUS_STEP_BRAGG_DS_AD (bragg_ds.cpp:114-127): with t1 = t +
+ * dt/2 at the potential step, species s couples while t1 - t_start <=
+ * duration[s] and only takes its phases afterwards.  t_start is the sequence's
+ * start time (seq.time = Get_t(), include/CRT_Base_IF_2.h:466).  Default: no
+ * window (duration = +inf). */
+ATUS_API int atus_set_pulse_windows(atus_ctx *ctx, double t_start, const double *duration /* 2 */);
 /* on = 1: FP64 contexts take the bragg_ad step in the eigenvalue-free form
  * U = e^{-i dt m}[cos(r dt) - i sin(r dt)/r (H - m)] (complex64 contexts always
  * do).  No counterpart in the reference: its eigen-form (bragg.cpp:254-277)
@@ -201,6 +218,10 @@ ATUS_API int atus_expval_momentum(atus_ctx *ctx, int comp, double *out /* dim */
 ATUS_API int atus_setup_momentum(atus_ctx *ctx, int comp, const double *p /* dim */);
 /* n momentum points k0 (n*dim), threshold thr: m_ar_k * sum |psi0^(k)|^2 per ball. */
 ATUS_API int atus_rabi_integrals(atus_ctx *ctx, const double *k0, int n, double thr, double *out);
+/* The same on component comp: the second species' sums of
+ * CRT_Base_IF_2::compute_rabi_integrals (include/CRT_Base_IF_2.h:115-210) use
+ * component no_int_states/2. */
+ATUS_API int atus_rabi_integrals_comp(atus_ctx *ctx, int comp, const double *k0, int n, double thr, double *out);
 
 /* ------------------------------------------------------------ Sobolev gradient */
 /* Ground-state descent of CSOB_Base on the context's grid: alpha per

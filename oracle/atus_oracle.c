@@ -22,6 +22,12 @@
  *   orc_bragg_ad              source/interferometry/src/bragg.cpp:185-304 (Do_Bragg_ad)
  *   orc_double_bragg_ad       source/interferometry/src/double_bragg.cpp:100-258
  *                             (Bragg_double::Do_Double_Bragg_ad)
+ *   orc_nl_if2_step           include/CRT_Base_IF_2.h:378-416 (freeprop of the
+ *                             two-species programs)
+ *   orc_bragg_ds_ad           source/interferometry/src/bragg_ds.cpp:111-322
+ *                             (Bragg_single::Do_Bragg_ad of bragg_ds)
+ *   orc_rabi_integrals_comp   include/CRT_Base_IF_2.h:115-210 (species 2 on
+ *                             component no_int_states/2)
  *   orc_block                 include/CRT_Base.h:776-786 / CRT_Base_IF.h:779-789
  *   orc_particle_number       include/CRT_Base.h:586-599
  *   orc_expval_position/momentum include/CRT_Base.h:480-580
@@ -78,6 +84,10 @@ typedef struct {
   double *lap[ORC_MAXC], *sob[ORC_MAXC], *grad[ORC_MAXC];
   double *op[ORC_MAXC], *op2[ORC_MAXC];
   double stepsize;
+  /* second species of the two-species programs and the pulse windows of
+   * their bragg_ad (seq.time, seq.duration[0..1]) */
+  orc_laser L2;
+  double win_t0, win_dur[2];
 } orc_ctx;
 
 /* ------------------------------------------------------------------ grid */
@@ -153,6 +163,7 @@ orc_ctx *orc_create(int dim, int ncomp, const long long *n, const double *d, con
   c->bwd = orc_fft_plan_create(dim, nn, +1);
   for (int i = 0; i < ncomp; i++) c->psi[i] = (double *)calloc((size_t)c->npts * 2, sizeof(double));
   c->dt = 0.001;
+  c->win_dur[0] = c->win_dur[1] = HUGE_VAL;
   return c;
 }
 
@@ -484,13 +495,147 @@ void orc_double_bragg_ad(orc_ctx *c, const orc_laser *L, double F) {
   }
 }
 
+/* ------------------------------------------------- two-species programs */
+
+void orc_set_species2(orc_ctx *c, const orc_laser *L2, double t_start, const double *duration) {
+  c->L2 = *L2;
+  c->win_t0 = t_start;
+  c->win_dur[0] = duration[0];
+  c->win_dur[1] = duration[1];
+}
+
+/* CRT_Base_IF_2::Do_NL_Step: species 1 = components [0, n/2) with Beta,
+ * species 2 = [n/2, n) with Beta_2; phi_i += beta_s x - DeltaL_i as one
+ * right-hand side, then *= -dt.  The reference loop is serial. */
+void orc_nl_if2_step(orc_ctx *c, const orc_laser *L) {
+  const double dt = -c->dt;
+  const int n = c->ncomp;
+  for (long l = 0; l < c->npts; l++) {
+    double phi[ORC_MAXC];
+    for (int i = 0; i < n; i++) {
+      phi[i] = 0;
+      for (int j = 0; j < n; j++) {
+        const double *P = c->psi[j];
+        phi[i] += c->gs[j + n * i] * (P[2 * l] * P[2 * l] + P[2 * l + 1] * P[2 * l + 1]);
+      }
+      double x[3];
+      orc_get_x(c, l, x);
+      const double b = (i < n / 2) ? L->beta[0] : c->L2.beta[0];
+      phi[i] += b * x[0] - L->DeltaL[i];
+      phi[i] *= dt;
+    }
+    apply_phases(c, l, phi);
+  }
+}
+
+/* complex products as GCC evaluates std::complex<double> without fused
+ * multiply-adds: (a + ib)(c + id) = (ac - bd) + i(ad + bc) */
+static inline void zmul(double ar, double ai, double br, double bi, double *r, double *i) {
+  *r = ar * br - ai * bi;
+  *i = ar * bi + ai * br;
+}
+
+/* One species' 2x2 step of bragg_ds.cpp:215-248 on (P, Q) at point l: the
+ * eigen-form with complex d0, d1 (imaginary parts zero, so the products
+ * reduce to real-times-complex), gamma = e^{-i dt E} / |d^2 + Omega^2| as a
+ * complex-by-real division, M01 = ((-Omega) eta) tmp, M10 = ((-Omega)
+ * conj(eta)) tmp. */
+static void ds_pair(double *P, double *Q, long l, double V11, double V22, double Omega, double er, double ei,
+                    double dt) {
+  const double tmp1 = sqrt((V11 - V22) * (V11 - V22) + 4.0 * Omega * Omega);
+  const double Ep = 0.5 * (V11 + V22 + tmp1);
+  const double Em = 0.5 * (V11 + V22 - tmp1);
+  const double d0 = V11 - Ep, d1 = V11 - Em;
+  double s, co;
+  sincos(-dt * Ep, &s, &co);
+  const double n0 = fabs(d0 * d0 + Omega * Omega);
+  const double g0r = co / n0, g0i = s / n0;
+  sincos(-dt * Em, &s, &co);
+  const double n1 = fabs(d1 * d1 + Omega * Omega);
+  const double g1r = co / n1, g1i = s / n1;
+  const double tr = d0 * g0r + d1 * g1r, ti = d0 * g0i + d1 * g1i;
+  const double O2 = Omega * Omega;
+  const double M00r = O2 * (g0r + g1r), M00i = O2 * (g0i + g1i);
+  double M01r, M01i, M10r, M10i;
+  zmul(-Omega * er, -Omega * ei, tr, ti, &M01r, &M01i);
+  zmul(-Omega * er, -Omega * (-ei), tr, ti, &M10r, &M10i);
+  const double q0 = d0 * d0, q1 = d1 * d1;
+  const double M11r = q0 * g0r + q1 * g1r, M11i = q0 * g0i + q1 * g1i;
+  const double a0r = P[2 * l], a0i = P[2 * l + 1], a1r = Q[2 * l], a1i = Q[2 * l + 1];
+  double xr, xi, yr, yi;
+  zmul(M00r, M00i, a0r, a0i, &xr, &xi);
+  zmul(M01r, M01i, a1r, a1i, &yr, &yi);
+  P[2 * l] = xr + yr;
+  P[2 * l + 1] = xi + yi;
+  zmul(M10r, M10i, a0r, a0i, &xr, &xi);
+  zmul(M11r, M11i, a1r, a1i, &yr, &yi);
+  Q[2 * l] = xr + yr;
+  Q[2 * l + 1] = xi + yi;
+}
+
+static void ds_phase(double *P, long l, double phi, double dt) {
+  double re1, im1;
+  sincos(-phi * dt, &im1, &re1);
+  const double tmp1 = P[2 * l];
+  P[2 * l] = tmp1 * re1 - P[2 * l + 1] * im1;
+  P[2 * l + 1] = tmp1 * im1 + P[2 * l + 1] * re1;
+}
+
+/* Bragg_single::Do_Bragg_ad of bragg_ds.  F multiplies both pulse flags
+ * (mode1, mode2; 1 reproduces the reference). */
+void orc_bragg_ds_ad(orc_ctx *c, const orc_laser *L, double F) {
+  const double dt = c->dt;
+  const double t1 = c->t + 0.5 * dt;
+  const orc_laser *L2 = &c->L2;
+  int mode1 = 1, mode2 = 1;
+  const double time = t1 - c->win_t0;
+  if (time > c->win_dur[0]) mode1 = 0;
+  if (time > c->win_dur[1]) mode2 = 0;
+  double *P[4] = {c->psi[0], c->psi[1], c->psi[2], c->psi[3]};
+  #pragma omp parallel for schedule(static)
+  for (long l = 0; l < c->npts; l++) {
+    double x[3];
+    orc_get_x(c, l, x);
+    double phi[4];
+    for (int i = 0; i < 4; i++) {
+      phi[i] = 0;
+      for (int j = 0; j < 4; j++)
+        phi[i] += c->gs[j + 4 * i] * (P[j][2 * l] * P[j][2 * l] + P[j][2 * l + 1] * P[j][2 * l + 1]);
+      phi[i] += ((i < 2) ? L->beta[0] : L2->beta[0]) * x[0] - L->DeltaL[i];
+    }
+    const double Omega = (mode1 * F) * L->Amp[0] *
+                         cos(L->laser_k[0] * x[0] - (L->laser_domh[0] + L->chirp_rate[0] * t1) * t1 + L->phase[0] / 2);
+    const double Omega2 = (mode2 * F) * L2->Amp[0] *
+                          cos(L2->laser_k[0] * x[0] - (L2->laser_domh[0] + L2->chirp_rate[0] * t1) * t1 +
+                              L2->phase[0] / 2);
+    double er, ei;
+    if (Omega == 0.0) {
+      ds_phase(P[0], l, phi[0], dt);
+      ds_phase(P[1], l, phi[1], dt);
+    } else {
+      sincos(-0.5 * (L->laser_dk[0] * x[0] + L->phase[0]), &ei, &er);
+      ds_pair(P[0], P[1], l, phi[0], phi[1], Omega, er, ei, dt);
+    }
+    if (Omega2 == 0.0) {
+      ds_phase(P[2], l, phi[2], dt);
+      ds_phase(P[3], l, phi[3], dt);
+    } else {
+      sincos(-0.5 * (L2->laser_dk[0] * x[0] + L2->phase[0]), &ei, &er);
+      ds_pair(P[2], P[3], l, phi[2], phi[3], Omega2, er, ei, dt);
+    }
+  }
+}
+
 /* Step kinds: 0 = CRT_Base freeprop, 1 = CRT_Base_IF freeprop, 2 = bragg_ad,
- * 3 = bragg_ad of the three-level double_bragg program. */
+ * 3 = bragg_ad of the three-level double_bragg program, 4 = CRT_Base_IF_2
+ * freeprop, 5 = bragg_ad of the two-species bragg_ds program. */
 static void nl_dispatch(orc_ctx *c, int kind, const orc_laser *L, double F) {
   if (kind == 0) orc_nl_step(c);
   else if (kind == 1) orc_nl_if_step(c, L);
   else if (kind == 2) orc_bragg_ad(c, L, F);
-  else orc_double_bragg_ad(c, L, F);
+  else if (kind == 3) orc_double_bragg_ad(c, L, F);
+  else if (kind == 4) orc_nl_if2_step(c, L);
+  else orc_bragg_ds_ad(c, L, F);
 }
 
 /* One outer iteration of run_sequence: half, (V, full)^(Nk-1), V, half.
@@ -556,8 +701,8 @@ void orc_setup_momentum(orc_ctx *c, int comp, const double *p) {
 
 /* k0: n points of dim coordinates.  The bin index advances only when a point
  * lies outside a ball, exactly as the reference loop (CRT_Base_IF.h:244-255). */
-void orc_rabi_integrals(orc_ctx *c, const double *k0, int n, double thr, double *out) {
-  double *P = c->psi[0];
+void orc_rabi_integrals_comp(orc_ctx *c, int comp, const double *k0, int n, double thr, double *out) {
+  double *P = c->psi[comp];
   for (int j = 0; j < n; j++) out[j] = 0.0;
   orc_ft(c, P, -1);
   for (long l = 0; l < c->npts; l++) {
@@ -579,6 +724,10 @@ void orc_rabi_integrals(orc_ctx *c, const double *k0, int n, double thr, double 
   }
   for (int j = 0; j < n; j++) out[j] = c->ar_k * out[j];
   orc_ft(c, P, +1);
+}
+
+void orc_rabi_integrals(orc_ctx *c, const double *k0, int n, double thr, double *out) {
+  orc_rabi_integrals_comp(c, 0, k0, n, thr, out);
 }
 
 /* -------------------------------------------------------------- sobmin */

@@ -23,6 +23,9 @@ REF_DIR = os.path.join(HERE, "_ref")
 KIND_NL = 0  # CRT_Base::Do_NL_Step (rt_solver "freeprop")
 KIND_NL_IF = 1  # CRT_Base_IF::Do_NL_Step (bragg "freeprop")
 KIND_BRAGG_AD = 2  # Bragg_single::Do_Bragg_ad
+KIND_DOUBLE_BRAGG_AD = 3  # Bragg_double::Do_Double_Bragg_ad (double_bragg)
+KIND_NL_IF_2 = 4  # CRT_Base_IF_2::Do_NL_Step (two-species "freeprop")
+KIND_BRAGG_DS_AD = 5  # Bragg_single::Do_Bragg_ad of bragg_ds
 
 
 class Laser(C.Structure):
@@ -93,6 +96,8 @@ def lib():
             "orc_expval_momentum": (None, [vp, i, dp]),
             "orc_setup_momentum": (None, [vp, i, dp]),
             "orc_rabi_integrals": (None, [vp, dp, i, d, dp]),
+            "orc_rabi_integrals_comp": (None, [vp, i, dp, i, d, dp]),
+            "orc_set_species2": (None, [vp, C.POINTER(Laser), d, dp]),
             "orc_ft": (None, [vp, dp, i]),
             "orc_fft_raw": (None, [vp, dp, i]),
             "orc_sob_init": (None, [vp, dp, d]),
@@ -215,11 +220,17 @@ class Oracle:
         a[: len(p)] = p
         lib().orc_setup_momentum(self._c, comp, _dp(a))
 
-    def rabi_integrals(self, k0, thr: float) -> np.ndarray:
+    def rabi_integrals(self, k0, thr: float, comp: int = 0) -> np.ndarray:
         k = np.ascontiguousarray(k0, dtype=np.float64).reshape(-1, self.dim)
         out = np.zeros(k.shape[0])
-        lib().orc_rabi_integrals(self._c, _dp(k), k.shape[0], float(thr), _dp(out))
+        lib().orc_rabi_integrals_comp(self._c, int(comp), _dp(k), k.shape[0], float(thr), _dp(out))
         return out
+
+    def set_species2(self, laser2: Laser, t_start: float = 0.0, durations=(np.inf, np.inf)) -> None:
+        """Second species of CRT_Base_IF_2 and the pulse windows of bragg_ds's
+        bragg_ad (seq.time and seq.duration[0..1])."""
+        dur = np.ascontiguousarray(durations, dtype=np.float64)
+        lib().orc_set_species2(self._c, C.byref(laser2), float(t_start), _dp(dur))
 
     def ft(self, data: np.ndarray, isign: int) -> None:
         """cft_Nd::ft on an external complex array (in place)."""

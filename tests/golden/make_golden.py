@@ -1,6 +1,7 @@
 """Generates the golden fixtures in this folder from the reference programs.
 
-Runs ATUS-2's own ``rt_solver``, ``bragg`` and ``sobmin`` (built unmodified
+Runs ATUS-2's own ``rt_solver``, ``bragg``, ``double_bragg``, ``bragg_ds`` and
+``sobmin`` (built unmodified
 from the ATUS-2 sources by ``make -C oracle ref``) single-threaded on small
 seeded inputs, and stores inputs and outputs as ``<case>.npz``.  The CPU tests
 replay every case on the oracle restatement and require bit-identical results;
@@ -110,6 +111,22 @@ DBRAGG_CASES = [
          Beta=[0.0, 0.02, 0.03]),
 ]
 
+# two species (bragg_ds): g is the 4 x 4 matrix row by row (GS_1..GS_4)
+_G4 = [100.0, 90.0, 20.0, 15.0, 90.0, 95.0, 15.0, 20.0, 20.0, 15.0, 80.0, 70.0, 15.0, 20.0, 70.0, 75.0]
+BRAGGDS_CASES = [
+    dict(name="braggds1d", dim=1, n=[256], lo=[-32.0], hi=[32.0], laser_k=2.0, laser_k_2=1.5, laser_domh=8.0,
+         laser_domh_2=4.5, laser_dk=0.2, laser_dk_2=0.3, Amp=4.0, Amp_2=3.0, durations=[0.0305, 0.0505], g=_G4,
+         Delta_L=[0.0, 0.3, 0.0, -0.2], Beta=[0.05], Beta_2=[-0.03], Alpha_2=0.35),
+    dict(name="braggds2d", dim=2, n=[64, 32], lo=[-16.0, -8.0], hi=[16.0, 8.0], laser_k=2.0, laser_k_2=1.5,
+         laser_domh=8.0, laser_domh_2=4.5, laser_dk=0.2, laser_dk_2=0.3, Amp=4.0, Amp_2=3.0,
+         durations=[0.0505, 0.0305], g=_G4, Delta_L=[0.0, 0.5, 0.1, 0.4], Beta=[0.1, 0.0], Beta_2=[0.02, 0.0],
+         Alpha_2=0.35),
+    dict(name="braggds3d", dim=3, n=[16, 8, 16], lo=[-8.0, -4.0, -8.0], hi=[8.0, 4.0, 8.0], laser_k=1.5,
+         laser_k_2=1.0, laser_domh=4.0, laser_domh_2=2.0, laser_dk=0.0, laser_dk_2=0.1, Amp=4.0, Amp_2=3.0,
+         durations=[0.0305, 0.0505], g=_G4, Delta_L=[0.0, 0.0, 0.0, 0.0], Beta=[0.0, 0.0, 0.0],
+         Beta_2=[0.01, 0.0, 0.0], Alpha_2=0.35),
+]
+
 SOB_CASES = [
     dict(name="sob1d", dim=1, n=[64], lo=[-8.0], hi=[8.0], g=50.0, Nparticles=1.0, alpha=0.5, stepsize=0.01,
          epsilon=1e-7, V_expr="0.5*x*x", guess_expr="exp(-0.5*x*x)"),
@@ -136,9 +153,12 @@ def run(prog, cwd):
 
 
 def seq_xml(seq, extra=""):
+    def dur(d):
+        return ",".join(repr(float(v)) for v in d) if isinstance(d, (list, tuple)) else repr(d)
+
     return "".join(
         f'<{s["name"]} dt="{s["dt"]!r}" Nk="{s["Nk"]}" output_freq="each" pn_freq="each"{extra if s.get("rabi") else ""}>'
-        f'{s["duration"]!r}</{s["name"]}>' for s in seq)
+        f'{dur(s["duration"])}</{s["name"]}>' for s in seq)
 
 
 def collect_outputs(cwd, ncomp, seq):
@@ -308,6 +328,79 @@ def make_dbragg(case, tmp):
                 params=json.dumps(params), xml=xml)
 
 
+def make_bragg_ds(case, tmp):
+    """The two-species program (bragg_ds): species 1 in components 1-2,
+    species 2 in 3-4, a Thomas-Fermi-like profile with noise in the first
+    state of each species; bragg_ad with one pulse window per species, then
+    freeprop."""
+    rng = np.random.default_rng(3)
+    dim = case["dim"]
+    h = binfmt.make_header(dim, case["n"], case["lo"], case["hi"], dt=0.001)
+    X = grid(h)
+    r2 = sum(x * x for x in X)
+    psi1 = np.sqrt(np.maximum(0.0, 1.0 - 0.1 * r2)) * (1 + 0.01 * rng.standard_normal(r2.shape))
+    psi3 = np.sqrt(np.maximum(0.0, 0.8 - 0.12 * r2)) * (1 + 0.01 * rng.standard_normal(r2.shape))
+    psi1, psi3 = psi1.astype(np.complex128), psi3.astype(np.complex128)
+    zero = np.zeros_like(psi1)
+    psi0 = np.stack([psi1, zero, psi3, zero])
+    for k in range(4):
+        binfmt.write_bin(os.path.join(tmp, f"inp_{k + 1}.bin"), h, psi0[k])
+    seq = [dict(name="bragg_ad", dt=0.001, Nk=10, duration=list(case["durations"]), rabi=True),
+           dict(name="freeprop", dt=0.001, Nk=20, duration=0.04, rabi=True)]
+    g = case["g"]
+    gs_xml = "".join(f"<GS_{i + 1}>{xml_vec(g[4 * i:4 * i + 4])}</GS_{i + 1}>" for i in range(4))
+    xml = f"""<SIMULATION>
+  <DIM>{dim}</DIM>
+  <FILENAME>inp_1.bin</FILENAME>
+  <FILENAME_2>inp_2.bin</FILENAME_2>
+  <FILENAME_3>inp_3.bin</FILENAME_3>
+  <FILENAME_4>inp_4.bin</FILENAME_4>
+  <CONSTANTS>
+    <laser_k>{case['laser_k']!r}</laser_k><laser_k_2>{case['laser_k_2']!r}</laser_k_2>
+    <laser_dk>{case['laser_dk']!r}</laser_dk><laser_dk_2>{case['laser_dk_2']!r}</laser_dk_2>
+    <laser_domh>{case['laser_domh']!r}</laser_domh><laser_domh_2>{case['laser_domh_2']!r}</laser_domh_2>
+    <rabi_threshold>1.0</rabi_threshold>
+  </CONSTANTS>
+  <VCONSTANTS>
+    <Amp_1>{case['Amp']!r},{case['Amp']!r}</Amp_1>
+    <Amp_2>{case['Amp_2']!r},{case['Amp_2']!r}</Amp_2>
+    <Alpha_1>{xml_vec([0.5] * dim)}</Alpha_1>
+    <Alpha_2>{xml_vec([case['Alpha_2']] * dim)}</Alpha_2>
+    <Delta_L>{xml_vec(case['Delta_L'])}</Delta_L>
+    {gs_xml}
+    <Beta>{xml_vec(case['Beta'])}</Beta>
+    <Beta_2>{xml_vec(case['Beta_2'])}</Beta_2>
+  </VCONSTANTS>
+  <ALGORITHM><DT>1</DT></ALGORITHM>
+  <SEQUENCE>{seq_xml(seq, ' rabi_output_freq="each"')}</SEQUENCE>
+</SIMULATION>"""
+    open(os.path.join(tmp, "run.xml"), "w").write(xml)
+    run("bragg_ds", tmp)
+    t, psi = collect_outputs(tmp, 4, seq)
+    rabi = []
+    for s in (1, 2):
+        rows = []
+        for sp in (1, 2):
+            fn = os.path.join(tmp, f"Spezie_{sp}_Rabi_{s}_0.txt")
+            rows.append([[float(v) for v in ln.split()[1:]] for ln in open(fn) if not ln.startswith("#") and ln.split()])
+        rabi += [r1 + r2 for r1, r2 in zip(*rows)]
+    k0 = np.zeros((3, dim))
+    k0[1, 0] = 2 * case["laser_k"]
+    k0[2, 0] = -2 * case["laser_k"]
+    k02 = np.zeros((3, dim))
+    k02[1, 0] = 2 * case["laser_k_2"]
+    k02[2, 0] = -2 * case["laser_k_2"]
+    params = dict(program="bragg_ds", dim=dim, ncomp=4, header_dt=0.001, algo_dt=1.0, Alpha_1=[0.5] * dim,
+                  Alpha_2=[case["Alpha_2"]] * dim, gs=g, sequence=seq,
+                  laser_k=case["laser_k"], laser_domh=case["laser_domh"], laser_dk=case["laser_dk"], chirp=0.0,
+                  laser_k_2=case["laser_k_2"], laser_domh_2=case["laser_domh_2"], laser_dk_2=case["laser_dk_2"],
+                  Amp_1=[case["Amp"], case["Amp"]], Amp_2=[case["Amp_2"], case["Amp_2"]],
+                  Delta_L=case["Delta_L"], Beta=case["Beta"], Beta_2=case["Beta_2"],
+                  rabi_threshold=1.0, rabi_k0=k0.tolist(), rabi_k0_2=k02.tolist())
+    return dict(header=h.tobytes(), psi0=psi0, t=t, psi=psi, rabi=np.array(rabi), params=json.dumps(params),
+                xml=xml)
+
+
 def make_sob(case, tmp):
     dim = case["dim"]
     ax = "XYZ"[:dim]
@@ -334,13 +427,14 @@ def make_sob(case, tmp):
 
 
 def main():
-    if not os.path.exists(os.path.join(REF, "double_bragg")):
+    if not os.path.exists(os.path.join(REF, "bragg_ds")):
         subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
     only = set(sys.argv[1:])
     keep = (lambda c: not only or c["name"] in only)
-    global CASES, BRAGG_CASES, DBRAGG_CASES, SOB_CASES
+    global CASES, BRAGG_CASES, DBRAGG_CASES, BRAGGDS_CASES, SOB_CASES
     CASES, BRAGG_CASES = [c for c in CASES if keep(c)], [c for c in BRAGG_CASES if keep(c)]
     DBRAGG_CASES, SOB_CASES = [c for c in DBRAGG_CASES if keep(c)], [c for c in SOB_CASES if keep(c)]
+    BRAGGDS_CASES = [c for c in BRAGGDS_CASES if keep(c)]
     for case in CASES:
         with tempfile.TemporaryDirectory() as tmp:
             d = make_rt(case, tmp)
@@ -354,6 +448,11 @@ def main():
     for case in DBRAGG_CASES:
         with tempfile.TemporaryDirectory() as tmp:
             d = make_dbragg(case, tmp)
+        np.savez_compressed(os.path.join(HERE, case["name"] + ".npz"), **d)
+        print("wrote", case["name"], d["psi"].shape, d["rabi"].shape)
+    for case in BRAGGDS_CASES:
+        with tempfile.TemporaryDirectory() as tmp:
+            d = make_bragg_ds(case, tmp)
         np.savez_compressed(os.path.join(HERE, case["name"] + ".npz"), **d)
         print("wrote", case["name"], d["psi"].shape, d["rabi"].shape)
     for case in SOB_CASES:

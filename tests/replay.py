@@ -17,7 +17,7 @@ import math
 
 import numpy as np
 
-KIND_NL, KIND_NL_IF, KIND_BRAGG_AD, KIND_DOUBLE_BRAGG_AD = 0, 1, 2, 3
+KIND_NL, KIND_NL_IF, KIND_BRAGG_AD, KIND_DOUBLE_BRAGG_AD, KIND_NL_IF_2, KIND_BRAGG_DS_AD = 0, 1, 2, 3, 4, 5
 
 
 def gaussian_pulse(tc: float, two_sigma2: float):
@@ -30,19 +30,22 @@ def gaussian_pulse(tc: float, two_sigma2: float):
     return F
 
 
-def laser_kwargs(p: dict) -> dict:
+def laser_kwargs(p: dict, species: int = 1) -> dict:
+    """Laser members of CRT_Base_IF (or, species 2, the *_2 members of
+    CRT_Base_IF_2: Beta_2, Amp_2, laser_k_2, laser_dk_2, laser_domh_2)."""
     dim = p["dim"]
-    beta = list(p.get("Beta", [0.0] * dim)) + [0.0] * (3 - dim)
+    sfx = "" if species == 1 else "_2"
+    beta = list(p.get("Beta" + sfx, [0.0] * dim)) + [0.0] * (3 - dim)
     return dict(
         beta=beta,
         DeltaL=(list(p.get("Delta_L", [0.0, 0.0])) + [0.0] * 4)[:4],
-        Amp=p.get("Amp_1", [0.0, 0.0]),
-        laser_k=[p.get("laser_k", 0.0), 0.0],
-        laser_dk=[p.get("laser_dk", 0.0), 0.0],
-        laser_domh=[p.get("laser_domh", 0.0), 0.0],
+        Amp=p.get("Amp_1" if species == 1 else "Amp_2", [0.0, 0.0]),
+        laser_k=[p.get("laser_k" + sfx, 0.0), 0.0],
+        laser_dk=[p.get("laser_dk" + sfx, 0.0), 0.0],
+        laser_domh=[p.get("laser_domh" + sfx, 0.0), 0.0],
         phase=[0.0, 0.0],
         chirp_rate=[0.0, 0.0],
-        chirp=p.get("chirp", 0.0),
+        chirp=p.get("chirp", 0.0) if species == 1 else 0.0,
     )
 
 
@@ -52,36 +55,49 @@ def run_rt(engine, p: dict, psi0, V=None, make_laser=None, on_block=None):
     p keys: dim, ncomp, header_dt (dt stored in the input file), algo_dt
     (ALGORITHM/DT), Alpha_1, gs (flat ncomp^2), sequence = list of dicts
     {name, dt, Nk, duration}, optional AMP_T pulse {tc, two_sigma2}, program
-    ('rt_solver', 'bragg' or 'double_bragg').  Returns the list of (t, [psi per comp]) after
-    every block, and the Rabi sums per block when the program is bragg.
+    ('rt_solver', 'bragg', 'double_bragg' or 'bragg_ds'; bragg_ds adds Alpha_2 and
+    the *_2 laser keys).  Returns the list of (t, [psi per comp]) after every
+    block, and the Rabi sums per block of the interferometry programs (both
+    species side by side for bragg_ds).
     """
     ncomp = p["ncomp"]
+    two_species = p["program"] == "bragg_ds"
     for c in range(ncomp):
         engine.set_psi(c, psi0[c])
     engine.set_dt(p["header_dt"])  # Init() inside the constructor, alpha still zero
     for c in range(ncomp):
-        engine.set_alpha(c, p["Alpha_1"])
+        # CRT_Base_2: Alpha_2 for the second species (components ncomp/2 ..)
+        engine.set_alpha(c, p["Alpha_2"] if two_species and 2 * c >= ncomp else p["Alpha_1"])
     engine.set_gs(np.asarray(p["gs"], dtype=np.float64))
     cur_dt = p["algo_dt"]
     if V is not None:
         engine.set_potential(0, V)
     laser = make_laser(**laser_kwargs(p)) if make_laser is not None else None
+    laser2 = make_laser(**laser_kwargs(p, 2)) if make_laser is not None and two_species else None
     F = gaussian_pulse(p["AMP_T"]["tc"], p["AMP_T"]["two_sigma2"]) if p.get("AMP_T") else None
     outputs, rabi = [], []
-    is_if = p["program"] in ("bragg", "double_bragg")
+    is_if = p["program"] in ("bragg", "double_bragg", "bragg_ds")
     for seq in p["sequence"]:
-        subN = int(seq["duration"] / seq["dt"])
+        durs = seq["duration"] if isinstance(seq["duration"], list) else [seq["duration"]]
+        subN = int(max(durs) / seq["dt"])
         nk = seq["Nk"]
         na = subN // nk
         if cur_dt != seq["dt"]:
             engine.set_dt(seq["dt"])
             cur_dt = seq["dt"]
         if seq["name"] == "bragg_ad":
-            kind = KIND_DOUBLE_BRAGG_AD if p["program"] == "double_bragg" else KIND_BRAGG_AD
+            kind = {"double_bragg": KIND_DOUBLE_BRAGG_AD, "bragg_ds": KIND_BRAGG_DS_AD}.get(p["program"],
+                                                                                         KIND_BRAGG_AD)
+        elif two_species:
+            kind = KIND_NL_IF_2
         elif is_if:
             kind = KIND_NL_IF
         else:
             kind = KIND_NL
+        if two_species and laser2 is not None:
+            # seq.time = Get_t() at the start of the sequence; pulse windows
+            # from the durations (bragg_ds.cpp:117-127 reads two)
+            engine.set_species2(laser2, engine.t, (durs + durs)[:2])
         for _ in range(na):
             Fv = None
             if kind in (KIND_BRAGG_AD, KIND_DOUBLE_BRAGG_AD):
@@ -94,7 +110,10 @@ def run_rt(engine, p: dict, psi0, V=None, make_laser=None, on_block=None):
             engine.block(nk, kind, laser, Fv)
             outputs.append((engine.t, [np.array(engine.psi(c)) for c in range(ncomp)]))
             if is_if and seq.get("rabi", False):
-                rabi.append(engine.rabi_integrals(p["rabi_k0"], p["rabi_threshold"]))
+                r = engine.rabi_integrals(p["rabi_k0"], p["rabi_threshold"])
+                if two_species:  # species 2 on component ncomp/2
+                    r = np.concatenate([r, engine.rabi_integrals(p["rabi_k0_2"], p["rabi_threshold"], ncomp // 2)])
+                rabi.append(r)
             if on_block is not None:
                 on_block(engine)
     return outputs, rabi

@@ -13,11 +13,12 @@ import numpy as np
 import pytest
 
 from atus2_b200 import PREC_FP64, PREC_MIXED, Laser, Solver, binfmt
-from golden_io import BRAGG_CASES, DBRAGG_CASES, RT_CASES, SOB_CASES, load, sob_inputs
+from golden_io import BRAGG_CASES, BRAGGDS_CASES, DBRAGG_CASES, RT_CASES, SOB_CASES, load, sob_inputs
 from gpu_util import rel_l2
 from oracle.oracle import Laser as OLaser
 from oracle.oracle import Oracle
-from replay import KIND_BRAGG_AD, KIND_DOUBLE_BRAGG_AD, KIND_NL, KIND_NL_IF, gaussian_pulse, run_rt
+from replay import (KIND_BRAGG_AD, KIND_BRAGG_DS_AD, KIND_DOUBLE_BRAGG_AD, KIND_NL, KIND_NL_IF, KIND_NL_IF_2,
+                    gaussian_pulse, run_rt)
 
 pytestmark = pytest.mark.gpu
 
@@ -41,7 +42,7 @@ def state_close(psi, ref, tol):
             assert rel_l2(psi[c], ref[c]) < tol, c
 
 
-@pytest.mark.parametrize("name", RT_CASES + BRAGG_CASES + DBRAGG_CASES)
+@pytest.mark.parametrize("name", RT_CASES + BRAGG_CASES + DBRAGG_CASES + BRAGGDS_CASES)
 def test_golden_realtime_fp64(name):
     g = load(name)
     p = g["params"]
@@ -51,7 +52,7 @@ def test_golden_realtime_fp64(name):
     for (t, psi), t_ref, psi_ref in zip(outs, g["t"], g["psi"]):
         assert t == t_ref
         state_close(psi, psi_ref, FP64_TOL)
-    if p["program"] in ("bragg", "double_bragg"):
+    if p["program"] in ("bragg", "double_bragg", "bragg_ds"):
         np.testing.assert_allclose(np.array(rabi), g["rabi"], rtol=5e-6, atol=1e-10)
 
 
@@ -288,6 +289,7 @@ def _run_cfg(h, ncomp, prec, psis, kind, nsteps, V=None, laser=None, F=None):
     ([256, 128], 1, KIND_NL),            # 2D, single component with a potential
     ([64, 32, 256], 3, KIND_NL),         # three components: potential pass on the tile kernel
     ([128, 64, 32], 3, KIND_DOUBLE_BRAGG_AD),
+    ([64, 32, 128], 4, KIND_BRAGG_DS_AD),
 ])
 def test_register_staged_passes_match_tile_kernel(prec, shape, ncomp, kind, monkeypatch):
     """The register-staged pass kernel and the shared-memory tile kernel run
@@ -298,7 +300,7 @@ def test_register_staged_passes_match_tile_kernel(prec, shape, ncomp, kind, monk
     psis = [(np.exp(-0.5 * r2 - 0.1 * c * r2) * np.exp(1j * (c + 1) * xs[0])).astype(np.complex128)
             for c in range(ncomp)]
     V = 0.5 * r2 if kind == KIND_NL else None
-    bragg = kind in (KIND_BRAGG_AD, KIND_DOUBLE_BRAGG_AD)
+    bragg = kind in (KIND_BRAGG_AD, KIND_DOUBLE_BRAGG_AD, KIND_BRAGG_DS_AD)
     laser = Laser.make(Amp=[4.0, 4.0], laser_k=[3.0, 0], laser_domh=[2.0, 0], beta=[0.3, 0.1, 0]) if bragg else None
     F = np.full(12, 0.8) if bragg else None
     res = []
@@ -337,6 +339,7 @@ def test_register_staged_sobolev_matches_tile_kernel(monkeypatch):
     ([16, 128, 128], 1, KIND_NL),
     ([16, 32, 32], 2, KIND_NL_IF),
     ([32, 32, 64], 3, KIND_DOUBLE_BRAGG_AD),
+    ([16, 32, 64], 4, KIND_BRAGG_DS_AD),
 ])
 def test_plane_pipeline_matches_axis_passes(prec, shape, ncomp, kind, monkeypatch):
     """The 3D real-space half step as one plane pipeline (IFFT_y, z pass with
@@ -350,7 +353,7 @@ def test_plane_pipeline_matches_axis_passes(prec, shape, ncomp, kind, monkeypatc
     V = 0.5 * r2 if kind == KIND_NL else None
     laser = (Laser.make(Amp=[4.0, 4.0], laser_k=[3.0, 0], laser_domh=[2.0, 0], beta=[0.2, 0, 0],
                         DeltaL=[0, -1.0, 0, 0]) if kind != KIND_NL else None)
-    F = np.full(12, 0.8) if kind in (KIND_BRAGG_AD, KIND_DOUBLE_BRAGG_AD) else None
+    F = np.full(12, 0.8) if kind in (KIND_BRAGG_AD, KIND_DOUBLE_BRAGG_AD, KIND_BRAGG_DS_AD) else None
     res = []
     for pipe in ("1", "0"):
         monkeypatch.setenv("ATUS_PIPE", pipe)
@@ -400,6 +403,55 @@ def test_double_bragg_matches_oracle(dim, prec, tol):
     assert min(n_o[1], n_o[2]) > 1e-3  # both side states populated
     np.testing.assert_allclose([s.particle_number(c) for c in range(3)], n_o,
                                rtol=(1e-11 if prec == PREC_FP64 else 1e-5))
+
+
+@pytest.mark.parametrize("prec,tol", [(PREC_FP64, FP64_TOL), (PREC_MIXED, MIXED_TOL)])
+@pytest.mark.parametrize("dim", [1, 2, 3])
+def test_bragg_ds_matches_oracle(dim, prec, tol):
+    """Two species of two states each (bragg_ds): per-species kinetic
+    coefficients, lasers, gravity terms and pulse windows (species 1 switches
+    off after 0.05, species 2 after 0.08) over 120 bragg_ad steps, then 40
+    two-species freeprop steps, against the oracle.  1D 4096 points on
+    [-64,64), 2D 256x128, 3D 32^3."""
+    n = {1: [4096], 2: [256, 128], 3: [32, 32, 32]}[dim]
+    L = {1: 128.0, 2: 32.0, 3: 16.0}[dim]
+    h = _grid(dim, n, L)
+    xs = _coords(h)
+    r2 = sum(x * x for x in xs)
+    w = 4.0 if dim == 1 else 1.5
+    a = np.exp(-0.5 * r2 / w).astype(np.complex128)
+    b = np.exp(-0.5 * r2 / (0.7 * w)).astype(np.complex128)
+    vol = float(np.prod([h[f"d{c}"] for c in "xyz"[:dim]]))
+    a /= math.sqrt(vol * np.sum(np.abs(a) ** 2))
+    b /= math.sqrt(vol * np.sum(np.abs(b) ** 2))
+    z = np.zeros_like(a)
+    gs = [40.0, 35.0, 10.0, 8.0, 35.0, 38.0, 8.0, 10.0, 10.0, 8.0, 30.0, 25.0, 8.0, 10.0, 25.0, 28.0]
+    o, s = _setup_pair(h, 4, [a, z, b, z], [0.5] * dim, gs, None, 1e-3, prec)
+    for e in (o, s):
+        for c in (2, 3):
+            e.set_alpha(c, [0.3] * dim)
+    kw1 = dict(beta=[0.4, 0.0, 0.0], DeltaL=[0.0, 0.5, 0.2, -0.3], Amp=[3.0, 3.0], laser_k=[4.0, 0],
+               laser_dk=[0.2, 0], laser_domh=[8.0, 0], phase=[0.0, 0], chirp_rate=[0, 0], chirp=0.0)
+    kw2 = dict(beta=[-0.2, 0.0, 0.0], Amp=[2.5, 2.5], laser_k=[3.0, 0], laser_dk=[0.3, 0], laser_domh=[2.7, 0],
+               phase=[0.4, 0], chirp_rate=[0.5, 0])
+    Lo, Ls = OLaser.make(**kw1), Laser.make(**kw1)
+    o.set_species2(OLaser.make(**kw2), o.t, (0.0505, 0.0805))
+    s.set_species2(Laser.make(**kw2), s.t, (0.0505, 0.0805))
+    for _ in range(3):
+        o.block(40, KIND_BRAGG_DS_AD, Lo)
+        s.block(40, KIND_BRAGG_DS_AD, Ls)
+    o.block(40, KIND_NL_IF_2, Lo)
+    s.block(40, KIND_NL_IF_2, Ls)
+    assert s.t == o.t
+    state_close([s.psi(c) for c in range(4)], [o.psi(c) for c in range(4)], tol)
+    n_o = [o.particle_number(c) for c in range(4)]
+    assert min(n_o[1], n_o[3]) > 1e-3  # both species transferred population
+    np.testing.assert_allclose([s.particle_number(c) for c in range(4)], n_o,
+                               rtol=(1e-11 if prec == PREC_FP64 else 1e-5))
+    k0 = np.zeros((3, dim))
+    k0[1, 0], k0[2, 0] = 6.0, -6.0
+    np.testing.assert_allclose(s.rabi_integrals(k0, 1.0, 2), o.rabi_integrals(k0, 1.0, 2),
+                               rtol=(1e-11 if prec == PREC_FP64 else 1e-4), atol=1e-12)
 
 
 def test_stable_bragg_form():
