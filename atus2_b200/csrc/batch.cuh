@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(NT) batch1d_kernel(const BInst1 *__restrict__ 
           C v[MAXC];
           v[0] = s[Pad<N>::idx(0, i)];
           v[1] = s[NP + Pad<N>::idx(0, i)];
-          nl_point<R>(nl, v, i, x0, om, ec, es);
+          nl_point<R, 2>(nl, v, i, x0, om, ec, es);
           s[Pad<N>::idx(0, i)] = v[0];
           s[NP + Pad<N>::idx(0, i)] = v[1];
         }
@@ -164,7 +164,7 @@ __global__ void __launch_bounds__(NT) batch1d_kernel(const BInst1 *__restrict__ 
           C v[MAXC];
           v[0] = rc ? oth : res;
           v[1] = rc ? res : oth;
-          nl_point<R>(nl, v, i, x0, om, ec, es);
+          nl_point<R, 2>(nl, v, i, x0, om, ec, es);
           s[Pad<N>::idx(0, i)] = rc ? v[1] : v[0];
           other[i] = rc ? v[0] : v[1];
         }
@@ -364,7 +364,7 @@ __global__ void __launch_bounds__(Tile<R>::NT) batch_tile_kernel(BPass bp) {
           C v[MAXC];
           #pragma unroll
           for (int c = 0; c < TC; c++) v[c] = s[c * B * NP + Pad<N>::idx(b, i)];
-          nl_point<R>(a.nl, v, l, x0, om, ec, es);
+          nl_point<R, TC>(a.nl, v, l, x0, om, ec, es);
           #pragma unroll
           for (int c = 0; c < TC; c++) s[c * B * NP + Pad<N>::idx(b, i)] = v[c];
         }

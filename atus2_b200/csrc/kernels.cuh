@@ -372,37 +372,42 @@ __device__ __forceinline__ void bragg_ds_point(const NLArgs &a, cplx<R> *v, doub
 // FP64: the reference's formulas (include/CRT_Base.h:410-439,
 // CRT_Base_IF.h:392-418, bragg.cpp:210-302).  Mixed: FP64 phase arguments,
 // FP32 field arithmetic, and the eigenvalue-free form of the 2x2 exponential.
-template <typename R>
+// TC: the number of components the calling kernel holds (ncomp <= TC); step
+// kinds that need more components are compiled out.
+template <typename R, int TC = MAXC>
 __device__ __forceinline__ void nl_point(const NLArgs &a, cplx<R> *v, int64_t l, double x0, double Omega,
                                          double eta_c, double eta_s) {
-  using C = cplx<R>;
-  if (a.kind == K_DBRAGG) {
-    dbragg_point<R>(a, v, l, x0);
-    return;
+  if constexpr (TC >= 3) {
+    if (a.kind == K_DBRAGG) {
+      dbragg_point<R>(a, v, l, x0);
+      return;
+    }
   }
-  if (a.kind == K_BRAGG_DS) {
-    bragg_ds_point<R>(a, v, x0);
-    return;
+  if constexpr (TC >= 4) {
+    if (a.kind == K_BRAGG_DS) {
+      bragg_ds_point<R>(a, v, x0);
+      return;
+    }
   }
   const int n = a.ncomp;
-  double rho[MAXC];
+  double rho[TC];
   #pragma unroll
-  for (int j = 0; j < MAXC; j++)
+  for (int j = 0; j < TC; j++)
     if (j < n) rho[j] = (double)v[j].x * (double)v[j].x + (double)v[j].y * (double)v[j].y;
-  if (a.kind != K_BRAGG) {
+  if (TC < 2 || a.kind != K_BRAGG) {
     #pragma unroll
-    for (int i = 0; i < MAXC; i++) {
+    for (int i = 0; i < TC; i++) {
       if (i >= n) break;
       double phi;
       if (a.kind == K_NL) {
         phi = a.V[i] ? a.V[i][l] : 0.0;
         #pragma unroll
-        for (int j = 0; j < MAXC; j++)
+        for (int j = 0; j < TC; j++)
           if (j < n) phi += a.gs[i * MAXC + j] * rho[j];
       } else {
         phi = 0.0;
         #pragma unroll
-        for (int j = 0; j < MAXC; j++)
+        for (int j = 0; j < TC; j++)
           if (j < n) phi += a.gs[i * MAXC + j] * rho[j];
         // CRT_Base_IF_2 (two species): beta of the component's species
         const double b = (a.kind == K_NL_IF2 && 2 * i >= n) ? a.L2.beta0 : a.L.beta0;
@@ -414,10 +419,12 @@ __device__ __forceinline__ void nl_point(const NLArgs &a, cplx<R> *v, int64_t l,
     }
     return;
   }
-  // Bragg 2x2 (components 0 and 1)
-  const double V11 = a.gs[0] * rho[0] + a.gs[1] * rho[1] + a.L.beta0 * x0;
-  const double V22 = a.gs[MAXC] * rho[0] + a.gs[MAXC + 1] * rho[1] - a.L.DeltaL[1] + a.L.beta0 * x0;
-  bragg_pair<R>(a.stable, a.dt, V11, V22, Omega, eta_c, eta_s, v[0], v[1]);
+  if constexpr (TC >= 2) {
+    // Bragg 2x2 (components 0 and 1)
+    const double V11 = a.gs[0] * rho[0] + a.gs[1] * rho[1] + a.L.beta0 * x0;
+    const double V22 = a.gs[MAXC] * rho[0] + a.gs[MAXC + 1] * rho[1] - a.L.DeltaL[1] + a.L.beta0 * x0;
+    bragg_pair<R>(a.stable, a.dt, V11, V22, Omega, eta_c, eta_s, v[0], v[1]);
+  }
 }
 
 // Omega(x0) and eta(x0) of the Bragg step (bragg.cpp:224, 243).
@@ -633,7 +640,7 @@ __global__ void __launch_bounds__(Tile<R>::NT, Tile<R>::MINB) pass_kernel(PassAr
           C v[MAXC];
           #pragma unroll
           for (int c = 0; c < TC; c++) v[c] = s[c * B * NP + Pad<N>::idx(b, i)];
-          nl_point<R>(a.nl, v, l, x0, om, ec, es);
+          nl_point<R, TC>(a.nl, v, l, x0, om, ec, es);
           #pragma unroll
           for (int c = 0; c < TC; c++) s[c * B * NP + Pad<N>::idx(b, i)] = v[c];
         }
@@ -734,7 +741,7 @@ __global__ void __launch_bounds__(BLOCK1D_NT) block1d_kernel(Block1DArgs a) {
       C v[MAXC];
       #pragma unroll
       for (int c = 0; c < TC; c++) v[c] = s[c * NP + Pad<N>::idx(0, i)];
-      nl_point<R>(nl, v, i, x0, om, ec, es);
+      nl_point<R, TC>(nl, v, i, x0, om, ec, es);
       #pragma unroll
       for (int c = 0; c < TC; c++) s[c * NP + Pad<N>::idx(0, i)] = v[c];
     }

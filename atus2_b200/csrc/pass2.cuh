@@ -242,7 +242,7 @@ __device__ __forceinline__ void p2_item(const PassArgs &a, const TileGeo &g, uns
         if (a.nl.kind == K_BRAGG) bragg_coupling(a.nl, x0, om, ec, es);
         C u[MAXC];
         u[0] = v[m];
-        if (live) nl_point<R>(a.nl, u, l, x0, om, ec, es);
+        if (live) nl_point<R, TC>(a.nl, u, l, x0, om, ec, es);
         v[m] = u[0];
       }
     } else {
@@ -274,7 +274,7 @@ __device__ __forceinline__ void p2_item(const PassArgs &a, const TileGeo &g, uns
           C u[MAXC];
           #pragma unroll
           for (int cc = 0; cc < TC; cc++) u[cc] = ex[(cc * B + pb) * PB + ex_at(i >> 4, i & 15)];
-          nl_point<R>(a.nl, u, l, x0, om, ec, es);
+          nl_point<R, TC>(a.nl, u, l, x0, om, ec, es);
           #pragma unroll
           for (int cc = 0; cc < TC; cc++) ex[(cc * B + pb) * PB + ex_at(i >> 4, i & 15)] = u[cc];
         }

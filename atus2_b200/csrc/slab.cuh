@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(512) slab_kernel(SlabArgs a) {
       C v[MAXC];
       #pragma unroll
       for (int c = 0; c < TC; c++) v[c] = s[(c * YB + yl) * NPZ + Pad<NZ>::idx(0, z)];
-      nl_point<R>(a.nl, v, l, x0, om, ec, es);
+      nl_point<R, TC>(a.nl, v, l, x0, om, ec, es);
       #pragma unroll
       for (int c = 0; c < TC; c++) s[(c * YB + yl) * NPZ + Pad<NZ>::idx(0, z)] = v[c];
     }
