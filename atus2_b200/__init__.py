@@ -12,6 +12,8 @@ from .engine import (  # noqa: F401
     STEP_DOUBLE_BRAGG_AD,
     STEP_NL_IF_2,
     STEP_BRAGG_DS_AD,
+    STEP_NUMERICAL_BRAGG,
+    STEP_NUMERICAL_RAMAN,
     STEP_NL,
     STEP_NL_IF,
     AtusError,

@@ -78,7 +78,7 @@ def build(jobs: int | None = None, force: bool = False, verbose: bool = False) -
 
 
 HOST = os.path.join(HERE, "host")
-PROGRAMS = ("rt_solver", "bragg", "double_bragg", "bragg_ds", "sobmin", "gen_psi_0")
+PROGRAMS = ("rt_solver", "bragg", "double_bragg", "bragg_ds", "raman", "sobmin", "gen_psi_0")
 
 
 def build_programs(verbose: bool = False) -> None:

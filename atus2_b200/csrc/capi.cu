@@ -107,6 +107,7 @@ static NLArgs nl_args(const atus_ctx *ctx, int kind, double t1, double F) {
   a.L.beta0 = ctx->laser.beta[0];
   for (int c = 0; c < MAXC; c++) a.L.DeltaL[c] = ctx->laser.DeltaL[c];
   a.L.Amp0 = ctx->laser.Amp[0];
+  a.L.Amp1 = ctx->laser.Amp[1];
   a.L.laser_k0 = ctx->laser.laser_k[0];
   a.L.laser_dk0 = ctx->laser.laser_dk[0];
   a.L.laser_domh0 = ctx->laser.laser_domh[0];
@@ -134,6 +135,7 @@ static NLArgs nl_args(const atus_ctx *ctx, int kind, double t1, double F) {
   a.L2.phase0 = ctx->laser2.phase[0];
   a.L2.chirp_rate0 = ctx->laser2.chirp_rate[0];
   a.F2 = F;
+  a.th = ctx->t;
   if (kind == K_BRAGG_DS) {
     // mode1 / mode2 of bragg_ds.cpp:117-127: time = t1 - seq.time
     const double time = t1 - ctx->win_t0;
@@ -689,10 +691,13 @@ int atus_ft_step(atus_ctx *ctx, int half) {
 }
 
 static int check_kind(atus_ctx *ctx, int kind) {
-  if (kind < K_NL || kind > K_BRAGG_DS) return fail(ctx, ATUS_E_ARG, "unknown step kind");
+  if (kind < K_NL || kind > K_RAMAN) return fail(ctx, ATUS_E_ARG, "unknown step kind");
   if (kind == K_NL_IF2 && (ctx->ncomp % 2) != 0)
     return fail(ctx, ATUS_E_ARG, "the two-species freeprop needs an even number of components");
   if (kind == K_BRAGG_DS && ctx->ncomp != 4) return fail(ctx, ATUS_E_ARG, "the two-species bragg_ad needs four components");
+  if (kind == K_NUM_BRAGG && (ctx->ncomp < 2 || ctx->ncomp > 3))
+    return fail(ctx, ATUS_E_ARG, "the numerical bragg step needs two or three components");
+  if (kind == K_RAMAN && ctx->ncomp != 3) return fail(ctx, ATUS_E_ARG, "the raman step needs three components");
   if (kind == K_BRAGG && ctx->ncomp != 2) return fail(ctx, ATUS_E_ARG, "bragg_ad needs two components");
   if (kind == K_DBRAGG && ctx->ncomp != 3) return fail(ctx, ATUS_E_ARG, "the three-level bragg_ad needs three components");
   return ATUS_OK;
@@ -718,10 +723,10 @@ int atus_strang_block(atus_ctx *ctx, int nk, int kind, const double *F) {
   if (!ctx || nk < 1) return ATUS_E_ARG;
   RUN(check_kind(ctx, kind));
   const double dt = ctx->dt;
-  if (ctx->dim == 1 && ctx->ncomp > 2) {
-    // more components than the resident 1D kernel holds: per step one
-    // kinetic pass (FFT, phase, IFFT per component) and one point-wise
-    // potential step
+  if (ctx->dim == 1 && (ctx->ncomp > 2 || kind == K_NUM_BRAGG)) {
+    // more components than the resident 1D kernel holds, or a step that reads
+    // the header time itself: per step one kinetic pass (FFT, phase, IFFT per
+    // component) and one point-wise potential step
     RUN(kinetic_pass(ctx, 1));
     ctx->t += 0.5 * dt;
     for (int j = 0; j < nk; j++) {

@@ -38,13 +38,15 @@ enum { OP_NONE = 0, OP_KIN = 1, OP_NL = 2, OP_FILT = 3 };
 enum { FILT_SOBOLEV = 0, FILT_LAPLACE = 1 };
 // step kinds: CRT_Base freeprop, CRT_Base_IF freeprop, bragg_ad, the
 // three-level bragg_ad (double_bragg), CRT_Base_IF_2 freeprop (two species),
-// the two-species bragg_ad (bragg_ds)
-enum { K_NL = 0, K_NL_IF = 1, K_BRAGG = 2, K_DBRAGG = 3, K_NL_IF2 = 4, K_BRAGG_DS = 5 };
+// the two-species bragg_ad (bragg_ds), and the numerical n-state "bragg" and
+// three-state "raman" steps of CRT_Base_IF
+enum { K_NL = 0, K_NL_IF = 1, K_BRAGG = 2, K_DBRAGG = 3, K_NL_IF2 = 4, K_BRAGG_DS = 5, K_NUM_BRAGG = 6, K_RAMAN = 7 };
 // modes of the register-staged pass kernel (pass2.cuh)
 enum { M2_FWD = 0, M2_INV = 1, M2_KIN = 2, M2_NL = 3 };
 
 struct LaserD {
   double beta0, DeltaL[MAXC], Amp0, laser_k0, laser_dk0, laser_domh0, phase0, chirp_rate0, chirp;
+  double Amp1;  // second amplitude (Amp_1 entry 1), used by the numerical steps
 };
 
 // Potential-step parameters (by value).
@@ -69,6 +71,7 @@ struct NLArgs {
   // laser_dk0, laser_domh0, phase0, chirp_rate0 used) and its pulse factor
   LaserD L2;
   double F2;
+  double th;  // header time at the potential step (the numerical "bragg" step's t1)
 };
 
 struct Geo {
@@ -367,6 +370,163 @@ __device__ __forceinline__ void bragg_ds_point(const NLArgs &a, cplx<R> *v, doub
   }
 }
 
+// ------------------------------------------------------------ numerical n-state steps
+// psi <- exp(-i h A) psi for a Hermitian 3x3 matrix A (n = 2: the third row
+// and column are zero and so is psi[2]).  The reference diagonalises A with
+// GSL's gsl_eigen_hermv and forms V diag(e^{-i h lambda}) V^H psi
+// (include/CRT_Base_IF.h:471-497, 581-607); here the same exponential comes
+// from its Taylor series on the vector: the mean of the diagonal is taken out
+// as a scalar phase, the rest is split into s substeps with
+// h ||A||_inf / s <= 1/4 (||.||_inf bounded by |Re| + |Im| row sums), and each
+// substep sums terms (-i h A / s)^k psi / k! until a term falls below 2^-60
+// of the sum (k <= 18; the truncation error at k = 18 is below 1e-22).  No
+// eigenvalues, so degenerate or nearly degenerate spectra need no care.
+__device__ __forceinline__ void herm_expm_apply(double2 (&A)[3][3], int n, double h, double2 (&p)[3]) {
+  double mu = 0.0;
+  #pragma unroll
+  for (int i = 0; i < 3; i++)
+    if (i < n) mu += A[i][i].x;
+  mu /= n;
+  #pragma unroll
+  for (int i = 0; i < 3; i++)
+    if (i < n) A[i][i].x -= mu;
+  double nu = 0.0;
+  #pragma unroll
+  for (int i = 0; i < 3; i++) {
+    double r = 0.0;
+    #pragma unroll
+    for (int j = 0; j < 3; j++) r += fabs(A[i][j].x) + fabs(A[i][j].y);
+    nu = fmax(nu, r);
+  }
+  nu *= h;
+  int steps = 1;
+  if (nu > 0.25) steps = (int)fmin(ceil(4.0 * nu), 1048576.0);
+  const double hs = h / steps;
+  // M = -i hs A
+  double2 M[3][3];
+  #pragma unroll
+  for (int i = 0; i < 3; i++)
+    #pragma unroll
+    for (int j = 0; j < 3; j++) M[i][j] = make_double2(hs * A[i][j].y, -hs * A[i][j].x);
+  constexpr double INVK[19] = {0.0,      1.0,       1.0 / 2,  1.0 / 3,  1.0 / 4,  1.0 / 5,  1.0 / 6,
+                               1.0 / 7,  1.0 / 8,   1.0 / 9,  1.0 / 10, 1.0 / 11, 1.0 / 12, 1.0 / 13,
+                               1.0 / 14, 1.0 / 15,  1.0 / 16, 1.0 / 17, 1.0 / 18};
+  for (int st = 0; st < steps; st++) {
+    double2 y[3] = {p[0], p[1], p[2]}, t[3] = {p[0], p[1], p[2]};
+    #pragma unroll 1
+    for (int k = 1; k <= 18; k++) {
+      double2 u[3];
+      #pragma unroll
+      for (int i = 0; i < 3; i++) {
+        double2 acc = cmul(M[i][0], t[0]);
+        acc = cadd(acc, cmul(M[i][1], t[1]));
+        acc = cadd(acc, cmul(M[i][2], t[2]));
+        u[i] = make_double2(acc.x * INVK[k], acc.y * INVK[k]);
+      }
+      double tn = 0.0, yn = 0.0;
+      #pragma unroll
+      for (int i = 0; i < 3; i++) {
+        t[i] = u[i];
+        y[i] = cadd(y[i], u[i]);
+        tn += fabs(u[i].x) + fabs(u[i].y);
+        yn += fabs(y[i].x) + fabs(y[i].y);
+      }
+      if (tn <= 0x1p-60 * yn) break;
+    }
+    p[0] = y[0];
+    p[1] = y[1];
+    p[2] = y[2];
+  }
+  double sn, cs;
+  sincos_step(-h * mu, &sn, &cs);
+  const double2 e = make_double2(cs, sn);
+  #pragma unroll
+  for (int i = 0; i < 3; i++) p[i] = cmul(p[i], e);
+}
+
+// beta . x over every axis at grid index l (x0 given; y and z from the index).
+__device__ __forceinline__ double beta_dot_x(const NLArgs &a, int64_t l, double x0) {
+  double bx = a.L.beta0 * x0;
+  if (a.lg1 > 0) {
+    const int iy = (int)((l >> a.lg2) & ((1 << a.lg1) - 1));
+    bx += a.beta1 * ((double)(iy - a.shift1) * a.dx1);
+  }
+  if (a.lg2 > 0) {
+    const int iz = (int)(l & ((1 << a.lg2) - 1));
+    bx += a.beta2 * ((double)(iz - a.shift2) * a.dx2);
+  }
+  return bx;
+}
+
+// The numerical steps of CRT_Base_IF at grid index l (n = ncomp components):
+// diagonal V_i = sum_j g_ij |psi_j|^2 + (beta . x - DeltaL_i);
+//  "bragg" (Numerical_Bragg, include/CRT_Base_IF.h:426-526): state 0 couples
+//   to state i+1 with eta_i = (Amp0 + Amp1)/2 cos(a_i) + i (Amp0 - Amp1)/2
+//   sin(a_i), a_i = (-domh + rate_i t) t + k_i x - phase/2, k_1 = -k_0,
+//   rate_1 = -rate_0, t the header time;
+//  "raman" (Numerical_Raman, :533-632): V_2 + domh, A_02 = Amp0/2 e^{i k x},
+//   A_12 = Amp1/2 e^{-i k x}.
+// Then psi <- exp(-i dt A) psi in FP64 for both field precisions.
+// Not inlined: the pass kernels that carry it keep their register budget for
+// the common steps.
+template <typename R, int TC>
+__device__ __noinline__ void num_point(const NLArgs &a, cplx<R> *v, int64_t l, double x0) {
+  constexpr int NC = TC < 3 ? TC : 3;
+  const int n = a.ncomp;
+  const double bx = beta_dot_x(a, l, x0);
+  double2 p[3];
+  double rho[3];
+  #pragma unroll
+  for (int j = 0; j < 3; j++) {
+    p[j] = (j < NC && j < n) ? to_d<R>(v[j]) : make_double2(0.0, 0.0);
+    rho[j] = p[j].x * p[j].x + p[j].y * p[j].y;
+  }
+  double2 A[3][3];
+  #pragma unroll
+  for (int i = 0; i < 3; i++)
+    #pragma unroll
+    for (int j = 0; j < 3; j++) A[i][j] = make_double2(0.0, 0.0);
+  #pragma unroll
+  for (int i = 0; i < NC; i++) {
+    if (i >= n) break;
+    double phi = 0.0;
+    #pragma unroll
+    for (int j = 0; j < NC; j++)
+      if (j < n) phi += a.gs[i * MAXC + j] * rho[j];
+    A[i][i].x = phi + (bx - a.L.DeltaL[i]);
+  }
+  if (a.kind == K_RAMAN) {
+    if constexpr (NC >= 3) {
+      A[2][2].x += a.L.laser_domh0;
+      double sn, cs;
+      sincos(a.L.laser_k0 * x0, &sn, &cs);
+      const double h0 = a.L.Amp0 / 2, h1 = a.L.Amp1 / 2;
+      A[0][2] = make_double2(h0 * cs, h0 * sn);
+      A[2][0] = make_double2(h0 * cs, -h0 * sn);
+      A[1][2] = make_double2(h1 * cs, -h1 * sn);
+      A[2][1] = make_double2(h1 * cs, h1 * sn);
+    }
+  } else {
+    const double t1 = a.th;
+    #pragma unroll
+    for (int i = 0; i + 1 < NC; i++) {
+      if (i + 1 >= n) break;
+      const double k = i == 0 ? a.L.laser_k0 : -a.L.laser_k0;
+      const double rate = i == 0 ? a.L.chirp_rate0 : -a.L.chirp_rate0;
+      double sn, cs;
+      sincos((-a.L.laser_domh0 + rate * t1) * t1 + k * x0 - 0.5 * a.L.phase0, &sn, &cs);
+      const double er = a.L.Amp0 * cs / 2 + a.L.Amp1 * cs / 2, ei = a.L.Amp0 * sn / 2 - a.L.Amp1 * sn / 2;
+      A[i + 1][0] = make_double2(er, ei);
+      A[0][i + 1] = make_double2(er, -ei);
+    }
+  }
+  herm_expm_apply(A, n, a.dt, p);
+  #pragma unroll
+  for (int j = 0; j < NC; j++)
+    if (j < n) v[j] = from_d<R>(p[j]);
+}
+
+
 // ------------------------------------------------------------ potential step
 // Point-wise potential step on the ncomp values v[] at grid index l.
 // FP64: the reference's formulas (include/CRT_Base.h:410-439,
@@ -386,6 +546,12 @@ __device__ __forceinline__ void nl_point(const NLArgs &a, cplx<R> *v, int64_t l,
   if constexpr (TC >= 4) {
     if (a.kind == K_BRAGG_DS) {
       bragg_ds_point<R>(a, v, x0);
+      return;
+    }
+  }
+  if constexpr (TC >= 2) {
+    if (a.kind == K_NUM_BRAGG || a.kind == K_RAMAN) {
+      num_point<R, TC>(a, v, l, x0);
       return;
     }
   }

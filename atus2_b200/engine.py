@@ -32,6 +32,7 @@ ATUS_OK = 0
 PREC_FP64 = 0
 PREC_MIXED = 1
 STEP_NL, STEP_NL_IF, STEP_BRAGG_AD, STEP_DOUBLE_BRAGG_AD, STEP_NL_IF_2, STEP_BRAGG_DS_AD = 0, 1, 2, 3, 4, 5
+STEP_NUMERICAL_BRAGG, STEP_NUMERICAL_RAMAN = 6, 7
 MAX_COMP = 4
 
 _ERRORS = {-1: "invalid argument", -2: "unsupported", -3: "CUDA error", -4: "bad state", -5: "out of device memory"}

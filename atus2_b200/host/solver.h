@@ -10,7 +10,8 @@
 // function (a user's StepFunction) needs it, and uploaded again afterwards.
 //
 // GPU step tags: "freeprop" (CRT_Base: V + g|psi|^2; CRT_Base_IF: g|psi|^2 +
-// beta.x - DeltaL) and those a subclass adds to m_gpu_steps (e.g. "bragg_ad").
+// beta.x - DeltaL), CRT_Base_IF's numerical "bragg" and "raman", and those a
+// subclass adds to m_gpu_steps (e.g. "bragg_ad").
 // Any other tag is looked up in m_map_stepfcts and runs on the host copy.
 #pragma once
 
@@ -367,7 +368,10 @@ class CRT_Base_IF : public CRT_Base<dim, no_int_states> {
 
  public:
   explicit CRT_Base_IF(ParameterHandler *params, int precision = ATUS_PREC_FP64) : Base(params, precision) {
+    // include/CRT_Base_IF.h:120-129: freeprop and the numerical bragg / raman steps
     this->m_gpu_steps["freeprop"] = ATUS_STEP_NL_IF;
+    this->m_gpu_steps["bragg"] = ATUS_STEP_NUMERICAL_BRAGG;
+    this->m_gpu_steps["raman"] = ATUS_STEP_NUMERICAL_RAMAN;
     UpdateParams();
   }
 

@@ -91,6 +91,12 @@ extern "C" {
 #define ATUS_STEP_BRAGG_DS_AD 5 /* "bragg_ad" of bragg_ds: a 2x2 Bragg exponential per species,
                                    components (0,1) and (2,3), Bragg_single::Do_Bragg_ad
                                    (bragg_ds.cpp:111-322) */
+#define ATUS_STEP_NUMERICAL_BRAGG 6 /* "bragg" of CRT_Base_IF: n-state (n = 2, 3) Bragg exponential,
+                                       CRT_Base_IF::Numerical_Bragg (include/CRT_Base_IF.h:426-526);
+                                       F is not used (the reference has no envelope here) */
+#define ATUS_STEP_NUMERICAL_RAMAN 7 /* "raman" of CRT_Base_IF: three-state Raman exponential,
+                                       CRT_Base_IF::Numerical_Raman (include/CRT_Base_IF.h:533-632);
+                                       F is not used */
 
 #define ATUS_MAX_COMP 4
 

@@ -28,6 +28,12 @@
  *                             (Bragg_single::Do_Bragg_ad of bragg_ds)
  *   orc_rabi_integrals_comp   include/CRT_Base_IF_2.h:115-210 (species 2 on
  *                             component no_int_states/2)
+ *   orc_numerical_bragg       include/CRT_Base_IF.h:426-526 (Numerical_Bragg)
+ *   orc_numerical_raman       include/CRT_Base_IF.h:533-632 (Numerical_Raman)
+ *                             Both call the GSL routines the reference calls;
+ *                             GSL is not installed here, so they come from the
+ *                             same shim the reference programs in oracle/_ref
+ *                             are built against (shim/gsl/gsl_shim_types.h).
  *   orc_block                 include/CRT_Base.h:776-786 / CRT_Base_IF.h:779-789
  *   orc_particle_number       include/CRT_Base.h:586-599
  *   orc_expval_position/momentum include/CRT_Base.h:480-580
@@ -44,6 +50,7 @@
 #include <string.h>
 
 #include "fft_cpu.h"
+#include "shim/gsl/gsl_shim_types.h"
 #include <omp.h>
 
 #ifndef M_PI
@@ -626,16 +633,140 @@ void orc_bragg_ds_ad(orc_ctx *c, const orc_laser *L, double F) {
   }
 }
 
+/* ------------------------------------------ numerical steps (GSL eigensolver) */
+
+/* Shared tail of Numerical_Bragg / Numerical_Raman: eigen-decompose A, form
+ * evec diag(e^{i dt lambda}) evec^H with dt = -header dt, apply it to psi at l. */
+typedef struct {
+  gsl_matrix_complex *A, *B, *evec;
+  gsl_eigen_hermv_workspace *w;
+  gsl_vector *eval;
+  gsl_vector_complex *P1, *P2;
+} orc_num_ws;
+
+static void num_ws_alloc(orc_num_ws *ws, int n) {
+  ws->A = gsl_matrix_complex_calloc(n, n);
+  ws->B = gsl_matrix_complex_calloc(n, n);
+  ws->w = gsl_eigen_hermv_alloc(n);
+  ws->eval = gsl_vector_alloc(n);
+  ws->P1 = gsl_vector_complex_alloc(n);
+  ws->P2 = gsl_vector_complex_alloc(n);
+  ws->evec = gsl_matrix_complex_alloc(n, n);
+}
+
+static void num_ws_free(orc_num_ws *ws) {
+  gsl_matrix_complex_free(ws->A);
+  gsl_matrix_complex_free(ws->B);
+  gsl_eigen_hermv_free(ws->w);
+  gsl_vector_free(ws->eval);
+  gsl_vector_complex_free(ws->P1);
+  gsl_vector_complex_free(ws->P2);
+  gsl_matrix_complex_free(ws->evec);
+}
+
+/* diagonal: phi_i = sum_j g_ij |psi_j|^2, then += beta.x - DeltaL_i (CPoint dot
+ * product over all axes from 0) */
+static void num_diagonal(orc_ctx *c, const orc_laser *L, long l, orc_num_ws *ws, double *phi, double *x) {
+  const int n = c->ncomp;
+  orc_get_x(c, l, x);
+  for (int i = 0; i < n; i++) {
+    phi[i] = 0;
+    for (int j = 0; j < n; j++) {
+      const double *P = c->psi[j];
+      phi[i] += c->gs[j + n * i] * (P[2 * l] * P[2 * l] + P[2 * l + 1] * P[2 * l + 1]);
+    }
+    double bx = 0;
+    for (int a = 0; a < c->dim; a++) bx += L->beta[a] * x[a];
+    phi[i] += bx - L->DeltaL[i];
+    gsl_matrix_complex_set(ws->A, i, i, gsl_complex_rect(phi[i], 0));
+  }
+}
+
+static void num_apply(orc_ctx *c, long l, orc_num_ws *ws) {
+  const int n = c->ncomp;
+  const double dt = -c->dt;
+  gsl_eigen_hermv(ws->A, ws->eval, ws->evec, ws->w);
+  for (int i = 0; i < n; i++) {
+    double re1, im1;
+    sincos(dt * gsl_vector_get(ws->eval, i), &im1, &re1);
+    gsl_matrix_complex_set(ws->B, i, i, gsl_complex_rect(re1, im1));
+  }
+  gsl_blas_zgemm(CblasNoTrans, CblasConjTrans, GSL_COMPLEX_ONE, ws->B, ws->evec, GSL_COMPLEX_ZERO, ws->A);
+  gsl_blas_zgemm(CblasNoTrans, CblasNoTrans, GSL_COMPLEX_ONE, ws->evec, ws->A, GSL_COMPLEX_ZERO, ws->B);
+  for (int i = 0; i < n; i++) gsl_vector_complex_set(ws->P1, i, gsl_complex_rect(c->psi[i][2 * l], c->psi[i][2 * l + 1]));
+  gsl_blas_zgemv(CblasNoTrans, GSL_COMPLEX_ONE, ws->B, ws->P1, GSL_COMPLEX_ZERO, ws->P2);
+  for (int i = 0; i < n; i++) {
+    c->psi[i][2 * l] = gsl_vector_complex_get(ws->P2, i).dat[0];
+    c->psi[i][2 * l + 1] = gsl_vector_complex_get(ws->P2, i).dat[1];
+  }
+}
+
+/* Numerical_Bragg: state 0 couples to states 1 .. n-1, the second coupling
+ * with laser_k[1] = -laser_k[0] and chirp_rate[1] = -chirp_rate[0]; t1 is the
+ * header time (no dt/2). */
+void orc_numerical_bragg(orc_ctx *c, const orc_laser *L) {
+  const int n = c->ncomp;
+  const double t1 = c->t;
+  const double lk[2] = {L->laser_k[0], -L->laser_k[0]};
+  const double cr[2] = {L->chirp_rate[0], -L->chirp_rate[0]};
+  orc_num_ws ws;
+  num_ws_alloc(&ws, n);
+  for (long l = 0; l < c->npts; l++) {
+    double phi[ORC_MAXC], x[3];
+    gsl_matrix_complex_set_zero(ws.A);
+    gsl_matrix_complex_set_zero(ws.B);
+    num_diagonal(c, L, l, &ws, phi, x);
+    for (int i = 0; i < n - 1; i++) {
+      double re1, im1, eta[2];
+      sincos(((-L->laser_domh[0] + cr[i] * t1) * t1 + lk[i] * x[0] - 0.5 * L->phase[0]), &im1, &re1);
+      eta[0] = L->Amp[0] * re1 / 2 + L->Amp[1] * re1 / 2;
+      eta[1] = L->Amp[0] * im1 / 2 - L->Amp[1] * im1 / 2;
+      gsl_matrix_complex_set(ws.A, i + 1, 0, gsl_complex_rect(eta[0], eta[1]));
+      gsl_matrix_complex_set(ws.A, 0, i + 1, gsl_complex_rect(eta[0], -eta[1]));
+    }
+    num_apply(c, l, &ws);
+  }
+  num_ws_free(&ws);
+}
+
+/* Numerical_Raman (three states): A_22 += laser_domh, A_02 = Amp0/2 e^{ikx},
+ * A_12 = Amp1/2 e^{-ikx}. */
+void orc_numerical_raman(orc_ctx *c, const orc_laser *L) {
+  orc_num_ws ws;
+  num_ws_alloc(&ws, c->ncomp);
+  for (long l = 0; l < c->npts; l++) {
+    double phi[ORC_MAXC], x[3], re1, im1, eta[2];
+    gsl_matrix_complex_set_zero(ws.A);
+    gsl_matrix_complex_set_zero(ws.B);
+    num_diagonal(c, L, l, &ws, phi, x);
+    gsl_matrix_complex_set(ws.A, 2, 2, gsl_complex_rect(phi[2] + L->laser_domh[0], 0));
+    sincos((L->laser_k[0] * x[0]), &im1, &re1);
+    eta[0] = L->Amp[0] / 2 * re1;
+    eta[1] = L->Amp[0] / 2 * im1;
+    gsl_matrix_complex_set(ws.A, 0, 2, gsl_complex_rect(eta[0], eta[1]));
+    gsl_matrix_complex_set(ws.A, 2, 0, gsl_complex_rect(eta[0], -eta[1]));
+    eta[0] = L->Amp[1] / 2 * re1;
+    eta[1] = L->Amp[1] / 2 * im1;
+    gsl_matrix_complex_set(ws.A, 1, 2, gsl_complex_rect(eta[0], -eta[1]));
+    gsl_matrix_complex_set(ws.A, 2, 1, gsl_complex_rect(eta[0], eta[1]));
+    num_apply(c, l, &ws);
+  }
+  num_ws_free(&ws);
+}
+
 /* Step kinds: 0 = CRT_Base freeprop, 1 = CRT_Base_IF freeprop, 2 = bragg_ad,
  * 3 = bragg_ad of the three-level double_bragg program, 4 = CRT_Base_IF_2
- * freeprop, 5 = bragg_ad of the two-species bragg_ds program. */
+ * freeprop, 5 = bragg_ad of the two-species bragg_ds program, 6 = the
+ * numerical "bragg" step, 7 = the numerical "raman" step (F unused by 6, 7). */
 static void nl_dispatch(orc_ctx *c, int kind, const orc_laser *L, double F) {
   if (kind == 0) orc_nl_step(c);
   else if (kind == 1) orc_nl_if_step(c, L);
   else if (kind == 2) orc_bragg_ad(c, L, F);
   else if (kind == 3) orc_double_bragg_ad(c, L, F);
   else if (kind == 4) orc_nl_if2_step(c, L);
-  else orc_bragg_ds_ad(c, L, F);
+  else if (kind == 5) orc_bragg_ds_ad(c, L, F);
+  else if (kind == 6) orc_numerical_bragg(c, L);
+  else orc_numerical_raman(c, L);
 }
 
 /* One outer iteration of run_sequence: half, (V, full)^(Nk-1), V, half.

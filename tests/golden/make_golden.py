@@ -1,7 +1,7 @@
 """Generates the golden fixtures in this folder from the reference programs.
 
-Runs ATUS-2's own ``rt_solver``, ``bragg``, ``double_bragg``, ``bragg_ds`` and
-``sobmin`` (built unmodified
+Runs ATUS-2's own ``rt_solver``, ``bragg``, ``double_bragg``, ``bragg_ds``,
+``raman`` and ``sobmin`` (built unmodified
 from the ATUS-2 sources by ``make -C oracle ref``) single-threaded on small
 seeded inputs, and stores inputs and outputs as ``<case>.npz``.  The CPU tests
 replay every case on the oracle restatement and require bit-identical results;
@@ -125,6 +125,28 @@ BRAGGDS_CASES = [
          laser_k_2=1.0, laser_domh=4.0, laser_domh_2=2.0, laser_dk=0.0, laser_dk_2=0.1, Amp=4.0, Amp_2=3.0,
          durations=[0.0305, 0.0505], g=_G4, Delta_L=[0.0, 0.0, 0.0, 0.0], Beta=[0.0, 0.0, 0.0],
          Beta_2=[0.01, 0.0, 0.0], Alpha_2=0.35),
+]
+
+# the numerical steps of CRT_Base_IF ("raman", "bragg"): GSL eigensolver in
+# the reference, the shim's Jacobi solver in the oracle build
+_G3 = [100.0, 90.0, 80.0, 90.0, 95.0, 85.0, 80.0, 85.0, 90.0]
+_NUM_SEQ = [dict(name="raman", dt=0.001, Nk=10, duration=0.04, rabi=True),
+            dict(name="bragg", dt=0.001, Nk=10, duration=0.03, rabi=True),
+            dict(name="freeprop", dt=0.001, Nk=10, duration=0.02, rabi=True)]
+NUM_CASES = [
+    dict(name="raman1d", program="raman", dim=1, n=[256], lo=[-32.0], hi=[32.0], laser_k=2.0, laser_domh=10.0,
+         laser_dk=0.0, Amp=[8.0, 6.0], chirp=0.0, g=_G3, Delta_L=[0.0, 0.5, -0.5], Beta=[0.05], seq=_NUM_SEQ),
+    dict(name="raman2d", program="raman", dim=2, n=[64, 32], lo=[-16.0, -8.0], hi=[16.0, 8.0], laser_k=2.0,
+         laser_domh=10.0, laser_dk=0.0, Amp=[8.0, 6.0], chirp=0.0, g=_G3, Delta_L=[0.0, 0.5, -0.5],
+         Beta=[0.1, 0.05], seq=_NUM_SEQ),
+    dict(name="raman3d", program="raman", dim=3, n=[16, 8, 16], lo=[-8.0, -4.0, -8.0], hi=[8.0, 4.0, 8.0],
+         laser_k=1.5, laser_domh=10.0, laser_dk=0.0, Amp=[8.0, 6.0], chirp=0.0, g=_G3, Delta_L=[0.0, 0.5, -0.5],
+         Beta=[0.02, 0.03, -0.01], seq=_NUM_SEQ),
+    dict(name="nbragg2d", program="bragg", dim=2, n=[64, 32], lo=[-16.0, -8.0], hi=[16.0, 8.0], laser_k=2.0,
+         laser_domh=8.0, laser_dk=0.0, Amp=[4.0, 3.0], chirp=0.0, g=[100.0, 90.0, 90.0, 95.0],
+         Delta_L=[0.0, 0.3], Beta=[0.1, 0.05],
+         seq=[dict(name="bragg", dt=0.001, Nk=10, duration=0.05, rabi=True),
+              dict(name="freeprop", dt=0.001, Nk=10, duration=0.02, rabi=True)]),
 ]
 
 SOB_CASES = [
@@ -401,6 +423,62 @@ def make_bragg_ds(case, tmp):
                 xml=xml)
 
 
+def make_numerical(case, tmp):
+    """The numerical steps of CRT_Base_IF ("raman" three-state, "bragg"
+    n-state) in the raman program (three states) or the bragg program (two):
+    the first state a Thomas-Fermi-like profile with noise, the others empty."""
+    rng = np.random.default_rng(4)
+    dim, prog = case["dim"], case["program"]
+    ncomp = 3 if prog == "raman" else 2
+    h = binfmt.make_header(dim, case["n"], case["lo"], case["hi"], dt=0.001)
+    X = grid(h)
+    r2 = sum(x * x for x in X)
+    psi1 = np.sqrt(np.maximum(0.0, 1.0 - 0.1 * r2)) * (1 + 0.01 * rng.standard_normal(r2.shape))
+    psi0 = np.zeros((ncomp,) + psi1.shape, dtype=np.complex128)
+    psi0[0] = psi1
+    for k in range(ncomp):
+        binfmt.write_bin(os.path.join(tmp, f"inp_{k + 1}.bin"), h, psi0[k])
+    seq = case["seq"]
+    g = case["g"]
+    files = "".join(f"<FILENAME_{k + 1}>inp_{k + 1}.bin</FILENAME_{k + 1}>" for k in range(1, ncomp))
+    gs_xml = "".join(f"<GS_{i + 1}>{xml_vec(g[ncomp * i:ncomp * i + ncomp])}</GS_{i + 1}>" for i in range(ncomp))
+    xml = f"""<SIMULATION>
+  <DIM>{dim}</DIM>
+  <FILENAME>inp_1.bin</FILENAME>
+  {files}
+  <CONSTANTS>
+    <laser_k>{case['laser_k']!r}</laser_k><laser_dk>{case['laser_dk']!r}</laser_dk>
+    <laser_domh>{case['laser_domh']!r}</laser_domh>
+    <rabi_threshold>1.0</rabi_threshold><chirp>{case['chirp']!r}</chirp>
+  </CONSTANTS>
+  <VCONSTANTS>
+    <Amp_1>{xml_vec(case['Amp'])}</Amp_1>
+    <Alpha_1>{xml_vec([0.5] * dim)}</Alpha_1>
+    <Delta_L>{xml_vec(case['Delta_L'])}</Delta_L>
+    {gs_xml}
+    <Beta>{xml_vec(case['Beta'])}</Beta>
+  </VCONSTANTS>
+  <ALGORITHM><DT>1</DT></ALGORITHM>
+  <SEQUENCE>{seq_xml(seq, ' rabi_output_freq="each"')}</SEQUENCE>
+</SIMULATION>"""
+    open(os.path.join(tmp, "run.xml"), "w").write(xml)
+    run(prog, tmp)
+    t, psi = collect_outputs(tmp, ncomp, seq)
+    rabi = []
+    for s in range(1, len(seq) + 1):
+        rows = [ln.split() for ln in open(os.path.join(tmp, f"Rabi_{s}_0.txt")) if not ln.startswith("#")]
+        rabi += [[float(v) for v in r[1:]] for r in rows if r]
+    k0 = np.zeros((3, dim))
+    k0[1, 0] = 2 * case["laser_k"]
+    k0[2, 0] = -2 * case["laser_k"]
+    params = dict(program=prog, dim=dim, ncomp=ncomp, header_dt=0.001, algo_dt=1.0, Alpha_1=[0.5] * dim,
+                  gs=g, sequence=seq, laser_k=case["laser_k"], laser_domh=case["laser_domh"],
+                  laser_dk=case["laser_dk"], chirp=case["chirp"], Amp_1=list(case["Amp"]),
+                  Delta_L=case["Delta_L"], Beta=case["Beta"], rabi_threshold=1.0, rabi_k0=k0.tolist())
+    return dict(header=h.tobytes(), psi0=psi0, t=t, psi=psi, rabi=np.array(rabi), params=json.dumps(params),
+                xml=xml)
+
+
 def make_sob(case, tmp):
     dim = case["dim"]
     ax = "XYZ"[:dim]
@@ -427,7 +505,7 @@ def make_sob(case, tmp):
 
 
 def main():
-    if not os.path.exists(os.path.join(REF, "bragg_ds")):
+    if not os.path.exists(os.path.join(REF, "raman")):
         subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
     only = set(sys.argv[1:])
     keep = (lambda c: not only or c["name"] in only)
@@ -435,6 +513,8 @@ def main():
     CASES, BRAGG_CASES = [c for c in CASES if keep(c)], [c for c in BRAGG_CASES if keep(c)]
     DBRAGG_CASES, SOB_CASES = [c for c in DBRAGG_CASES if keep(c)], [c for c in SOB_CASES if keep(c)]
     BRAGGDS_CASES = [c for c in BRAGGDS_CASES if keep(c)]
+    global NUM_CASES
+    NUM_CASES = [c for c in NUM_CASES if keep(c)]
     for case in CASES:
         with tempfile.TemporaryDirectory() as tmp:
             d = make_rt(case, tmp)
@@ -453,6 +533,11 @@ def main():
     for case in BRAGGDS_CASES:
         with tempfile.TemporaryDirectory() as tmp:
             d = make_bragg_ds(case, tmp)
+        np.savez_compressed(os.path.join(HERE, case["name"] + ".npz"), **d)
+        print("wrote", case["name"], d["psi"].shape, d["rabi"].shape)
+    for case in NUM_CASES:
+        with tempfile.TemporaryDirectory() as tmp:
+            d = make_numerical(case, tmp)
         np.savez_compressed(os.path.join(HERE, case["name"] + ".npz"), **d)
         print("wrote", case["name"], d["psi"].shape, d["rabi"].shape)
     for case in SOB_CASES:

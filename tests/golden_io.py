@@ -13,6 +13,7 @@ RT_CASES = ["rt1d", "rt1d_tables_at_ctor", "rt2d_slit", "rt3d"]
 BRAGG_CASES = ["bragg1d", "bragg2d", "bragg3d"]
 DBRAGG_CASES = ["dbragg1d", "dbragg2d", "dbragg3d"]
 BRAGGDS_CASES = ["braggds1d", "braggds2d", "braggds3d"]
+NUM_CASES = ["raman1d", "raman2d", "raman3d", "nbragg2d"]
 SOB_CASES = ["sob1d", "sob2d", "sob3d"]
 
 

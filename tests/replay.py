@@ -18,6 +18,7 @@ import math
 import numpy as np
 
 KIND_NL, KIND_NL_IF, KIND_BRAGG_AD, KIND_DOUBLE_BRAGG_AD, KIND_NL_IF_2, KIND_BRAGG_DS_AD = 0, 1, 2, 3, 4, 5
+KIND_NUMERICAL_BRAGG, KIND_NUMERICAL_RAMAN = 6, 7
 
 
 def gaussian_pulse(tc: float, two_sigma2: float):
@@ -55,8 +56,9 @@ def run_rt(engine, p: dict, psi0, V=None, make_laser=None, on_block=None):
     p keys: dim, ncomp, header_dt (dt stored in the input file), algo_dt
     (ALGORITHM/DT), Alpha_1, gs (flat ncomp^2), sequence = list of dicts
     {name, dt, Nk, duration}, optional AMP_T pulse {tc, two_sigma2}, program
-    ('rt_solver', 'bragg', 'double_bragg' or 'bragg_ds'; bragg_ds adds Alpha_2 and
-    the *_2 laser keys).  Returns the list of (t, [psi per comp]) after every
+    ('rt_solver', 'bragg', 'double_bragg', 'bragg_ds' or 'raman'; bragg_ds adds
+    Alpha_2 and the *_2 laser keys; sequence tags freeprop, bragg_ad and the
+    numerical bragg / raman).  Returns the list of (t, [psi per comp]) after every
     block, and the Rabi sums per block of the interferometry programs (both
     species side by side for bragg_ds).
     """
@@ -76,7 +78,7 @@ def run_rt(engine, p: dict, psi0, V=None, make_laser=None, on_block=None):
     laser2 = make_laser(**laser_kwargs(p, 2)) if make_laser is not None and two_species else None
     F = gaussian_pulse(p["AMP_T"]["tc"], p["AMP_T"]["two_sigma2"]) if p.get("AMP_T") else None
     outputs, rabi = [], []
-    is_if = p["program"] in ("bragg", "double_bragg", "bragg_ds")
+    is_if = p["program"] in ("bragg", "double_bragg", "bragg_ds", "raman")
     for seq in p["sequence"]:
         durs = seq["duration"] if isinstance(seq["duration"], list) else [seq["duration"]]
         subN = int(max(durs) / seq["dt"])
@@ -88,6 +90,10 @@ def run_rt(engine, p: dict, psi0, V=None, make_laser=None, on_block=None):
         if seq["name"] == "bragg_ad":
             kind = {"double_bragg": KIND_DOUBLE_BRAGG_AD, "bragg_ds": KIND_BRAGG_DS_AD}.get(p["program"],
                                                                                          KIND_BRAGG_AD)
+        elif seq["name"] == "raman":
+            kind = KIND_NUMERICAL_RAMAN
+        elif seq["name"] == "bragg":
+            kind = KIND_NUMERICAL_BRAGG
         elif two_species:
             kind = KIND_NL_IF_2
         elif is_if:

@@ -13,12 +13,12 @@ import numpy as np
 import pytest
 
 from atus2_b200 import PREC_FP64, PREC_MIXED, Laser, Solver, binfmt
-from golden_io import BRAGG_CASES, BRAGGDS_CASES, DBRAGG_CASES, RT_CASES, SOB_CASES, load, sob_inputs
+from golden_io import BRAGG_CASES, BRAGGDS_CASES, DBRAGG_CASES, NUM_CASES, RT_CASES, SOB_CASES, load, sob_inputs
 from gpu_util import rel_l2
 from oracle.oracle import Laser as OLaser
 from oracle.oracle import Oracle
 from replay import (KIND_BRAGG_AD, KIND_BRAGG_DS_AD, KIND_DOUBLE_BRAGG_AD, KIND_NL, KIND_NL_IF, KIND_NL_IF_2,
-                    gaussian_pulse, run_rt)
+                    KIND_NUMERICAL_BRAGG, KIND_NUMERICAL_RAMAN, gaussian_pulse, run_rt)
 
 pytestmark = pytest.mark.gpu
 
@@ -42,7 +42,7 @@ def state_close(psi, ref, tol):
             assert rel_l2(psi[c], ref[c]) < tol, c
 
 
-@pytest.mark.parametrize("name", RT_CASES + BRAGG_CASES + DBRAGG_CASES + BRAGGDS_CASES)
+@pytest.mark.parametrize("name", RT_CASES + BRAGG_CASES + DBRAGG_CASES + BRAGGDS_CASES + NUM_CASES)
 def test_golden_realtime_fp64(name):
     g = load(name)
     p = g["params"]
@@ -52,7 +52,7 @@ def test_golden_realtime_fp64(name):
     for (t, psi), t_ref, psi_ref in zip(outs, g["t"], g["psi"]):
         assert t == t_ref
         state_close(psi, psi_ref, FP64_TOL)
-    if p["program"] in ("bragg", "double_bragg", "bragg_ds"):
+    if p["program"] in ("bragg", "double_bragg", "bragg_ds", "raman"):
         np.testing.assert_allclose(np.array(rabi), g["rabi"], rtol=5e-6, atol=1e-10)
 
 
@@ -452,6 +452,40 @@ def test_bragg_ds_matches_oracle(dim, prec, tol):
     k0[1, 0], k0[2, 0] = 6.0, -6.0
     np.testing.assert_allclose(s.rabi_integrals(k0, 1.0, 2), o.rabi_integrals(k0, 1.0, 2),
                                rtol=(1e-11 if prec == PREC_FP64 else 1e-4), atol=1e-12)
+
+
+@pytest.mark.parametrize("prec,tol", [(PREC_FP64, FP64_TOL), (PREC_MIXED, MIXED_TOL)])
+@pytest.mark.parametrize("dim", [1, 3])
+def test_numerical_steps_match_oracle(dim, prec, tol):
+    """The numerical "raman" and "bragg" steps of the interferometry programs
+    (a Hermitian 3x3 exponential per grid point; the reference diagonalises
+    it with GSL, the oracle with the same Jacobi solver the reference build
+    links) against the oracle: 1D 4096 points on [-64,64), 3D 32^3 on
+    [-8,8)^3, 60 raman steps, 60 bragg steps, then 60 raman steps with the
+    couplings switched off (a diagonal, degenerate matrix)."""
+    n = [4096] if dim == 1 else [32, 32, 32]
+    L = 128.0 if dim == 1 else 16.0
+    h = _grid(dim, n, L)
+    xs = _coords(h)
+    r2 = sum(x * x for x in xs)
+    psi0 = np.exp(-0.5 * r2 / (4.0 if dim == 1 else 1.5)).astype(np.complex128)
+    psi0 /= math.sqrt(float(np.prod([h[f"d{a}"] for a in "xyz"[:dim]])) * np.sum(np.abs(psi0) ** 2))
+    z = np.zeros_like(psi0)
+    o, s = _setup_pair(h, 3, [psi0, z, z], [0.5] * dim, list(np.linspace(20.0, 40.0, 9)), None, 1e-3, prec)
+    kw = dict(beta=[0.4, 0.2, 0.1][:dim] + [0] * (3 - dim), DeltaL=[0.0, 0.5, -0.3, 0], Amp=[30.0, 20.0],
+              laser_k=[4.0, 0], laser_dk=[0, 0], laser_domh=[15.0, 0], phase=[0.3, 0], chirp_rate=[2.0, 0],
+              chirp=0.0)
+    for kind, k in ((KIND_NUMERICAL_RAMAN, kw), (KIND_NUMERICAL_BRAGG, kw), (KIND_NUMERICAL_RAMAN,
+                    dict(kw, Amp=[0.0, 0.0], DeltaL=[0.0, 0.0, 0.0, 0], beta=[0, 0, 0], laser_domh=[0.0, 0]))):
+        for e, Lc in ((o, OLaser), (s, Laser)):
+            e.block(30, kind, Lc.make(**k))
+            e.block(30, kind, Lc.make(**k))
+    assert s.t == o.t
+    state_close([s.psi(c) for c in range(3)], [o.psi(c) for c in range(3)], tol)
+    n_o = [o.particle_number(c) for c in range(3)]
+    assert min(n_o[1], n_o[2]) > 1e-4  # the couplings moved population
+    np.testing.assert_allclose([s.particle_number(c) for c in range(3)], n_o,
+                               rtol=(1e-11 if prec == PREC_FP64 else 1e-5), atol=1e-14)
 
 
 def test_stable_bragg_form():

@@ -1,19 +1,19 @@
 """The oracle restatement reproduces the reference programs bit for bit.
 
 The golden fixtures were produced by ATUS-2's own rt_solver / bragg /
-double_bragg / bragg_ds / sobmin
+double_bragg / bragg_ds / raman / sobmin
 compiled from the reference sources (tests/golden/make_golden.py); the
 restatement (oracle/atus_oracle.c) replays the same XML programs here.
 """
 import numpy as np
 import pytest
 
-from golden_io import BRAGG_CASES, BRAGGDS_CASES, DBRAGG_CASES, RT_CASES, SOB_CASES, load, sob_inputs
+from golden_io import BRAGG_CASES, BRAGGDS_CASES, DBRAGG_CASES, NUM_CASES, RT_CASES, SOB_CASES, load, sob_inputs
 from oracle.oracle import Laser, Oracle
 from replay import run_rt
 
 
-@pytest.mark.parametrize("name", RT_CASES + BRAGG_CASES + DBRAGG_CASES + BRAGGDS_CASES)
+@pytest.mark.parametrize("name", RT_CASES + BRAGG_CASES + DBRAGG_CASES + BRAGGDS_CASES + NUM_CASES)
 def test_realtime_bit_exact(name):
     g = load(name)
     p = g["params"]
@@ -25,7 +25,7 @@ def test_realtime_bit_exact(name):
         assert t == t_ref
         for c in range(p["ncomp"]):
             np.testing.assert_array_equal(psi[c], psi_ref[c])
-    if p["program"] in ("bragg", "double_bragg", "bragg_ds"):
+    if p["program"] in ("bragg", "double_bragg", "bragg_ds", "raman"):
         # Rabi_<seq>_<chirp>.txt holds 6 significant digits
         np.testing.assert_allclose(np.array(rabi), g["rabi"], rtol=5e-6, atol=1e-12)
 

@@ -14,7 +14,7 @@ import numpy as np
 import pytest
 
 from atus2_b200 import binfmt
-from golden_io import BRAGG_CASES, BRAGGDS_CASES, DBRAGG_CASES, RT_CASES, SOB_CASES, load
+from golden_io import BRAGG_CASES, BRAGGDS_CASES, DBRAGG_CASES, NUM_CASES, RT_CASES, SOB_CASES, load
 from gpu_util import rel_l2
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -84,13 +84,13 @@ def _outputs(tmp, ncomp):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", RT_CASES + BRAGG_CASES + DBRAGG_CASES + BRAGGDS_CASES)
+@pytest.mark.parametrize("name", RT_CASES + BRAGG_CASES + DBRAGG_CASES + BRAGGDS_CASES + NUM_CASES)
 def test_realtime_program_matches_reference(name):
     from test_gpu_parity import FP64_TOL, state_close
 
     g = load(name)
     p = g["params"]
-    prog = p["program"] if p["program"] in ("bragg", "double_bragg", "bragg_ds") else "rt_solver"
+    prog = p["program"] if p["program"] in ("bragg", "double_bragg", "bragg_ds", "raman") else "rt_solver"
 
     def rabi_rows(path):
         return [[float(v) for v in ln.split()[1:]] for ln in open(path) if not ln.startswith("#") and ln.split()]
@@ -100,7 +100,7 @@ def test_realtime_program_matches_reference(name):
         run(prog, tmp)
         outs = _outputs(tmp, p["ncomp"])
         rabi = []
-        for s in (1, 2):
+        for s in range(1, len(p["sequence"]) + 1):
             if prog == "bragg_ds":  # Spezie_<species>_Rabi_<seq>_<chirp>.txt, species side by side
                 r1 = rabi_rows(os.path.join(tmp, f"Spezie_1_Rabi_{s}_0.txt"))
                 r2 = rabi_rows(os.path.join(tmp, f"Spezie_2_Rabi_{s}_0.txt"))
