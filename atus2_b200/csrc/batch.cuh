@@ -233,6 +233,7 @@ __global__ void __launch_bounds__(Tile2<R>::NT, Tile2<R>::MINB) batch_pass2_kern
     if (!setup) {  // twiddle rows (the same for every instance of the class)
       p2_setup<R, N, TC, M2_INV>(sa, smem_raw);
       setup = true;
+      __syncthreads();  // twiddle rows visible to every warp before the first exchange
     }
     p2_item<R, N, TC, MODE, STRIDED, false>(sa, tile_geo<Cfg::B, N>(sa, w % bp.items), smem_raw, false, s_om, s_ec,
                                             s_es);

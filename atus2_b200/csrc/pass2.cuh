@@ -80,14 +80,17 @@ __device__ __forceinline__ void p2_stage2(const cplx<R> *ex, const typename TwTa
 
 // One transform of the thread's 16 values v (stage-1 inputs j + R2 r on entry,
 // points j + R2 m on return).  The leading barrier protects the exchange rows
-// that other threads may still be reading from the previous use.
-template <typename R, int N, int DIR>
+// that other threads may still be reading from the previous use.  WARP: the
+// R2 threads of each pencil are consecutive lanes of one warp (the contiguous
+// mapping), so the exchange needs only a warp barrier; the strided mapping
+// spreads a pencil over the CTA's warps and needs the CTA barrier.
+template <typename R, int N, int DIR, bool WARP = false>
 __device__ __forceinline__ void p2_transform(cplx<R> *v, cplx<R> *ex, const typename TwTab<R>::type *twS, int j) {
   dft16<DIR>(v);
-  __syncthreads();
+  if constexpr (WARP) __syncwarp(); else __syncthreads();
   #pragma unroll
   for (int q = 0; q < 16; q++) ex[ex_at(j, q)] = v[q];
-  __syncthreads();
+  if constexpr (WARP) __syncwarp(); else __syncthreads();
   p2_stage2<R, N, DIR>(ex, twS, j, v);
 }
 
@@ -169,11 +172,11 @@ __device__ __forceinline__ void p2_item(const PassArgs &a, const TileGeo &g, uns
   for (int r = 0; r < 16; r++) v[r] = live ? (L2LOAD ? __ldcg(&src[r * step]) : src[r * step]) : mk<R>(0, 0);
 
   if constexpr (MODE == M2_FWD) {
-    p2_transform<R, N, -1>(v, my, twS, j);
+    p2_transform<R, N, -1, !STRIDED>(v, my, twS, j);
   } else if constexpr (MODE == M2_INV) {
-    p2_transform<R, N, +1>(v, my, twS, j);
+    p2_transform<R, N, +1, !STRIDED>(v, my, twS, j);
   } else if constexpr (MODE == M2_KIN) {
-    p2_transform<R, N, -1>(v, my, twS, j);
+    p2_transform<R, N, -1, !STRIDED>(v, my, twS, j);
     int p0[3];
     idx3(a.g, lb, p0[0], p0[1], p0[2]);
     if (a.op == OP_KIN) {
@@ -226,9 +229,9 @@ __device__ __forceinline__ void p2_item(const PassArgs &a, const TileGeo &g, uns
         v[m].y = (R)((double)v[m].y * fk);
       }
     }
-    p2_transform<R, N, +1>(v, my, twS, j);
+    p2_transform<R, N, +1, !STRIDED>(v, my, twS, j);
   } else {  // M2_NL: IFFT -> potential step -> FFT
-    p2_transform<R, N, +1>(v, my, twS, j);
+    p2_transform<R, N, +1, !STRIDED>(v, my, twS, j);
     if constexpr (TC == 1) {
       int p0[3];
       idx3(a.g, lb, p0[0], p0[1], p0[2]);
@@ -286,7 +289,7 @@ __device__ __forceinline__ void p2_item(const PassArgs &a, const TileGeo &g, uns
         v[r] = my[ex_at(i >> 4, i & 15)];
       }
     }
-    p2_transform<R, N, -1>(v, my, twS, j);
+    p2_transform<R, N, -1, !STRIDED>(v, my, twS, j);
   }
 
   if (live) {
@@ -296,15 +299,38 @@ __device__ __forceinline__ void p2_item(const PassArgs &a, const TileGeo &g, uns
   }
 }
 
+// Strided tiles: asks L2 for the CTA's next tile (one prefetch per 128-byte
+// line; the B pencils of a row are adjacent, the N rows sa apart) while this
+// one is transformed, so that its loads wait on L2 rather than HBM.  (The
+// same for contiguous tiles and for the plane pipeline measured slower.)
+template <typename R, int N, int TC>
+__device__ __forceinline__ void p2_prefetch_l2(const PassArgs &a, const TileGeo &g) {
+  using Cfg = P2Cfg<R, N, TC>;
+  constexpr int LINE = 128 / (int)sizeof(cplx<R>);  // complex values per 128-byte line
+  constexpr int SEG = (Cfg::B + LINE - 1) / LINE;
+  const int nc = a.per_comp ? 1 : a.nc;
+  for (int e = threadIdx.x; e < nc * N * SEG; e += Cfg::NT) {
+    const int c = e / (N * SEG), rem = e % (N * SEG);
+    const int i = rem / SEG, seg = rem % SEG;
+    if (seg * LINE >= g.nb) continue;
+    const cplx<R> *f = (const cplx<R> *)pick(a.psi, g.comp0 + c);
+    const cplx<R> *p = f + g.base0 + (int64_t)(seg * LINE) * g.pstride + (int64_t)i * a.sa;
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+  }
+}
+
 template <typename R, int N, int TC, int MODE, bool STRIDED>
 __global__ void __launch_bounds__(Tile2<R>::NT, Tile2<R>::MINB) pass2_kernel(PassArgs a) {
   using Cfg = P2Cfg<R, N, TC>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double s_om[Cfg::B], s_ec[Cfg::B], s_es[Cfg::B];
   const bool kt_shared = p2_setup<R, N, TC, MODE>(a, smem_raw);
+  __syncthreads();  // twiddle rows and kinetic factors visible to every warp
   const int64_t W = a.per_comp ? a.ntiles * a.ncomp_grid : a.ntiles;
-  for (int64_t w = blockIdx.x; w < W; w += gridDim.x)
+  for (int64_t w = blockIdx.x; w < W; w += gridDim.x) {
+    if (STRIDED && w + gridDim.x < W) p2_prefetch_l2<R, N, TC>(a, tile_geo<Cfg::B, N>(a, w + gridDim.x));
     p2_item<R, N, TC, MODE, STRIDED, false>(a, tile_geo<Cfg::B, N>(a, w), smem_raw, kt_shared, s_om, s_ec, s_es);
+  }
 }
 
 }  // namespace atus
