@@ -36,7 +36,7 @@ struct atus_ctx {
   int64_t launches = 0;
   bool use_slab = true;         // 3D: fused (y,z) cluster pass when available
   bool use_pass2 = true;        // register-staged passes for pencils of 32..256 points
-  bool use_pipe = true;         // 3D: real-space half step as one plane pipeline
+  bool use_pipe = false;        // 3D: real-space half step as one plane pipeline (ATUS_PIPE=1)
   bool pipe_mixed = false;      // ... also for complex64 fields
   PipeQueue *pipe = nullptr;    // its device-resident work queue
   unsigned pipe_epoch = 0;      // pipeline launches since the queue was zeroed

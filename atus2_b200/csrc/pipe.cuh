@@ -55,7 +55,7 @@ struct PipeCfg {
 };
 
 template <typename R, int N, int TC>
-__global__ void __launch_bounds__(Tile2<R>::NT, (sizeof(R) == 8 ? 512 : 1024) / Tile2<R>::NT) pipe_kernel(PipeArgs a) {
+__global__ void __launch_bounds__(Tile2<R>::NT, (sizeof(R) == 8 ? 512 : 768) / Tile2<R>::NT) pipe_kernel(PipeArgs a) {
   using CT = P2Cfg<R, N, 1>;
   using CZ = P2Cfg<R, N, TC>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
