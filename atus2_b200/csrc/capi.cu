@@ -1155,33 +1155,22 @@ static int sob_iterate_dev(atus_ctx *ctx) {
     RUN(sob_filter(ctx, ctx->sob_grad[i], FILT_SOBOLEV, ctx->sob_alpha[i]));
   }
   for (int i = 0; i < n; i++) {
-    RedArgs r;
+    RedArgs r;  // the projection's two products and the norm of psi in one pass
     memset(&r, 0, sizeof(r));
     r.mode = RED_DOT2;
-    r.nq = 2;
+    r.nq = 3;
     r.a = ctx->psi[i];
     r.b = ctx->sob_grad[i];
     r.c = ctx->sob_psi[i];
     RUN(reduce_dev(ctx, r, d->q[i]));
-    sob_proj_kernel<<<blocks, 256, 0, ctx->stream>>>((double2 *)ctx->sob_grad[i], (const double2 *)ctx->sob_psi[i], d,
-                                                    i, ctx->npts);
-    LAUNCHED(ctx);
-  }
-  for (int i = 0; i < n; i++) {
-    RedArgs r;
-    memset(&r, 0, sizeof(r));
-    r.mode = RED_NORM;
-    r.nq = 1;
-    r.a = ctx->sob_grad[i];
-    RUN(reduce_dev(ctx, r, &d->g2[i]));
-  }
-  for (int i = 0; i < n; i++) {
-    RedArgs r;
-    memset(&r, 0, sizeof(r));
-    r.mode = RED_NORM;
-    r.nq = 1;
-    r.a = ctx->psi[i];
-    RUN(reduce_dev(ctx, r, &d->n[i]));
+    RedArgs p;  // Project_Sobolev_Gradient fused with the norm of the projected gradient
+    memset(&p, 0, sizeof(p));
+    p.mode = RED_PROJ;
+    p.nq = 1;
+    p.w = (double2 *)ctx->sob_grad[i];
+    p.c = ctx->sob_psi[i];
+    p.fq = d->q[i];
+    RUN(reduce_dev(ctx, p, &d->g2[i]));
   }
   sob_scalars_kernel<<<1, 1, 0, ctx->stream>>>(d, ctx->ar, n);
   LAUNCHED(ctx);

@@ -997,7 +997,7 @@ struct SobArgs {
 // ------------------------------------------------------------ reductions
 // Quantities per mode (all FP64 accumulations, fixed order per thread, fixed
 // tree per block, partials summed in block order by reduce_final).
-enum { RED_NORM = 0, RED_POS = 1, RED_MOM = 2, RED_RABI = 3, RED_DOT2 = 4, RED_MU = 5 };
+enum { RED_NORM = 0, RED_POS = 1, RED_MOM = 2, RED_RABI = 3, RED_DOT2 = 4, RED_MU = 5, RED_PROJ = 6 };
 constexpr int RED_MAXQ = 8;
 constexpr int RED_BLOCKS = 592;  // 4 x 148 SMs
 constexpr int RED_THREADS = 256;
@@ -1017,11 +1017,24 @@ struct RedArgs {
   const void *psi_all[MAXC];
   int ncomp, comp;
   double gs[MAXC * MAXC];
+  // projection: w <- w - (fq[0] / fq[1]) c, then |w|^2 (FP64 fields)
+  double2 *w;
+  const double *fq;
 };
 
 template <typename R>
 __device__ __forceinline__ void red_point(const RedArgs &a, int64_t l, double *q) {
   using C = cplx<R>;
+  if (a.mode == RED_PROJ) {  // Project_Sobolev_Gradient and the norm of the result in one pass
+    const double fak = a.fq[0] / a.fq[1];
+    double2 v = a.w[l];
+    const double2 u = ((const double2 *)a.c)[l];
+    v.x -= fak * u.x;
+    v.y -= fak * u.y;
+    a.w[l] = v;
+    q[0] += v.x * v.x + v.y * v.y;
+    return;
+  }
   const C v = ((const C *)a.a)[l];
   const double den = (double)v.x * (double)v.x + (double)v.y * (double)v.y;
   if (a.mode == RED_NORM) { q[0] += den; return; }
@@ -1053,13 +1066,14 @@ __device__ __forceinline__ void red_point(const RedArgs &a, int64_t l, double *q
     }
     return;
   }
-  if (a.mode == RED_DOT2) {  // Re<a,b>, Re<a,c>
+  if (a.mode == RED_DOT2) {  // Re<a,b>, Re<a,c> (and <a,a> when nq is 3)
     const C b = ((const C *)a.b)[l];
     q[0] += (double)v.x * (double)b.x + (double)v.y * (double)b.y;
     if (a.c) {
       const C c = ((const C *)a.c)[l];
       q[1] += (double)v.x * (double)c.x + (double)v.y * (double)c.y;
     }
+    if (a.nq > 2) q[2] += den;
     return;
   }
   if (a.mode == RED_MU) {  // a = psi_i, b = Lap psi_i

@@ -54,9 +54,8 @@ __global__ void reduce_final(const double *partial, int nblocks, int nq, double 
 // runs (as a CUDA graph) without host round trips.  Per component: q = the two
 // projections Re<psi, G>, Re<psi, psi_sob>; g2 = sum |G|^2; n = sum |psi|^2.
 struct SobDev {
-  double q[MAXC][2];
+  double q[MAXC][3];    // Re<psi, G>, Re<psi, psi_sob>, <psi, psi> (one reduction)
   double g2[MAXC];
-  double n[MAXC];
   double scale[MAXC];   // renormalisation factor of this iteration (1: none)
   double res;           // residual of the last active iteration
   double N[MAXC];       // particle numbers of the last active iteration
@@ -90,7 +89,7 @@ __global__ void sob_scalars_kernel(SobDev *d, double ar, int ncomp) {
   for (int i = 0; i < ncomp; i++) {
     const double q = d->g2[i] * ar;
     res += q * q;
-    d->N[i] = ar * d->n[i];
+    d->N[i] = ar * d->q[i][2];
     if (fabs(d->N[i] - 1) > 1e-5) renorm = true;
   }
   res = sqrt(res);
