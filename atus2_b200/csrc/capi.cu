@@ -1015,46 +1015,6 @@ static int sob_renorm(atus_ctx *ctx) {
   return ATUS_OK;
 }
 
-// Compute_Sobolev_Psi and Compute_Laplace of component i with one set of
-// forward transforms along the axes after the first: psi is copied, those
-// axes are transformed once, and the copy is split into the Sobolev-filtered
-// and the Laplacian buffers, each finished by its own axis-0 filter pass and
-// the inverse transforms -- the same operations on the same values as two
-// sob_filter calls, so the results are identical.
-static int sob_filter_pair(atus_ctx *ctx, int i) {
-  const int saved = ctx->prec;
-  ctx->prec = ATUS_PREC_FP64;
-  void *fs[1] = {ctx->sob_psi[i]}, *fl[1] = {ctx->sob_lap[i]};
-  int r = ATUS_OK;
-  if (cudaMemcpyAsync(ctx->sob_psi[i], ctx->psi[i], 16 * ctx->npts, cudaMemcpyDeviceToDevice, ctx->stream) != cudaSuccess)
-    r = fail(ctx, ATUS_E_CUDA, "sob_filter_pair copy");
-  for (int ax = ctx->dim - 1; ax >= 1 && r == ATUS_OK; ax--) r = run_pass(ctx, ax, T_FWD, OP_NONE, T_NONE, nullptr, 0, fs, 1);
-  if (r == ATUS_OK &&
-      cudaMemcpyAsync(ctx->sob_lap[i], ctx->sob_psi[i], 16 * ctx->npts, cudaMemcpyDeviceToDevice, ctx->stream) != cudaSuccess)
-    r = fail(ctx, ATUS_E_CUDA, "sob_filter_pair copy");
-  for (int k = 0; k < 2 && r == ATUS_OK; k++) {
-    PassArgs a;
-    memset(&a, 0, sizeof(a));
-    a.psi[0] = k == 0 ? ctx->sob_psi[i] : ctx->sob_lap[i];
-    a.t1 = T_FWD;
-    a.op = OP_FILT;
-    a.t2 = T_INV;
-    a.per_comp = 1;
-    a.nc = 1;
-    a.filt_mode = k == 0 ? FILT_SOBOLEV : FILT_LAPLACE;
-    a.filt_alpha = ctx->sob_alpha[i];
-    a.filt_scale = round_trip_scale(ctx);
-    const int saved_nc = ctx->ncomp;
-    ctx->ncomp = 1;
-    r = dispatch_pass(ctx, a, 0, 1);
-    ctx->ncomp = saved_nc;
-  }
-  for (int ax = 1; ax < ctx->dim && r == ATUS_OK; ax++) r = run_pass(ctx, ax, T_INV, OP_NONE, T_NONE, nullptr, 0, fs, 1);
-  for (int ax = 1; ax < ctx->dim && r == ATUS_OK; ax++) r = run_pass(ctx, ax, T_INV, OP_NONE, T_NONE, nullptr, 0, fl, 1);
-  ctx->prec = saved;
-  return r;
-}
-
 static int sob_laplace(atus_ctx *ctx) {
   for (int i = 0; i < ctx->ncomp; i++) {
     CK(cudaMemcpyAsync(ctx->sob_lap[i], ctx->psi[i], 16 * ctx->npts, cudaMemcpyDeviceToDevice, ctx->stream));
@@ -1135,15 +1095,22 @@ static int sob_iterate_once(atus_ctx *ctx, double *res_out, double *N_out) {
 // the same kernels and reductions in the same order; psi changes only in an
 // active iteration (not yet converged, below max_iter).
 static int sob_iterate_dev(atus_ctx *ctx) {
+  // The reference's gradient S(-Lap psi + W psi), W = V + sum_j g_ij |psi_j|^2,
+  // S = 1/(1 + alpha k^2), taken as S(W psi) + psi - S psi: S alpha k^2 = 1 - S,
+  // so the Laplacian's transforms drop out (two filters per component instead
+  // of three; the same quantities up to rounding).
   const int n = ctx->ncomp;
   const int blocks = grid_blocks(ctx->npts, 256);
   SobDev *d = (SobDev *)ctx->sob_dev;
-  for (int i = 0; i < n; i++) RUN(sob_filter_pair(ctx, i));  // Compute_Sobolev_Psi and Compute_Laplace
-  for (int i = 0; i < n; i++) {
+  for (int i = 0; i < n; i++) {  // Compute_Sobolev_Psi
+    CK(cudaMemcpyAsync(ctx->sob_psi[i], ctx->psi[i], 16 * ctx->npts, cudaMemcpyDeviceToDevice, ctx->stream));
+    RUN(sob_filter(ctx, ctx->sob_psi[i], FILT_SOBOLEV, ctx->sob_alpha[i]));
+  }
+  for (int i = 0; i < n; i++) {  // S(W psi)
     SobArgs a;
     memset(&a, 0, sizeof(a));
     for (int j = 0; j < MAXC; j++) a.psi[j] = (const double2 *)ctx->psi[j];
-    a.lap = (const double2 *)ctx->sob_lap[i];
+    a.lap = nullptr;
     a.V = ctx->V[i];
     a.grad = (double2 *)ctx->sob_grad[i];
     a.comp = i;
@@ -1155,13 +1122,13 @@ static int sob_iterate_dev(atus_ctx *ctx) {
     RUN(sob_filter(ctx, ctx->sob_grad[i], FILT_SOBOLEV, ctx->sob_alpha[i]));
   }
   for (int i = 0; i < n; i++) {
-    RedArgs r;  // the projection's two products and the norm of psi in one pass
+    RedArgs r;  // G = S(W psi) + psi - S psi, the projection's two products and <psi, psi> in one pass
     memset(&r, 0, sizeof(r));
-    r.mode = RED_DOT2;
+    r.mode = RED_SOBG;
     r.nq = 3;
     r.a = ctx->psi[i];
-    r.b = ctx->sob_grad[i];
     r.c = ctx->sob_psi[i];
+    r.w = (double2 *)ctx->sob_grad[i];
     RUN(reduce_dev(ctx, r, d->q[i]));
     RedArgs p;  // Project_Sobolev_Gradient fused with the norm of the projected gradient
     memset(&p, 0, sizeof(p));

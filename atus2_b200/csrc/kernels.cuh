@@ -997,7 +997,7 @@ struct SobArgs {
 // ------------------------------------------------------------ reductions
 // Quantities per mode (all FP64 accumulations, fixed order per thread, fixed
 // tree per block, partials summed in block order by reduce_final).
-enum { RED_NORM = 0, RED_POS = 1, RED_MOM = 2, RED_RABI = 3, RED_DOT2 = 4, RED_MU = 5, RED_PROJ = 6 };
+enum { RED_NORM = 0, RED_POS = 1, RED_MOM = 2, RED_RABI = 3, RED_DOT2 = 4, RED_MU = 5, RED_PROJ = 6, RED_SOBG = 7 };
 constexpr int RED_MAXQ = 8;
 constexpr int RED_BLOCKS = 592;  // 4 x 148 SMs
 constexpr int RED_THREADS = 256;
@@ -1025,6 +1025,20 @@ struct RedArgs {
 template <typename R>
 __device__ __forceinline__ void red_point(const RedArgs &a, int64_t l, double *q) {
   using C = cplx<R>;
+  if (a.mode == RED_SOBG) {
+    // w = S(W psi) becomes the Sobolev gradient S(-Lap psi + W psi) =
+    // S(W psi) + psi - S psi (S = 1/(1 + alpha k^2), so S alpha k^2 = 1 - S),
+    // then Re<psi, G>, Re<psi, S psi>, <psi, psi>
+    const double2 p = ((const double2 *)a.a)[l], ps = ((const double2 *)a.c)[l];
+    double2 g = a.w[l];
+    g.x += p.x - ps.x;
+    g.y += p.y - ps.y;
+    a.w[l] = g;
+    q[0] += p.x * g.x + p.y * g.y;
+    q[1] += p.x * ps.x + p.y * ps.y;
+    q[2] += p.x * p.x + p.y * p.y;
+    return;
+  }
   if (a.mode == RED_PROJ) {  // Project_Sobolev_Gradient and the norm of the result in one pass
     const double fak = a.fq[0] / a.fq[1];
     double2 v = a.w[l];

@@ -15,8 +15,13 @@ __global__ void sob_assemble_kernel(SobArgs a) {
       }
     }
     const double pot = a.V ? a.V[l] : 0.0;
-    const double2 p = a.psi[a.comp][l], L = a.lap[l];
-    a.grad[l] = make_double2(-L.x + (pot + nl) * p.x, -L.y + (pot + nl) * p.y);
+    const double2 p = a.psi[a.comp][l];
+    if (a.lap) {
+      const double2 L = a.lap[l];
+      a.grad[l] = make_double2(-L.x + (pot + nl) * p.x, -L.y + (pot + nl) * p.y);
+    } else {  // the potential term alone (W psi)
+      a.grad[l] = make_double2((pot + nl) * p.x, (pot + nl) * p.y);
+    }
   }
 }
 
