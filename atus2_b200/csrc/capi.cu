@@ -972,16 +972,15 @@ int atus_rabi_integrals_comp(atus_ctx *ctx, int comp, const double *k0, int n, d
 // ------------------------------------------------------------------ Sobolev gradient
 // Real k-space filter of an FP64 buffer over all axes: forward transforms,
 // filter inside the axis-0 pass, inverse transforms.
-static int sob_filter(atus_ctx *ctx, void *buf, int mode, double alpha) {
+static int sob_filter_n(atus_ctx *ctx, void *const *bufs, int nb, int mode, double alpha) {
   const int saved = ctx->prec;
   ctx->prec = ATUS_PREC_FP64;
-  void *f[1] = {buf};
   int r = ATUS_OK;
-  for (int ax = ctx->dim - 1; ax >= 1 && r == ATUS_OK; ax--) r = run_pass(ctx, ax, T_FWD, OP_NONE, T_NONE, nullptr, 0, f, 1);
+  for (int ax = ctx->dim - 1; ax >= 1 && r == ATUS_OK; ax--) r = run_pass(ctx, ax, T_FWD, OP_NONE, T_NONE, nullptr, 0, bufs, nb);
   if (r == ATUS_OK) {
     PassArgs a;
     memset(&a, 0, sizeof(a));
-    a.psi[0] = buf;
+    for (int k = 0; k < nb; k++) a.psi[k] = bufs[k];
     a.t1 = T_FWD;
     a.op = OP_FILT;
     a.t2 = T_INV;
@@ -991,13 +990,18 @@ static int sob_filter(atus_ctx *ctx, void *buf, int mode, double alpha) {
     a.filt_alpha = alpha;
     a.filt_scale = round_trip_scale(ctx);
     const int saved_nc = ctx->ncomp;
-    ctx->ncomp = 1;
+    ctx->ncomp = nb;
     r = dispatch_pass(ctx, a, 0, 1);
     ctx->ncomp = saved_nc;
   }
-  for (int ax = 1; ax < ctx->dim && r == ATUS_OK; ax++) r = run_pass(ctx, ax, T_INV, OP_NONE, T_NONE, nullptr, 0, f, 1);
+  for (int ax = 1; ax < ctx->dim && r == ATUS_OK; ax++) r = run_pass(ctx, ax, T_INV, OP_NONE, T_NONE, nullptr, 0, bufs, nb);
   ctx->prec = saved;
   return r;
+}
+
+static int sob_filter(atus_ctx *ctx, void *buf, int mode, double alpha) {
+  void *f[1] = {buf};
+  return sob_filter_n(ctx, f, 1, mode, alpha);
 }
 
 static int sob_norms(atus_ctx *ctx, double *N) {
@@ -1102,11 +1106,8 @@ static int sob_iterate_dev(atus_ctx *ctx) {
   const int n = ctx->ncomp;
   const int blocks = grid_blocks(ctx->npts, 256);
   SobDev *d = (SobDev *)ctx->sob_dev;
-  for (int i = 0; i < n; i++) {  // Compute_Sobolev_Psi
+  for (int i = 0; i < n; i++) {  // S psi (Compute_Sobolev_Psi) and S(W psi), filtered together
     CK(cudaMemcpyAsync(ctx->sob_psi[i], ctx->psi[i], 16 * ctx->npts, cudaMemcpyDeviceToDevice, ctx->stream));
-    RUN(sob_filter(ctx, ctx->sob_psi[i], FILT_SOBOLEV, ctx->sob_alpha[i]));
-  }
-  for (int i = 0; i < n; i++) {  // S(W psi)
     SobArgs a;
     memset(&a, 0, sizeof(a));
     for (int j = 0; j < MAXC; j++) a.psi[j] = (const double2 *)ctx->psi[j];
@@ -1119,7 +1120,8 @@ static int sob_iterate_dev(atus_ctx *ctx) {
     a.npts = ctx->npts;
     sob_assemble_kernel<<<blocks, 256, 0, ctx->stream>>>(a);
     LAUNCHED(ctx);
-    RUN(sob_filter(ctx, ctx->sob_grad[i], FILT_SOBOLEV, ctx->sob_alpha[i]));
+    void *bufs[2] = {ctx->sob_psi[i], ctx->sob_grad[i]};
+    RUN(sob_filter_n(ctx, bufs, 2, FILT_SOBOLEV, ctx->sob_alpha[i]));
   }
   for (int i = 0; i < n; i++) {
     RedArgs r;  // G = S(W psi) + psi - S psi, the projection's two products and <psi, psi> in one pass
