@@ -1107,13 +1107,13 @@ static int sob_iterate_dev(atus_ctx *ctx) {
   const int blocks = grid_blocks(ctx->npts, 256);
   SobDev *d = (SobDev *)ctx->sob_dev;
   for (int i = 0; i < n; i++) {  // S psi (Compute_Sobolev_Psi) and S(W psi), filtered together
-    CK(cudaMemcpyAsync(ctx->sob_psi[i], ctx->psi[i], 16 * ctx->npts, cudaMemcpyDeviceToDevice, ctx->stream));
-    SobArgs a;
+    SobArgs a;  // W psi into the gradient buffer, psi into the Sobolev buffer, one pass
     memset(&a, 0, sizeof(a));
     for (int j = 0; j < MAXC; j++) a.psi[j] = (const double2 *)ctx->psi[j];
     a.lap = nullptr;
     a.V = ctx->V[i];
     a.grad = (double2 *)ctx->sob_grad[i];
+    a.copy = (double2 *)ctx->sob_psi[i];
     a.comp = i;
     a.ncomp = n;
     for (int k = 0; k < MAXC * MAXC; k++) a.gs[k] = ctx->gs[k];

@@ -989,6 +989,7 @@ struct SobArgs {
   const double2 *lap;
   const double *V;
   double2 *grad;
+  double2 *copy;  // when set, also receives psi[comp]
   int comp, ncomp;
   double gs[MAXC * MAXC];
   int64_t npts;

@@ -16,6 +16,7 @@ __global__ void sob_assemble_kernel(SobArgs a) {
     }
     const double pot = a.V ? a.V[l] : 0.0;
     const double2 p = a.psi[a.comp][l];
+    if (a.copy) a.copy[l] = p;
     if (a.lap) {
       const double2 L = a.lap[l];
       a.grad[l] = make_double2(-L.x + (pot + nl) * p.x, -L.y + (pot + nl) * p.y);
