@@ -488,6 +488,27 @@ def test_numerical_steps_match_oracle(dim, prec, tol):
                                rtol=(1e-11 if prec == PREC_FP64 else 1e-5), atol=1e-14)
 
 
+@pytest.mark.parametrize("prec,tol", [(PREC_FP64, FP64_TOL), (PREC_MIXED, MIXED_TOL)])
+def test_numerical_bragg_two_states_1d(prec, tol):
+    """The numerical "bragg" step with two components in 1D, where it runs
+    through the per-step kinetic pass and point-wise potential kernel (it
+    reads the header time), against the oracle: 4096 points on [-64,64), 3 x
+    40 steps with a chirp, so the header time enters the coupling phase."""
+    h = _grid(1, [4096], 128.0)
+    (x,) = _coords(h)
+    psi0 = np.exp(-x * x / 8.0).astype(np.complex128)
+    psi0 /= math.sqrt(float(h["dx"]) * np.sum(np.abs(psi0) ** 2))
+    o, s = _setup_pair(h, 2, [psi0, np.zeros_like(psi0)], [0.5], [30.0, 25.0, 25.0, 28.0], None, 1e-3, prec)
+    kw = dict(beta=[0.3, 0, 0], DeltaL=[0.0, 0.4, 0, 0], Amp=[20.0, 12.0], laser_k=[3.0, 0], laser_dk=[0, 0],
+              laser_domh=[9.0, 0], phase=[0.2, 0], chirp_rate=[4.0, 0], chirp=0.0)
+    for _ in range(3):
+        o.block(40, KIND_NUMERICAL_BRAGG, OLaser.make(**kw))
+        s.block(40, KIND_NUMERICAL_BRAGG, Laser.make(**kw))
+    assert s.t == o.t
+    state_close([s.psi(c) for c in range(2)], [o.psi(c) for c in range(2)], tol)
+    assert o.particle_number(1) > 1e-3
+
+
 def test_stable_bragg_form():
     """The eigenvalue-free FP64 Bragg step agrees with the reference's
     eigen-form where that one is sound, and stays unitary in a pulse tail
