@@ -21,7 +21,10 @@ struct P5Cfg {
   static constexpr int NT = E / VPT;         // 128 threads
   static constexpr int B = E / (N * TC);     // pencils per tile
   static constexpr int NPC = B * TC;
-  static constexpr int PB = 17 * 32 + 4;     // exchange pitch, = 4 mod 16: conflict-free for both thread layouts
+  // exchange pitch in 8-byte values, = 2 mod 16: in the strided layout the
+  // 16 lanes of a half warp are 8 pencils b x 2 rows j, at b * PB + j (mod 16)
+  // -- distinct; in the contiguous layout they are 16 columns of one pencil
+  static constexpr int PB = 17 * 32 + 2;
   static constexpr int TP = 33;              // twiddle row pitch
   static constexpr size_t smem_ex = sizeof(cplx<R>) * NPC * PB;
   static constexpr size_t smem = smem_ex + sizeof(typename TwTab<R>::type) * 16 * TP;
