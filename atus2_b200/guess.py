@@ -16,7 +16,7 @@ The network trains (atus_guess_train, hand-written CUDA kernels) on the
 coefficients of ground states that plain sobmin itself computed: the
 projections of each converged state on the basis.  Plain sobmin from the
 Thomas-Fermi guess stays the fallback; the converged residual and chemical
-potential judge the learned guess.
+potential tell how good the learned guess was.
 
     python -m atus2_b200.guess generate --count 256 --out atus2_b200/data/sob_train_64.npz
 """

@@ -2,7 +2,7 @@
 fixtures of the reference programs.
 
 Tolerances: FP64 path relative L2 <= 1e-11 against the reference / oracle
-(north-star bar); mixed path (complex64 fields, FP64 phase arguments)
+(the drop-in bar); mixed path (complex64 fields, FP64 phase arguments)
 relative L2 <= 1e-4 after the few hundred steps these tests run (the
 random-walk growth of complex64 transform rounding; bench.py reports the
 error after the full step counts).
