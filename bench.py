@@ -311,7 +311,7 @@ def run_cpu_baseline(n_steps_sample=(1, 3)):
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
 # FP64 kernels, from one ncu capture each (profiles/pass2_potential_fp64_bragg256.md,
 # profiles/pipe_kernel_fp64_bragg256.md, profiles/pass2_kinetic_fp64_bragg256.md).
-NCU_TRAFFIC_FP64 = {"pass2_kernel M2_NL (z)": 1.0769e9, "pipe_kernel": 1.0204e9, "pass2_kernel M2_KIN": 1.0142e9}
+NCU_TRAFFIC_FP64 = {"pass2_kernel M2_NL (z)": 1.0769e9, "pipe_kernel": 1.0204e9, "pass2_kernel M2_KIN": 1.0433e9}
 
 
 def roofline(s, kind, peak, peak_kind, fp64=True):
