@@ -208,7 +208,7 @@ __device__ __forceinline__ void p5_item(const PassArgs &a, const TileGeo &g, uns
       __syncthreads();
       constexpr int PPT = 32 / TC;
       const bool bragg = (a.nl.kind == K_BRAGG);
-      #pragma unroll 2
+      #pragma unroll 1  // as the 256-point passes: the rolled loop measured faster
       for (int u_ = 0; u_ < PPT; u_++) {
         const int p = tid + NT * u_;
         int pb, i;
