@@ -69,10 +69,42 @@ __global__ void na_final_kernel(const double *__restrict__ partials, int nchunks
 }
 
 // Device address of na_partials, looked up once per device with that device
-// current (the first call on the device does it).
+// current (the first call on the device does it), together with the id of the
+// CUDA context it belongs to.  Context ids are never reused within a process,
+// so after cudaDeviceReset (a new primary context, the module loaded again at
+// another address) the next call sees a different id and looks the address
+// up again instead of launching with a stale one.
 constexpr int NA_MAX_DEVICES = 64;
-double *na_addr[NA_MAX_DEVICES];
+struct NaSlot {
+  unsigned long long ctx_id;
+  double *addr;
+};
+NaSlot na_slot[NA_MAX_DEVICES];
 std::mutex na_mu;
+
+// cuCtxGetCurrent and cuCtxGetId through the runtime's driver entry points
+// (no link against the driver library); null where the driver lacks them.
+using CtxGetCurrentFn = int (*)(void **);
+using CtxGetIdFn = int (*)(void *, unsigned long long *);
+template <typename F> F na_driver_fn(const char *name) {
+  void *fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPointByVersion(name, &fn, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+      q != cudaDriverEntryPointSuccess)
+    return nullptr;
+  return reinterpret_cast<F>(fn);
+}
+
+// Id of the calling thread's current context; false when there is none yet
+// (the runtime creates the primary context on its first real call) or the
+// driver cannot tell.
+bool na_current_ctx(unsigned long long *id) {
+  static const CtxGetCurrentFn get_cur = na_driver_fn<CtxGetCurrentFn>("cuCtxGetCurrent");
+  static const CtxGetIdFn get_id = na_driver_fn<CtxGetIdFn>("cuCtxGetId");
+  void *ctx = nullptr;
+  if (!get_cur || !get_id || get_cur(&ctx) != 0 || !ctx) return false;
+  return get_id(ctx, id) == 0;
+}
 
 }  // namespace
 
@@ -86,12 +118,20 @@ extern "C" ATUS_API int atus_particle_number_noalloc(const void *psi_dev, int64_
   double *partials = nullptr;
   {
     std::lock_guard<std::mutex> lock(na_mu);
-    if (!na_addr[dev]) {
+    unsigned long long id = 0;
+    const bool known = na_current_ctx(&id);
+    NaSlot &slot = na_slot[dev];
+    if (!slot.addr || !known || slot.ctx_id != id) {
       void *p = nullptr;
       if (cudaGetSymbolAddress(&p, na_partials) != cudaSuccess || !p) return ATUS_E_CUDA;
-      na_addr[dev] = static_cast<double *>(p);
+      // the lookup made the device's context current; without a context id
+      // the address is not cached and every call looks it up
+      slot.addr = na_current_ctx(&id) ? static_cast<double *>(p) : nullptr;
+      slot.ctx_id = id;
+      partials = static_cast<double *>(p);
+    } else {
+      partials = slot.addr;
     }
-    partials = na_addr[dev];
   }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int nchunks = (int)((npts + NA_CHUNK - 1) / NA_CHUNK);

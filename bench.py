@@ -17,6 +17,14 @@ through the C ABI with host buffers -- every step of the e2e loop is one
 output block of 100 Strang steps framed by the host->device upload and the
 device->host download of both components (pinned host memory).
 
+Variants in the same JSON line: the mixed-precision form of the same
+workload (complex64 fields, FP64 phase arguments) with its error against the
+FP64 path after 10^4 steps (5000 pulse + 5000 free steps); the 1D rt_solver
+workload (N = 4096, 20000 steps) and the 2D double slit (2048^2, FP64 and
+mixed, 10^4-step accuracy); the batched Bragg sweep; sobmin time to residual
+1e-10 with and without the learned guess.  Each carries the reference
+program's rate on this host's cores where one is timed.
+
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl atus|reference]
 """
 from __future__ import annotations
@@ -260,27 +268,300 @@ def run_e2e(steps, stream):
     return ms, 2 * 16 * npts, 2 * 16 * npts
 
 
-def run_cpu_baseline(n_steps_sample=(1, 3)):
-    """The reference program (oracle/_ref/bragg, built from the ATUS-2 sources
-    with the FFTW-API shim) on this host's cores: two runs of the 256^3 Bragg
-    workload of n1 and n2 Strang steps; (t2 - t1)/(n2 - n1) is the steady
-    per-step cost with the set-up cancelled."""
-    prog = os.path.join(ROOT, "oracle", "_ref", "bragg")
-    if not os.path.exists(prog):
-        return None
+# ------------------------------------------------------------------ accuracy at full length
+ACC_PULSE_STEPS, ACC_FREE_STEPS, ACC_NK = 5000, 5000, 1000
+
+
+def _norm(s, ncomp):
+    return sum(s.particle_number(c) for c in range(ncomp))
+
+
+def run_accuracy3(stream):
+    """The 256^3 Bragg workload at full length from t = 0: 5000 bragg_ad steps
+    (pulse centred at 2.5, sigma 0.5) then 5000 freeprop steps, in blocks of
+    1000, in FP64 and in mixed precision.  The FP64 GPU path is the yardstick
+    (it matches the oracle to 1e-11 at this grid in the tests; the oracle
+    itself would need hours for 10^4 steps).  Returns the relative L2 error of
+    the mixed state per component and in total, the norm drift of both forms
+    and the Rabi populations."""
+    import torch
+
+    from atus2_b200 import PREC_FP64, PREC_MIXED, STEP_BRAGG_AD, STEP_NL_IF, Laser, Solver
+
+    h = header()
+    h["t"] = 0.0
+    psi1, psi2 = initial_state(h)
+    res = {}
+    final = {}
+    for name, prec in (("fp64", PREC_FP64), ("mixed", PREC_MIXED)):
+        s = Solver(h, 2, prec)
+        s.set_stream(stream.cuda_stream)
+        s.set_psi(0, psi1)
+        s.set_psi(1, psi2)
+        for c in range(2):
+            s.set_alpha(c, [0.5, 0.5, 0.5])
+        s.set_gs([G] * 4)
+        s.set_dt(DT)
+        s.set_laser(Laser.make(**laser_kw()))
+        n0 = _norm(s, 2)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(ACC_PULSE_STEPS // ACC_NK):
+            s.block(ACC_NK, STEP_BRAGG_AD, None, pulse_train(s.t, ACC_NK))
+        pops_pulse = [s.particle_number(c) for c in range(2)]
+        for _ in range(ACC_FREE_STEPS // ACC_NK):
+            s.block(ACC_NK, STEP_NL_IF)
+        s.synchronize()
+        wall = time.perf_counter() - t0
+        n1 = _norm(s, 2)
+        res[name] = {"norm_drift": (n1 - n0) / n0, "populations_after_pulse": pops_pulse,
+                     "populations_end": [s.particle_number(c) for c in range(2)], "wall_s": wall}
+        final[name] = [s.psi(c) for c in range(2)]
+        s.close()
+    ref, got = final["fp64"], final["mixed"]
+    err = [float(np.linalg.norm(g - r) / np.linalg.norm(r)) for g, r in zip(got, ref)]
+    tot = float(math.sqrt(sum(np.linalg.norm(g - r) ** 2 for g, r in zip(got, ref)) /
+                          sum(np.linalg.norm(r) ** 2 for r in ref)))
+    res["mixed"]["rel_l2_vs_fp64"] = {"component_1": err[0], "component_2": err[1], "state": tot}
+    res["steps"] = ACC_PULSE_STEPS + ACC_FREE_STEPS
+    res["sequence"] = (f"{ACC_PULSE_STEPS} bragg_ad + {ACC_FREE_STEPS} freeprop steps from t = 0, blocks of {ACC_NK}, "
+                       "dt = 1e-3")
+    res["bar"] = "relative L2 <= 1e-5 against FP64 after 10^4 steps"
+    return res
+
+
+# ------------------------------------------------------------------ config 1: 1D rt_solver
+C1_N, C1_NK, C1_BLOCKS = 4096, 1000, 20
+
+
+def config1_inputs():
+    """N = 4096 on [-100,100), V = x^2/2, psi = exp(-(x-5)^2/2) e^{2ix} plus
+    complex noise of amplitude 1e-6 (seed 0), normalised; g = 10, dt = 1e-3."""
     from atus2_b200 import binfmt
 
+    h = binfmt.make_header(1, [C1_N], [-100.0], [100.0], dt=DT)
+    x = binfmt.x_coords(h, 0)
+    rng = np.random.default_rng(0)
+    psi = np.exp(-0.5 * (x - 5) ** 2) * np.exp(2j * x) + 1e-6 * (rng.standard_normal(C1_N) +
+                                                              1j * rng.standard_normal(C1_N))
+    psi /= math.sqrt(float(h["dx"]) * float(np.sum(np.abs(psi) ** 2)))
+    return h, psi, 0.5 * x * x
+
+
+def run_config1(stream, with_cpu):
+    """Config 1 at full length: 20 blocks of 1000 Strang steps of the 1D
+    rt_solver workload, FP64, one CTA holding the field in shared memory."""
+    import torch
+
+    from atus2_b200 import PREC_FP64, STEP_NL, Solver
+
+    h, psi, V = config1_inputs()
+    s = Solver(h, 1, PREC_FP64)
+    s.set_stream(stream.cuda_stream)
+    s.set_psi(0, psi)
+    s.set_alpha(0, [0.5])
+    s.set_gs([10.0])
+    s.set_potential(0, V)
+    s.set_dt(DT)
+    s.block(C1_NK, STEP_NL)  # warm-up block (state advances; timing only)
+    s.set_psi(0, psi)
+    s.t = 0.0
+    n0 = s.particle_number(0)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = s.launches
+    e0.record(stream)
+    for _ in range(C1_BLOCKS):
+        s.block(C1_NK, STEP_NL)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    steps = C1_NK * C1_BLOCKS
+    out = {
+        "metric": "grid-pt-steps/s (1D rt_solver, N=4096, FP64)",
+        "value": C1_N * steps / (ms * 1e-3),
+        "unit": UNIT,
+        "ms": ms,
+        "steps": steps,
+        "us_per_step": ms * 1e3 / steps,
+        "gpu_launches": s.launches - l0,
+        "norm_drift": (s.particle_number(0) - n0) / n0,
+        "dtype": "f64",
+        "bound": "latency / FP64 issue of one SM: the 64 KB field stays in one CTA's shared memory for a "
+                 "whole block, so HBM is not on the path (72 B/pt-step model: "
+                 f"{72.0 * C1_N * steps / (ms * 1e-3) / 1e9:.1f} GB/s equivalent)",
+    }
+    s.close()
+    if with_cpu and _ref_prog("rt_solver"):
+        from atus2_b200 import binfmt
+
+        def inputs(tmp):
+            binfmt.write_bin(os.path.join(tmp, "inp_1.bin"), h, psi)
+
+        def xml(ns):
+            return f"""<SIMULATION>
+  <DIM>1</DIM><FILENAME>inp_1.bin</FILENAME><POTENTIAL_1D>0.5*x*x</POTENTIAL_1D>
+  <CONSTANTS><unused>0</unused></CONSTANTS>
+  <VCONSTANTS><Alpha_1>0.5</Alpha_1><GS_1>10</GS_1></VCONSTANTS>
+  <ALGORITHM><DT>0.001</DT></ALGORITHM>
+  <SEQUENCE><freeprop dt="0.001" Nk="{ns}" output_freq="none" pn_freq="none">{ns * DT!r}</freeprop></SEQUENCE>
+</SIMULATION>"""
+
+        r = time_ref_program(_ref_prog("rt_solver"), inputs, xml, 1000, 5000, repeats=3)
+        if r:
+            out["cpu_reference"] = {"value": C1_N / r["per_step_s"], "unit": UNIT, "cores": r["cores"],
+                                    "kind": "reference", "sample": f"ATUS-2 rt_solver (oracle/_ref, shim FFT), "
+                                    f"{r['runs']} freeprop steps, difference of medians", "wall_s": r["wall_s"]}
+    return out
+
+
+# ------------------------------------------------------------------ config 2: 2D double slit
+C2_N, C2_L, C2_DT, C2_G = 2048, 128.0, 5e-4, 1.0
+C2_V_EXPR = "200*rect(x,-0.5,0.5)*(1-rect(y,-5,-3)-rect(y,3,5))"
+
+
+def config2_inputs():
+    """2048^2 on [-64,64)^2: V = 200 on |x| < 0.5 except the slits |y -+ 4| < 1,
+    packet exp(-((x+20)^2 + y^2)/32) e^{8ix} normalised, g = 1, dt = 5e-4."""
+    from atus2_b200 import binfmt
+
+    h = binfmt.make_header(2, [C2_N, C2_N], [-C2_L / 2] * 2, [C2_L / 2] * 2, dt=C2_DT)
+    x = binfmt.x_coords(h, 0)[:, None]
+    y = binfmt.x_coords(h, 1)[None, :]
+    V = np.where((np.abs(x) < 0.5) & ~((np.abs(y - 4) < 1) | (np.abs(y + 4) < 1)), 200.0, 0.0)
+    psi = np.exp(-((x + 20) ** 2 + y ** 2) / 32.0) * np.exp(8j * x)
+    psi /= math.sqrt(float(h["dx"] * h["dy"]) * float(np.sum(np.abs(psi) ** 2)))
+    return h, psi, V
+
+
+def _c2_solver(prec, stream, h, psi, V):
+    from atus2_b200 import Solver
+
+    s = Solver(h, 1, prec)
+    s.set_stream(stream.cuda_stream)
+    s.set_psi(0, psi)
+    s.set_alpha(0, [0.5, 0.5])
+    s.set_gs([C2_G])
+    s.set_potential(0, V)
+    s.set_dt(C2_DT)
+    return s
+
+
+def run_config2(stream, steps, warmup, peak, peak_kind, with_cpu, accuracy=True):
+    """Config 2: throughput of `steps` Strang steps as one block (fields
+    resident), FP64 and mixed, with the per-pass roofline (72 B/pt-step FP64,
+    40 B mixed: 2 half steps x read+write of the field + the FP64 potential);
+    then 10^4 steps (10 blocks of 1000) of both forms for the mixed form's
+    error and the norm drift."""
+    import torch
+
+    from atus2_b200 import PREC_FP64, PREC_MIXED, STEP_NL
+
+    h, psi, V = config2_inputs()
+    npts = C2_N * C2_N
+    out = {"metric": "grid-pt-steps/s (2D double slit, 2048^2)", "unit": UNIT,
+           "l2": "field 64 MB (FP64) + potential 32 MB: below the 126 MB L2 in part; DRAM bytes from ncu"}
+    for name, prec, model in (("fp64", PREC_FP64, 72.0), ("mixed", PREC_MIXED, 40.0)):
+        s = _c2_solver(prec, stream, h, psi, V)
+        s.block(warmup, STEP_NL)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = s.launches
+        e0.record(stream)
+        s.block(steps, STEP_NL)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        rate = npts * steps / (ms * 1e-3)
+        prof = s.profile_passes(STEP_NL, reps=5)
+        names = ["x pass (FFT_x, kinetic, IFFT_x)", "y pass (IFFT_y, potential, FFT_y)"]
+        out[name] = {
+            "value": rate, "ms_per_step": ms / steps, "gpu_launches": s.launches - l0,
+            "model_bytes_per_pt_step": model,
+            "roofline": {"bound": "hbm", "achieved": model * rate / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": model * rate / 1e9 / peak, "peak_source": peak_kind,
+                         "passes": [{"kernel": names[q] if q < len(names) else f"pass {q}", "ms": p[0],
+                                     "bytes": p[2], "GBps": p[2] / (p[0] * 1e-3) / 1e9} for q, p in enumerate(prof)]},
+        }
+        s.close()
+    out["mixed"]["speedup_vs_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    out["value"] = out["fp64"]["value"]
+    if accuracy:
+        final = {}
+        for name, prec in (("fp64", PREC_FP64), ("mixed", PREC_MIXED)):
+            s = _c2_solver(prec, stream, h, psi, V)
+            n0 = s.particle_number(0)
+            for _ in range(10):
+                s.block(1000, STEP_NL)
+            out[name]["norm_drift_10k"] = (s.particle_number(0) - n0) / n0
+            final[name] = s.psi(0)
+            s.close()
+        out["mixed"]["rel_l2_vs_fp64_10k"] = float(np.linalg.norm(final["mixed"] - final["fp64"]) /
+                                                   np.linalg.norm(final["fp64"]))
+        out["accuracy_steps"] = 10000
+    if with_cpu and _ref_prog("rt_solver"):
+        from atus2_b200 import binfmt
+
+        def inputs(tmp):
+            binfmt.write_bin(os.path.join(tmp, "inp_1.bin"), h, psi)
+
+        def xml(ns):
+            return f"""<SIMULATION>
+  <DIM>2</DIM><FILENAME>inp_1.bin</FILENAME><POTENTIAL_2D>{C2_V_EXPR}</POTENTIAL_2D>
+  <CONSTANTS><unused>0</unused></CONSTANTS>
+  <VCONSTANTS><Alpha_1>0.5,0.5</Alpha_1><GS_1>1</GS_1></VCONSTANTS>
+  <ALGORITHM><DT>0.0005</DT></ALGORITHM>
+  <SEQUENCE><freeprop dt="0.0005" Nk="{ns}" output_freq="none" pn_freq="none">{ns * C2_DT!r}</freeprop></SEQUENCE>
+</SIMULATION>"""
+
+        r = time_ref_program(_ref_prog("rt_solver"), inputs, xml, 2, 8, repeats=3)
+        if r:
+            out["cpu_reference"] = {"value": npts / r["per_step_s"], "unit": UNIT, "cores": r["cores"],
+                                    "kind": "reference", "sample": f"ATUS-2 rt_solver (oracle/_ref, shim FFT), "
+                                    f"{r['runs']} freeprop steps, difference of medians", "wall_s": r["wall_s"]}
+    return out
+
+
+def _ref_prog(name):
+    p = os.path.join(ROOT, "oracle", "_ref", name)
+    return p if os.path.exists(p) else None
+
+
+def time_ref_program(prog, make_inputs, xml_for, n_short, n_long, repeats=3, timeout=900):
+    """Wall time of the reference program ``prog`` (oracle/_ref, built from
+    the ATUS-2 sources with the FFTW-API shim) on all host cores, for runs of
+    n_short and n_long Strang steps, each repeated; the per-step cost is the
+    difference of the medians over (n_long - n_short), so the set-up (file
+    reads, tables, potentials) cancels.  make_inputs(tmp) writes the input
+    files, xml_for(nsteps) returns the run's XML."""
     cores = os.cpu_count() or 1
-    h = header()
-    psi1, psi2 = initial_state(h)
-    times = []
+    env = dict(os.environ, MY_NO_OF_THREADS=str(cores), OMP_NUM_THREADS=str(cores))
+    times = {n_short: [], n_long: []}
     with tempfile.TemporaryDirectory() as tmp:
-        binfmt.write_bin(os.path.join(tmp, "inp_1.bin"), h, psi1)
-        binfmt.write_bin(os.path.join(tmp, "inp_2.bin"), h, psi2)
-        for ns in n_steps_sample:
-            xml = f"""<SIMULATION>
+        make_inputs(tmp)
+        for _ in range(repeats):
+            for ns in (n_short, n_long):
+                open(os.path.join(tmp, "run.xml"), "w").write(xml_for(ns))
+                t0 = time.perf_counter()
+                r = subprocess.run([prog, "run.xml"], cwd=tmp, env=env, capture_output=True, text=True,
+                                   timeout=timeout)
+                times[ns].append(time.perf_counter() - t0)
+                if r.returncode != 0:
+                    return None
+    med_s, med_l = statistics.median(times[n_short]), statistics.median(times[n_long])
+    per_step = max((med_l - med_s) / (n_long - n_short), 1e-12)
+    # spread: the per-step cost from the fastest and slowest pairing of runs
+    lo = max((min(times[n_long]) - max(times[n_short])) / (n_long - n_short), 1e-12)
+    hi = max((max(times[n_long]) - min(times[n_short])) / (n_long - n_short), 1e-12)
+    return {"per_step_s": per_step, "per_step_range_s": [lo, hi], "cores": cores, "seconds": times,
+            "runs": f"{repeats} x ({n_short} and {n_long} steps)", "wall_s": sum(times[n_short]) + sum(times[n_long])}
+
+
+def bragg_xml(ns, pulse_tc=PULSE_TC, pulse_sigma=PULSE_SIGMA):
+    """bragg program input for the 256^3 workload: one bragg_ad block of ns steps."""
+    return f"""<SIMULATION>
   <DIM>3</DIM><FILENAME>inp_1.bin</FILENAME><FILENAME_2>inp_2.bin</FILENAME_2>
-  <AMP_T>exp(-(t-{PULSE_TC!r})*(t-{PULSE_TC!r})/{2 * PULSE_SIGMA * PULSE_SIGMA!r})</AMP_T>
+  <AMP_T>exp(-(t-{pulse_tc!r})*(t-{pulse_tc!r})/{2 * pulse_sigma * pulse_sigma!r})</AMP_T>
   <CONSTANTS><laser_k>8</laser_k><laser_dk>0</laser_dk><laser_domh>16</laser_domh>
     <rabi_threshold>1</rabi_threshold><chirp>0</chirp></CONSTANTS>
   <VCONSTANTS><Amp_1>4,4</Amp_1><Alpha_1>0.5,0.5,0.5</Alpha_1><Delta_L>0,0</Delta_L>
@@ -288,29 +569,44 @@ def run_cpu_baseline(n_steps_sample=(1, 3)):
   <ALGORITHM><DT>1</DT></ALGORITHM>
   <SEQUENCE><bragg_ad dt="0.001" Nk="{ns}" output_freq="none" pn_freq="none">{ns * DT!r}</bragg_ad></SEQUENCE>
 </SIMULATION>"""
-            open(os.path.join(tmp, "run.xml"), "w").write(xml)
-            env = dict(os.environ, MY_NO_OF_THREADS=str(cores), OMP_NUM_THREADS=str(cores))
-            t0 = time.perf_counter()
-            r = subprocess.run([prog, "run.xml"], cwd=tmp, env=env, capture_output=True, text=True, timeout=900)
-            times.append(time.perf_counter() - t0)
-            if r.returncode != 0:
-                return None
-    n1, n2 = n_steps_sample
-    per_step = max((times[1] - times[0]) / (n2 - n1), 1e-9)
+
+
+def run_cpu_baseline(n_short=1, n_long=5, repeats=3):
+    """The reference bragg program on this host's cores on the 256^3 Bragg
+    workload (the same state and pulse as the GPU runs)."""
+    prog = _ref_prog("bragg")
+    if prog is None:
+        return None
+    from atus2_b200 import binfmt
+
+    def inputs(tmp):
+        h = header()
+        psi1, psi2 = initial_state(h)
+        binfmt.write_bin(os.path.join(tmp, "inp_1.bin"), h, psi1)
+        binfmt.write_bin(os.path.join(tmp, "inp_2.bin"), h, psi2)
+
+    r = time_ref_program(prog, inputs, bragg_xml, n_short, n_long, repeats)
+    if r is None:
+        return None
     return {
-        "value": N ** 3 / per_step,
+        "value": N ** 3 / r["per_step_s"],
+        "value_range": [N ** 3 / r["per_step_range_s"][1], N ** 3 / r["per_step_range_s"][0]],
         "unit": UNIT,
-        "cores": cores,
+        "cores": r["cores"],
         "kind": "reference",
-        "sample": f"ATUS-2 bragg (oracle/_ref, shim FFT) at 256^3 x 2 components, runs of {n1} and {n2} "
-                  f"Strang steps (Nk = steps), per-step = difference / {n2 - n1}; MY_NO_OF_THREADS={cores}",
-        "seconds": times,
+        "fft": "FFTW-API shim (oracle/fft_cpu.c, FP64 mixed-radix, OpenMP over pencils); FFTW 3.3.8 is not installed",
+        "sample": f"ATUS-2 bragg program (oracle/_ref) at 256^3 x 2 components, {r['runs']} bragg_ad steps "
+                  f"(Nk = steps), per-step cost = difference of the medians / {n_long - n_short}; "
+                  f"MY_NO_OF_THREADS={r['cores']}",
+        "seconds": r["seconds"],
+        "wall_s": r["wall_s"],
     }
 
 
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
-# FP64 kernels, from one ncu capture each (profiles/pass2_potential_fp64_bragg256.md,
-# profiles/pipe_kernel_fp64_bragg256.md, profiles/pass2_kinetic_fp64_bragg256.md).
+# FP64 256^3 x 2 kernels, each from one ncu capture of that kernel on this
+# workload on a B200 (a profiler cannot run inside the timed bench, so the
+# capture's figure is carried here).
 NCU_TRAFFIC_FP64 = {"pass2_kernel M2_NL (z)": 1.0769e9, "pipe_kernel": 1.0204e9, "pass2_kernel M2_KIN": 1.0433e9}
 
 
@@ -334,6 +630,8 @@ def roofline(s, kind, peak, peak_kind, fp64=True):
         "frac": achieved / peak,
         "peak_source": peak_kind,
         "traffic": traffic,
+        "traffic_source": "ncu capture of this kernel at this size (dram__bytes_read.sum + dram__bytes_write.sum)"
+                          if traffic else None,
         "kernel": name,
         "algorithmic_bytes_per_launch": by,
         "passes": [{"kernel": names[q] if q < len(names) else f"pass {q}", "ms": p[0], "launches_per_step": p[1],
@@ -395,12 +693,22 @@ def atus_arm(args, rank, ws, local, dist):
     sm.close()
     # end-to-end through the C ABI with host buffers
     barrier(dist)
-    e2e_steps = max(1, min(args.steps // 20, 5))
+    e2e_steps = max(3, min(args.steps // 20, 5))
     ms_e, bi, bo = run_e2e(e2e_steps, stream)
     ms_e = max_over_ranks(dist, ms_e)
     out["e2e"] = {"value": whole_job_rate(ws, npts * E2E_NK * e2e_steps, ms_e), "unit": UNIT,
                   "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo,
                   "step": f"upload 2 components, {E2E_NK} Strang steps, download 2 components", "steps": e2e_steps}
+    if not args.no_accuracy:
+        barrier(dist)
+        out["variants"]["mixed"]["accuracy_10k"] = run_accuracy3(stream)
+    if not args.no_configs:
+        barrier(dist)
+        cpu = rank == 0 and ws == 1 and not args.no_cpu_baseline
+        out["variants"]["config1_1d"] = run_config1(stream, cpu)
+        barrier(dist)
+        out["variants"]["config2_2d"] = run_config2(stream, args.steps, args.warmup, peak, peak_kind, cpu,
+                                                    accuracy=not args.no_accuracy)
     if not args.no_batch:
         barrier(dist)
         out["variants"]["batch"] = run_batch()
@@ -587,39 +895,85 @@ def run_sobmin(no_cpu=False):
         "step": guess.STEP,
     }
     if not no_cpu:
-        # the oracle port's iteration at 128^3 on all host cores, times the GPU's iteration count
-        from oracle.oracle import Oracle
-
         wy, wz, g = H[0]
-        h = guess.header(SOB_N)
-        V = guess.potential(h, wy, wz)
-        cores = os.cpu_count() or 1
-        o = Oracle(h, 1, threads=cores)
-        o.set_psi(0, guess.tf_guess(h, V, g))
-        o.set_potential(0, V)
-        o.set_gs([g])
-        o.sob_init([guess.ALPHA], guess.STEP)
-        o.sob_renormalize()
-        o.sob_iterate()
-        t0 = time.perf_counter()
-        for _ in range(5):
-            o.sob_iterate()
-        per_it = (time.perf_counter() - t0) / 5
-        out["cpu_baseline"] = {"value": per_it * out["iterations_mean"], "unit": "s", "cores": cores, "kind": "port",
-                               "sample": f"5 Sobolev iterations of the oracle restatement at 128^3 on {cores} threads, "
-                                         "times the mean plain iteration count"}
+        r = time_ref_sobmin(wy, wz, g)
+        if r is not None:
+            out["cpu_baseline"] = {"value": r["per_iter_s"] * out["iterations_mean"], "unit": "s",
+                                   "cores": r["cores"], "kind": "reference",
+                                   "per_iteration_s": r["per_iter_s"],
+                                   "sample": f"ATUS-2 sobmin (oracle/_ref, shim FFT) at 128^3 on {r['cores']} threads, "
+                                             f"held-out draw 0, {r['iters']} iterations timed from the program's own "
+                                             "per-iteration output lines (set-up excluded), per-iteration time x the "
+                                             "mean plain iteration count of the GPU runs"}
     return out
+
+
+def time_ref_sobmin(wy, wz, g, seconds=15.0):
+    """Per-iteration wall time of the reference sobmin program at 128^3 on all
+    host cores: the program prints one line per iteration ("--- k"); the
+    time between the first and the last line read within `seconds` (after
+    the first iteration) over the iterations between them.  The run is then
+    stopped (the residual target 1e-10 would take hours)."""
+    prog = _ref_prog("sobmin")
+    if prog is None:
+        return None
+    from atus2_b200 import guess
+
+    cores = os.cpu_count() or 1
+    h = guess.header(SOB_N)
+    V = guess.potential(h, wy, wz)
+    tf = np.abs(guess.tf_guess(h, V, g))
+    i = np.unravel_index(int(np.argmax(tf)), tf.shape)
+    mu_tf = float(g * tf[i] ** 2 + V[i])  # the Thomas-Fermi mu: mu - V = g |psi|^2 inside the cloud
+    vexpr = f"0.5*(x^2+{wy * wy!r}*y^2+{wz * wz!r}*z^2)"
+    m = f"({mu_tf!r}-{vexpr})"
+    half = guess.L_BOX / 2
+    axes = "".join(f"<N{a}>{SOB_N}</N{a}><{a}MIN>{-half!r}</{a}MIN><{a}MAX>{half!r}</{a}MAX>" for a in "XYZ")
+    xml = f"""<SIMULATION>
+  <DIM>3</DIM><FILENAME>final.bin</FILENAME>
+  <GUESS_3D>sqrt((abs{m}+{m})/{2 * g!r})</GUESS_3D>
+  <POTENTIAL_3D>{vexpr}</POTENTIAL_3D>
+  <CONSTANTS><epsilon>{guess.EPS!r}</epsilon><stepsize>{guess.STEP!r}</stepsize></CONSTANTS>
+  <VCONSTANTS><Alpha_1>{guess.ALPHA!r}</Alpha_1><GS_1>{g!r}</GS_1><N>1</N></VCONSTANTS>
+  <ALGORITHM>{axes}</ALGORITHM>
+</SIMULATION>"""
+    env = dict(os.environ, MY_NO_OF_THREADS=str(cores), OMP_NUM_THREADS=str(cores))
+    stamps = []
+    with tempfile.TemporaryDirectory() as tmp:
+        open(os.path.join(tmp, "run.xml"), "w").write(xml)
+        proc = subprocess.Popen([prog, "run.xml"], cwd=tmp, env=env, stdout=subprocess.PIPE,
+                                stderr=subprocess.DEVNULL, text=True, bufsize=1)
+        try:
+            t_end = None
+            for line in proc.stdout:
+                if line.startswith("--- "):
+                    now = time.perf_counter()
+                    stamps.append(now)
+                    if t_end is None:
+                        t_end = now + seconds
+                    elif now >= t_end:
+                        break
+        finally:
+            proc.kill()
+            proc.wait()
+    if len(stamps) < 3:
+        return None
+    return {"per_iter_s": (stamps[-1] - stamps[0]) / (len(stamps) - 1), "iters": len(stamps) - 1, "cores": cores}
 
 
 # ------------------------------------------------------------------ reference arm
 def reference_arm(args, rank, ws, dist):
+    """The reference bragg program on this host's cores: runs of W and W + K
+    Strang steps (W = --warmup, K = --steps), three repeats each; the K-step
+    cost is the difference of the medians, so the `steps` printed are the
+    steps timed."""
     if rank != 0:
         return
-    cb = run_cpu_baseline()
+    w, k = args.warmup, args.steps
+    cb = run_cpu_baseline(n_short=w, n_long=w + k, repeats=3)
     if cb is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/bragg is not built (needs the ATUS-2 sources)"}))
         return
-    # steps of the reference arm: each step one Strang step, timed from the difference runs
     per_step_s = N ** 3 / cb["value"]
     out = {
         "impl": "reference",
@@ -627,17 +981,23 @@ def reference_arm(args, rank, ws, dist):
         "value": cb["value"],
         "unit": UNIT,
         "n_gpus": ws,
-        "steps": args.steps,
-        "warmup": args.warmup,
+        "steps": k,
+        "warmup": w,
         "ms_per_step": per_step_s * 1e3,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded Thomas-Fermi state)",
-        "config": {"workload": "3D two-component Bragg pulse (bragg_ad), 256^3, reference CPU program",
-                   "grid": [N, N, N], "components": 2},
-        "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "config": {"workload": "3D two-component Bragg pulse (bragg_ad), 256^3 on [-32,32)^3, g=100, k_L=4, delta=16, "
+                               "Omega peak 8, sigma_t 0.5, dt=1e-3; reference CPU program",
+                   "grid": [N, N, N], "components": 2,
+                   "fft": cb["fft"],
+                   "timing": f"runs of {w} and {w + k} bragg_ad steps, 3 repeats each; "
+                             f"{k}-step time = difference of the medians"},
+        "value_range": cb["value_range"],
+        "seconds": cb["seconds"],
+        "cpu_baseline": {kk: cb[kk] for kk in ("value", "unit", "cores", "kind", "sample")},
         "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out))
@@ -652,6 +1012,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-sweep variant")
     ap.add_argument("--no-sobmin", action="store_true", help="skip the ground-state variant")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the 10^4-step accuracy runs")
+    ap.add_argument("--no-configs", action="store_true", help="skip the 1D and 2D workloads")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, ws, local, dist = dist_init()

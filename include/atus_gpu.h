@@ -212,7 +212,10 @@ ATUS_API int atus_particle_number(atus_ctx *ctx, int comp, double *out);
  * per 32768 points in a 32 KB array); larger fields return ATUS_E_LIMIT and
  * launch nothing.  The first call on a device looks up the array's device
  * address (cudaGetSymbolAddress) with that device current; make that first
- * call before any stream capture.  All calls on a device share the array, so
+ * call before any stream capture.  The address is kept per device together
+ * with the id of the CUDA context it belongs to: after cudaDeviceReset, or
+ * under another context, the next call looks it up again (so make that call,
+ * too, outside a capture).  All calls on a device share the array, so
  * calls whose kernels overlap on the GPU (other streams, other host threads)
  * race and may return wrong sums: order them on one stream.  The result
  * equals atus_particle_number's to rounding (another summation order). */

@@ -2,12 +2,13 @@
 
 Runs ATUS-2's own ``rt_solver``, ``bragg``, ``double_bragg``, ``bragg_ds``,
 ``raman`` and ``sobmin`` (built unmodified
-from the ATUS-2 sources by ``make -C oracle ref``) single-threaded on small
+from the ATUS-2 sources by ``make -C oracle ref REF=<tree>``) single-threaded on small
 seeded inputs, and stores inputs and outputs as ``<case>.npz``.  The CPU tests
 replay every case on the oracle restatement and require bit-identical results;
 the GPU tests use the same inputs.
 
-Usage (needs the reference sources, i.e. only where oracle/_ref can be built):
+Usage (needs the reference programs in oracle/_ref, or the ATUS-2 source
+tree named by ATUS2_REFERENCE_TREE to build them):
 
     python tests/golden/make_golden.py            # all cases
 """
@@ -506,7 +507,10 @@ def make_sob(case, tmp):
 
 def main():
     if not os.path.exists(os.path.join(REF, "raman")):
-        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+        tree = os.environ.get("ATUS2_REFERENCE_TREE")
+        if not tree:
+            sys.exit("oracle/_ref is not built: set ATUS2_REFERENCE_TREE to the ATUS-2 source tree")
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={tree}"], check=True)
     only = set(sys.argv[1:])
     keep = (lambda c: not only or c["name"] in only)
     global CASES, BRAGG_CASES, DBRAGG_CASES, BRAGGDS_CASES, SOB_CASES
