@@ -73,38 +73,64 @@ def build(jobs: int | None = None, force: bool = False, verbose: bool = False) -
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
         os.replace(tmp, LIB)
-    build_programs(verbose=verbose)
     return LIB
 
 
 HOST = os.path.join(HERE, "host")
-PROGRAMS = ("rt_solver", "bragg", "double_bragg", "bragg_ds", "raman", "sobmin", "gen_psi_0")
+DROPIN = os.path.join(HERE, "dropin")
+# The ATUS-2 programs, by their source path in the ATUS-2 tree, and the
+# headers each one uses without including them (the real FFTW / muParser /
+# GSL headers pulled them in): the same force-includes as the oracle recipe.
+PROGRAMS = {
+    "rt_solver": ("source/SOLVER/src/rt_solver.cpp", []),
+    "bragg": ("source/interferometry/src/bragg.cpp", []),
+    "double_bragg": ("source/interferometry/src/double_bragg.cpp", []),
+    "bragg_ds": ("source/interferometry/src/bragg_ds.cpp", ["complex"]),
+    "raman": ("source/interferometry/src/raman.cpp", []),
+    "sobmin": ("source/SOLVER/src/sob_solver.cpp", []),
+    "gen_psi_0": ("source/utils/src/gen_psi_0.cpp", []),
+}
 
 
-def build_programs(verbose: bool = False) -> None:
-    """The XML programs (host/programs/*.cpp) linked against libatus_gpu.so,
-    found at run time next to the package (rpath $ORIGIN/../..)."""
+def build_programs(tree: str | None = None, verbose: bool = False) -> list[str]:
+    """Compiles ATUS-2's own program sources, unmodified, from the source tree
+    `tree` (default: $ATUS2_REFERENCE_TREE) against the drop-in headers
+    (atus2_b200/dropin: CRT_Base, CRT_Base_IF, CRT_Base_IF_2, CSOB_Base,
+    cft_*d, ParameterHandler, muParser, fftw3) and libatus_gpu.so, into
+    host/bin (found at run time next to the package, rpath $ORIGIN/../..).
+    Without a tree nothing is built and the list is empty."""
+    tree = tree or os.environ.get("ATUS2_REFERENCE_TREE")
+    if not tree or not os.path.isdir(os.path.join(tree, "source")):
+        return []
     out = os.path.join(HOST, "bin")
     os.makedirs(out, exist_ok=True)
-    deps = [LIB] + glob.glob(os.path.join(HOST, "*.h")) + [os.path.join(INCLUDE, "atus_gpu.h")]
+    deps = [LIB] + glob.glob(os.path.join(HOST, "*.h")) + glob.glob(os.path.join(DROPIN, "*.h"))
+    deps.append(os.path.join(INCLUDE, "atus_gpu.h"))
     newest = max(os.path.getmtime(d) for d in deps)
-    for p in PROGRAMS:
-        src = os.path.join(HOST, "programs", p + ".cpp")
+    built = []
+    for p, (rel, force) in PROGRAMS.items():
+        src = os.path.join(tree, rel)
         exe = os.path.join(out, p)
+        built.append(exe)
         if os.path.exists(exe) and os.path.getmtime(exe) >= max(newest, os.path.getmtime(src)):
             continue
-        cmd = ["g++", "-O2", "-std=c++17", "-fopenmp", "-I", INCLUDE, "-o", exe, src, "-L", HERE,
+        inc = [a for f in force for a in ("-include", f)]
+        cmd = ["g++", "-O2", "-std=c++17", "-fopenmp", *inc, "-I", DROPIN, "-I", INCLUDE, "-o", exe, src, "-L", HERE,
                "-l:libatus_gpu.so", "-Wl,-rpath,$ORIGIN/../.."]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
-            raise RuntimeError(f"g++ failed on {p}:\n{r.stdout}\n{r.stderr}")
+            raise RuntimeError(f"g++ failed on {p} ({rel}):\n{r.stdout}\n{r.stderr}")
         if verbose:
             print("built", exe)
+    return built
 
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--jobs", type=int, default=None)
     ap.add_argument("--force", action="store_true")
+    ap.add_argument("--programs", metavar="TREE", help="also build ATUS-2's programs from this source tree")
     args = ap.parse_args()
     print(build(args.jobs, args.force, verbose=True))
+    if args.programs:
+        build_programs(args.programs, verbose=True)

@@ -426,6 +426,16 @@ static int scratch_forward(atus_ctx *ctx) {
   return r;
 }
 
+// psi *= fak in FP64 (the scale pass of cft_Nd::ft)
+template <typename R>
+__global__ void ft_scale_kernel(void *psi, double fak, int64_t n) {
+  cplx<R> *p = static_cast<cplx<R> *>(psi);
+  for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < n; l += (int64_t)gridDim.x * blockDim.x) {
+    const cplx<R> v = p[l];
+    p[l] = mk<R>((R)((double)v.x * fak), (R)((double)v.y * fak));
+  }
+}
+
 // ------------------------------------------------------------------ API
 extern "C" {
 
@@ -682,6 +692,24 @@ int atus_download_psi(atus_ctx *ctx, int comp, double *psi) {
 int atus_device_psi(atus_ctx *ctx, int comp, void **dptr) {
   if (!ctx || !dptr || comp < 0 || comp >= ctx->ncomp) return ATUS_E_ARG;
   *dptr = ctx->psi[comp];
+  return ATUS_OK;
+}
+
+// cft_Nd::ft (cft_1d.cpp:61-77, cft_2d.cpp:58-74, cft_3d.cpp:58-74) on one
+// component: the unnormalised transform over every axis (isign -1: FFTW's
+// forward sign, +1: backward), then the scale pass with (dx/sqrt(2 pi))^dim
+// after a forward and (dk/sqrt(2 pi))^dim after a backward transform.
+int atus_ft(atus_ctx *ctx, int comp, int isign) {
+  if (!ctx || comp < 0 || comp >= ctx->ncomp || (isign != -1 && isign != 1)) return ATUS_E_ARG;
+  void *f[1] = {ctx->psi[comp]};
+  const int dir = (isign < 0) ? T_FWD : T_INV;
+  for (int ax = ctx->dim - 1; ax >= 0; ax--) RUN(run_pass(ctx, ax, dir, OP_NONE, T_NONE, nullptr, 0, f, 1));
+  const double fak = scale_fak(ctx->dim, isign < 0 ? ctx->d : ctx->dk);
+  if (ctx->prec == ATUS_PREC_FP64)
+    ft_scale_kernel<double><<<grid_blocks(ctx->npts, 256), 256, 0, ctx->stream>>>(ctx->psi[comp], fak, ctx->npts);
+  else
+    ft_scale_kernel<float><<<grid_blocks(ctx->npts, 256), 256, 0, ctx->stream>>>(ctx->psi[comp], fak, ctx->npts);
+  LAUNCHED(ctx);
   return ATUS_OK;
 }
 

@@ -106,6 +106,7 @@ SIGNATURES = {
     "atus_upload_psi": (_i, [_vp, _i, _dp]),
     "atus_download_psi": (_i, [_vp, _i, _dp]),
     "atus_device_psi": (_i, [_vp, _i, C.POINTER(C.c_void_p)]),
+    "atus_ft": (_i, [_vp, _i, _i]),
     "atus_ft_step": (_i, [_vp, _i]),
     "atus_nl_step": (_i, [_vp, _i, _d]),
     "atus_strang_block": (_i, [_vp, _i, _i, _dp]),
@@ -301,6 +302,11 @@ class Solver:
         return v.value
 
     # ------------------------------------------------------------ steps
+    def ft(self, comp: int, isign: int) -> None:
+        """cft_Nd::ft on component comp: transform over all axes (isign -1
+        forward, +1 backward) with the reference's scale."""
+        self._ok(self._L.atus_ft(self._c, int(comp), int(isign)), "ft")
+
     def ft_step(self, half: bool) -> None:
         self._ok(self._L.atus_ft_step(self._c, 1 if half else 0), "ft_step")
 

@@ -194,6 +194,7 @@ class ParameterHandler {
     return it->second;
   }
   bool Has_simulation(const std::string &k) const { return m_simulation.count(k) != 0; }
+  const std::map<std::string, double> &constants() const { return m_constants; }
   double Get_Constant(const std::string &k) const {
     auto it = m_constants.find(k);
     if (it == m_constants.end()) throw std::string("Error: Could not find the key: " + k + " in section CONSTANT.");

@@ -24,6 +24,7 @@
  *                                   (include/CRT_Base_IF.h:65-77, 144-168)
  *   atus_upload_psi/atus_download_psi  m_fields[c]->Getp2In() contents
  *                                   (source/libs/lib_myutils/cft_base.h:175)
+ *   atus_ft                         cft_Nd::ft (source/libs/lib_myutils/cft_3d.cpp:58-74)
  *   atus_ft_step                    Do_FT_Step_full / Do_FT_Step_half
  *                                   (include/CRT_Base.h:336-392)
  *   atus_nl_step                    Do_NL_Step (include/CRT_Base.h:396-441),
@@ -172,6 +173,12 @@ ATUS_API int atus_upload_psi(atus_ctx *ctx, int comp, const double *psi);
 ATUS_API int atus_download_psi(atus_ctx *ctx, int comp, double *psi);
 /* Device pointer of component comp (complex128 or complex64 per precision). */
 ATUS_API int atus_device_psi(atus_ctx *ctx, int comp, void **dptr);
+/* cft_Nd::ft(isign) on component comp, in place (source/libs/lib_myutils/
+ * cft_1d.cpp:61-77, cft_2d.cpp:58-74, cft_3d.cpp:58-74): the transform over
+ * every axis with FFTW's sign convention (isign -1 forward, +1 backward),
+ * natural (unshifted) order, then the scale (dx/sqrt(2 pi))^dim after a
+ * forward and (dk/sqrt(2 pi))^dim after a backward transform. */
+ATUS_API int atus_ft(atus_ctx *ctx, int comp, int isign);
 
 /* ------------------------------------------------------------ steps */
 ATUS_API int atus_ft_step(atus_ctx *ctx, int half);

@@ -212,6 +212,24 @@ def test_primitives_match_oracle():
     np.testing.assert_allclose(s.rabi_integrals(k0, 1.0), o.rabi_integrals(k0, 1.0), rtol=1e-12, atol=1e-14)
 
 
+@pytest.mark.parametrize("dim,n", [(1, [4096]), (2, [64, 256]), (3, [16, 32, 256])])
+def test_field_transform_matches_oracle(dim, n):
+    """atus_ft (cft_Nd::ft: transform over all axes, then the reference's
+    scale) forward and back against the oracle's cft restatement, FP64."""
+    h = _grid(dim, n, 10.0)
+    rng = np.random.default_rng(3)
+    a = (rng.standard_normal(n) + 1j * rng.standard_normal(n)).astype(np.complex128)
+    o = Oracle(h, 1)
+    s = Solver(h, 1, PREC_FP64)
+    s.set_psi(0, a)
+    ref = np.ascontiguousarray(a.copy())
+    for isign in (-1, +1):
+        s.ft(0, isign)
+        o.ft(ref, isign)
+        assert rel_l2(s.psi(0), ref) < 1e-13, isign
+    assert rel_l2(s.psi(0), a) < 1e-13  # a round trip is the identity (dk = 2 pi / L)
+
+
 def test_sobmin_mu_matches_oracle():
     h = _grid(3, [32, 32, 16], 12.0)
     x, y, z = _coords(h)
