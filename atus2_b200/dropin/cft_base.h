@@ -13,6 +13,10 @@
 //     (device_changed());
 //   * host_view() reads the mirror without making the device copy stale (file
 //     output).
+// Step functions call Getp2In() from every thread of an OpenMP parallel
+// region (bragg.cpp:196-197 does), so bringing the mirror up to date is done
+// once, under a lock: a second thread must not download over the first
+// thread's updates.
 // ft(isign) is cft_Nd::ft on the GPU: the unnormalised transform over all
 // axes with FFTW's sign convention, then the reference's scale, in place.  A
 // field constructed by a program (not by a solver) gets a one-component GPU
@@ -27,6 +31,7 @@
 #include <cstring>
 #include <fstream>
 #include <iostream>
+#include <mutex>
 #include <string>
 
 #include "CPoint.h"
@@ -92,7 +97,11 @@ class cft_base {
 
   double *Getp2InReal() { return m_in_real; }
   fftw_complex *Getp2In() {
-    pull();
+    std::lock_guard<std::mutex> lock(m_sync);
+    if (m_host_stale && m_ctx) {
+      check(atus_download_psi(m_ctx, m_comp, &m_in[0][0]), "download");
+      m_host_stale = false;
+    }
     m_dev_stale = true;
     return m_in;
   }
@@ -129,6 +138,7 @@ class cft_base {
   atus_ctx *atus_context() const { return m_ctx; }
   // upload the mirror if the program may have changed it
   void push() {
+    std::lock_guard<std::mutex> lock(m_sync);
     if (m_dev_stale && m_ctx) {
       check(atus_upload_psi(m_ctx, m_comp, &m_in[0][0]), "upload");
       m_dev_stale = false;
@@ -149,6 +159,7 @@ class cft_base {
 
  protected:
   void pull() {
+    std::lock_guard<std::mutex> lock(m_sync);
     if (m_host_stale && m_ctx) {
       check(atus_download_psi(m_ctx, m_comp, &m_in[0][0]), "download");
       m_host_stale = false;
@@ -195,6 +206,7 @@ class cft_base {
   atus_ctx *m_ctx = nullptr;
   atus_ctx *m_own_ctx = nullptr;
   int m_comp = 0;
+  std::mutex m_sync;
   bool m_dev_stale = true, m_host_stale = false;
 };
 
