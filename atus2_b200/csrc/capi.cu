@@ -258,6 +258,57 @@ static int kinetic_pass(atus_ctx *ctx, int half) {
   return run_pass(ctx, 0, T_FWD, OP_KIN, T_INV, nullptr, half);
 }
 
+// Rabi balls requested with a block: per component comps[c] (c < ncomp) the
+// centres k0[(c * n + m) * dim ..] (m < n), radius thr.
+struct RabiReq {
+  int ncomp, n;
+  int comps[2];
+  const double *k0;
+  double thr;
+};
+
+// The kinetic pass with the Rabi sums of the requested components folded in:
+// after FFT_x every axis is in k-space and |psi^|^2 does not see the kinetic
+// phase, so the sums of the state after the pass are taken there.  Unscaled
+// sums go to ctx->red_partial (one row per CTA), the totals to sums[c*n+m].
+// ATUS_E_UNSUPPORTED (fields untouched) where the register-staged x pass does
+// not apply.
+static int kinetic_pass_rabi(atus_ctx *ctx, int half, const RabiReq &rr, double *sums) {
+  if (!ctx->use_pass2 || ctx->dim < 2 || ctx->n[0] < 32 || ctx->n[0] > 256) return ATUS_E_UNSUPPORTED;
+  PassArgs a;
+  memset(&a, 0, sizeof(a));
+  for (int c = 0; c < MAXC; c++) a.psi[c] = (c < ctx->ncomp) ? ctx->psi[c] : nullptr;
+  a.t1 = T_FWD;
+  a.op = OP_KIN;
+  a.t2 = T_INV;
+  a.per_comp = 1;
+  a.nc = 1;
+  for (int c = 0; c < MAXC; c++)
+    for (int ax = 0; ax < 3; ax++) a.kt[c][ax] = (c < ctx->ncomp) ? ctx->kt[half ? 0 : 1][c][ax] : nullptr;
+  a.s_f = scale_fak(ctx->dim, ctx->d);
+  a.s_b = scale_fak(ctx->dim, ctx->dk);
+  a.rabi_ncomp = rr.ncomp;
+  a.rabi_n = rr.n;
+  for (int c = 0; c < rr.ncomp; c++) {
+    a.rabi_comp[c] = rr.comps[c];
+    for (int m = 0; m < rr.n; m++)
+      for (int ax = 0; ax < 3; ax++)
+        a.rabi_k0[c * rr.n + m][ax] = (ax < ctx->dim) ? rr.k0[(c * rr.n + m) * ctx->dim + ax] : 0.0;
+  }
+  a.rabi_thr = rr.thr;
+  a.rabi_partial = ctx->red_partial;
+  CK(cudaMemsetAsync(ctx->red_partial, 0, sizeof(double) * RED_BLOCKS * RED_MAXQ, ctx->stream));
+  const int r = (ctx->prec == ATUS_PREC_FP64) ? launch_pass2_d_kr(ctx, a, 0) : launch_pass2_f_kr(ctx, a, 0);
+  if (r != ATUS_OK) return r;
+  const int nq = rr.ncomp * rr.n;
+  reduce_final<<<1, 32, 0, ctx->stream>>>(ctx->red_partial, RED_BLOCKS, nq, ctx->red_out);
+  LAUNCHED(ctx);
+  CK(cudaMemcpyAsync(ctx->h_red, ctx->red_out, sizeof(double) * nq, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (int q = 0; q < nq; q++) sums[q] = ctx->h_red[q];
+  return ATUS_OK;
+}
+
 // Arguments of one pass over the context's fields, with the geometry the
 // launchers fill in (the plane pipeline takes three of them as they are).
 static PassArgs pass_args(const atus_ctx *ctx, int axis, int t1, int op, int t2, const NLArgs *nl) {
@@ -751,7 +802,41 @@ int atus_nl_step(atus_ctx *ctx, int kind, double F) {
   return ATUS_OK;
 }
 
+static int strang_block(atus_ctx *ctx, int nk, int kind, const double *F, const RabiReq *rr, double *sums,
+                        bool *fused);
+
 int atus_strang_block(atus_ctx *ctx, int nk, int kind, const double *F) {
+  return strang_block(ctx, nk, kind, F, nullptr, nullptr, nullptr);
+}
+
+int atus_strang_block_rabi(atus_ctx *ctx, int nk, int kind, const double *F, int ncomp_r, const int *comps,
+                           const double *k0, int n, double thr, double *out) {
+  if (!ctx || !out || !comps || !k0 || ncomp_r < 1 || ncomp_r > 2 || n < 1 || ncomp_r * n > RED_MAXQ)
+    return ATUS_E_ARG;
+  for (int c = 0; c < ncomp_r; c++)
+    if (comps[c] < 0 || comps[c] >= ctx->ncomp) return ATUS_E_ARG;
+  RabiReq rr;
+  rr.ncomp = ncomp_r;
+  rr.n = n;
+  rr.comps[0] = comps[0];
+  rr.comps[1] = ncomp_r > 1 ? comps[1] : -1;
+  rr.k0 = k0;
+  rr.thr = thr;
+  double sums[RED_MAXQ];
+  bool fused = false;
+  RUN(strang_block(ctx, nk, kind, F, &rr, sums, &fused));
+  if (!fused) {  // the separate transform and reduction of compute_rabi_integrals
+    for (int c = 0; c < ncomp_r; c++)
+      RUN(atus_rabi_integrals_comp(ctx, comps[c], k0 + (size_t)c * n * ctx->dim, n, thr, out + c * n));
+    return ATUS_OK;
+  }
+  const double f = scale_fak(ctx->dim, ctx->d);
+  for (int q = 0; q < ncomp_r * n; q++) out[q] = ctx->ar_k * (f * f * sums[q]);
+  return ATUS_OK;
+}
+
+static int strang_block(atus_ctx *ctx, int nk, int kind, const double *F, const RabiReq *rr, double *sums,
+                        bool *fused) {
   if (!ctx || nk < 1) return ATUS_E_ARG;
   RUN(check_kind(ctx, kind));
   const double dt = ctx->dt;
@@ -824,7 +909,13 @@ int atus_strang_block(atus_ctx *ctx, int nk, int kind, const double *F) {
     const NLArgs nl = nl_args(ctx, kind, ctx->t + 0.5 * dt, F ? F[j] : 1.0);
     RUN(potential_pass(ctx, nl));
     const bool last = (j == nk - 1);
-    RUN(kinetic_pass(ctx, last ? 1 : 0));
+    int r = ATUS_E_UNSUPPORTED;
+    if (last && rr) {
+      r = kinetic_pass_rabi(ctx, 1, *rr, sums);
+      if (r == ATUS_OK && fused) *fused = true;
+    }
+    if (r == ATUS_E_UNSUPPORTED) r = kinetic_pass(ctx, last ? 1 : 0);
+    RUN(r);
     ctx->t += last ? 0.5 * dt : dt;
   }
   RUN(transform_inner(ctx, T_INV));

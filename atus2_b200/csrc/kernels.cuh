@@ -42,7 +42,10 @@ enum { FILT_SOBOLEV = 0, FILT_LAPLACE = 1 };
 // three-state "raman" steps of CRT_Base_IF
 enum { K_NL = 0, K_NL_IF = 1, K_BRAGG = 2, K_DBRAGG = 3, K_NL_IF2 = 4, K_BRAGG_DS = 5, K_NUM_BRAGG = 6, K_RAMAN = 7 };
 // modes of the register-staged pass kernel (pass2.cuh)
-enum { M2_FWD = 0, M2_INV = 1, M2_KIN = 2, M2_NL = 3 };
+// M2_KIN_RABI: M2_KIN that also sums |psi^(k)|^2 over the Rabi balls of the
+// requested components while every axis is in k-space (the last kinetic pass
+// of a block); a separate instantiation, so M2_KIN keeps its registers.
+enum { M2_FWD = 0, M2_INV = 1, M2_KIN = 2, M2_NL = 3, M2_KIN_RABI = 4 };
 
 struct LaserD {
   double beta0, DeltaL[MAXC], Amp0, laser_k0, laser_dk0, laser_domh0, phase0, chirp_rate0, chirp;
@@ -102,6 +105,14 @@ struct PassArgs {
   double filt_alpha, filt_scale;
   double dk[3];
   int n[3];
+  // M2_KIN_RABI: balls k0[c * rabi_n + m] (m < rabi_n) of component
+  // rabi_comp[c] (c < rabi_ncomp), radius rabi_thr; per-CTA sums of the
+  // unscaled |psi^|^2 to rabi_partial[blockIdx.x * 8 + q]
+  int rabi_ncomp, rabi_n;
+  int rabi_comp[2];
+  double rabi_thr;
+  double rabi_k0[8][3];
+  double *rabi_partial;
 };
 
 __device__ __forceinline__ void idx3(const Geo &g, int64_t l, int &ix, int &iy, int &iz) {

@@ -117,7 +117,7 @@ static inline int launch_block1d_n(atus_ctx *ctx, Block1DArgs &a) {
 template <typename R, int N, int TC, int MODE, bool STRIDED>
 static inline int launch_pass2_t(atus_ctx *ctx, PassArgs &a, int axis) {
   using Cfg = P2Cfg<R, N, TC>;
-  constexpr size_t smem = (MODE == M2_KIN && Cfg::kin_smem) ? Cfg::smem_kin : Cfg::smem;
+  constexpr size_t smem = ((MODE == M2_KIN || MODE == M2_KIN_RABI) && Cfg::kin_smem) ? Cfg::smem_kin : Cfg::smem;
   static int resident = 0;
   static int nsm = 0;
   if (!resident) {
@@ -157,7 +157,8 @@ static inline int launch_pass2_t(atus_ctx *ctx, PassArgs &a, int axis) {
   a.ncomp_grid = ctx->ncomp;
   const int64_t work = a.per_comp ? ntiles * ctx->ncomp : ntiles;
   const int64_t slots = (int64_t)nsm * resident;
-  const unsigned grid = (unsigned)(work < slots ? work : slots);
+  unsigned grid = (unsigned)(work < slots ? work : slots);
+  if (MODE == M2_KIN_RABI && grid > RED_BLOCKS) grid = RED_BLOCKS;  // one partial row per CTA
   pass2_kernel<R, N, TC, MODE, STRIDED><<<grid, Cfg::NT, smem, ctx->stream>>>(a);
   LAUNCHED(ctx);
   return ATUS_OK;

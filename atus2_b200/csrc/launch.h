@@ -23,6 +23,9 @@ int launch_pass2_d_t(atus_ctx *ctx, PassArgs &a, int axis, int mode, bool stride
 int launch_pass2_f_t(atus_ctx *ctx, PassArgs &a, int axis, int mode, bool strided);
 int launch_pass2_d_k(atus_ctx *ctx, PassArgs &a, int axis);
 int launch_pass2_f_k(atus_ctx *ctx, PassArgs &a, int axis);
+// _kr: the _k kinetic pass that also sums the Rabi balls (M2_KIN_RABI)
+int launch_pass2_d_kr(atus_ctx *ctx, PassArgs &a, int axis);
+int launch_pass2_f_kr(atus_ctx *ctx, PassArgs &a, int axis);
 int launch_pass2_d_nl(atus_ctx *ctx, PassArgs &a, int axis, int tc);
 int launch_pass2_f_nl(atus_ctx *ctx, PassArgs &a, int axis, int tc);
 // Plane pipeline of the 3D real-space half step (pipe.cuh) for n1 == n2 in

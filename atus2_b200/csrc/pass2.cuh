@@ -113,7 +113,7 @@ __device__ __forceinline__ bool p2_setup(const PassArgs &a, unsigned char *smem_
   }
   // k-space passes: along-axis kinetic factors of components 0 and 1
   double2 *const s_kt = reinterpret_cast<double2 *>(smem_raw + Cfg::smem);
-  const bool kt_shared = (MODE == M2_KIN) && Cfg::kin_smem && a.op == OP_KIN && a.ncomp_grid <= 2;
+  const bool kt_shared = (MODE == M2_KIN || MODE == M2_KIN_RABI) && Cfg::kin_smem && a.op == OP_KIN && a.ncomp_grid <= 2;
   if (kt_shared) {
     for (int e = tid; e < a.ncomp_grid * N; e += NT) {
       const int cc = e / N, i = e % N;
@@ -128,9 +128,45 @@ __device__ __forceinline__ bool p2_setup(const PassArgs &a, unsigned char *smem_
 // One work item: the tile g of the pass described by a.  Field loads go
 // through L2 only (ld.global.cg) when L2LOAD is set -- the fused plane
 // pipeline reads data that other CTAs of the same launch wrote.
+// Rabi sums of one thread's 16 values (k-space points j + R2 m of the pencil
+// whose point 0 has axis indices p0) into rq, with the ball rule of
+// compute_rabi_integrals (include/CRT_Base_IF.h:231-257): a point inside a
+// ball adds to the current bin and the bin index does not advance for it.
+template <typename R, int N>
+__device__ __forceinline__ void p2_rabi(const PassArgs &a, int ci, const int *p0, int j, const cplx<R> *v, double *rq) {
+  constexpr int R2 = N / 16;
+  #pragma unroll 1
+  for (int m = 0; m < 16; m++) {
+    const int i = j + R2 * m;
+    const double den = (double)v[m].x * (double)v[m].x + (double)v[m].y * (double)v[m].y;
+    double k[3];
+    #pragma unroll
+    for (int ax = 0; ax < 3; ax++) {
+      const int idx = (ax == a.axis) ? i : p0[ax];
+      const int sh = a.n[ax] / 2;
+      const int t = (idx + sh) % a.n[ax];
+      k[ax] = a.dk[ax] * (double)(t - sh);
+    }
+    int jb = 0;
+    for (int q = 0; q < a.rabi_n; q++) {
+      double dd = 0;
+      #pragma unroll
+      for (int ax = 0; ax < 3; ax++) {
+        const double d = a.rabi_k0[ci * a.rabi_n + q][ax] - k[ax];
+        dd += d * d;
+      }
+      if (sqrt(dd) < a.rabi_thr) {
+        rq[ci * a.rabi_n + jb] += den;
+        continue;
+      }
+      jb++;
+    }
+  }
+}
+
 template <typename R, int N, int TC, int MODE, bool STRIDED, bool L2LOAD>
 __device__ __forceinline__ void p2_item(const PassArgs &a, const TileGeo &g, unsigned char *smem_raw, bool kt_shared,
-                                        double *s_om, double *s_ec, double *s_es) {
+                                        double *s_om, double *s_ec, double *s_es, double *rq = nullptr) {
   using C = cplx<R>;
   using TW = typename TwTab<R>::type;
   using Cfg = P2Cfg<R, N, TC>;
@@ -175,10 +211,16 @@ __device__ __forceinline__ void p2_item(const PassArgs &a, const TileGeo &g, uns
     p2_transform<R, N, -1, !STRIDED>(v, my, twS, j);
   } else if constexpr (MODE == M2_INV) {
     p2_transform<R, N, +1, !STRIDED>(v, my, twS, j);
-  } else if constexpr (MODE == M2_KIN) {
+  } else if constexpr (MODE == M2_KIN || MODE == M2_KIN_RABI) {
     p2_transform<R, N, -1, !STRIDED>(v, my, twS, j);
     int p0[3];
     idx3(a.g, lb, p0[0], p0[1], p0[2]);
+    if constexpr (MODE == M2_KIN_RABI) {
+      int ci = -1;
+      for (int c = 0; c < a.rabi_ncomp; c++)
+        if (a.rabi_comp[c] == g.comp0) ci = c;
+      if (live && ci >= 0) p2_rabi<R, N>(a, ci, p0, j, v, rq);
+    }
     if (a.op == OP_KIN) {
       // psi^ <- ((psi^ s_f) K) s_b in FP64, K = K_along (product of the other
       // two axis factors, x before y before z); complex64 fields take the
@@ -327,9 +369,28 @@ __global__ void __launch_bounds__(Tile2<R>::NT, Tile2<R>::MINB) pass2_kernel(Pas
   const bool kt_shared = p2_setup<R, N, TC, MODE>(a, smem_raw);
   __syncthreads();  // twiddle rows and kinetic factors visible to every warp
   const int64_t W = a.per_comp ? a.ntiles * a.ncomp_grid : a.ntiles;
+  double rq[MODE == M2_KIN_RABI ? RED_MAXQ : 1];
+  #pragma unroll
+  for (int q = 0; q < (MODE == M2_KIN_RABI ? RED_MAXQ : 1); q++) rq[q] = 0.0;
   for (int64_t w = blockIdx.x; w < W; w += gridDim.x) {
     if (STRIDED && w + gridDim.x < W) p2_prefetch_l2<R, N, TC>(a, tile_geo<Cfg::B, N>(a, w + gridDim.x));
-    p2_item<R, N, TC, MODE, STRIDED, false>(a, tile_geo<Cfg::B, N>(a, w), smem_raw, kt_shared, s_om, s_ec, s_es);
+    p2_item<R, N, TC, MODE, STRIDED, false>(a, tile_geo<Cfg::B, N>(a, w), smem_raw, kt_shared, s_om, s_ec, s_es, rq);
+  }
+  if constexpr (MODE == M2_KIN_RABI) {
+    // per-CTA sums in a fixed tree (the tiles of a CTA are fixed by the grid
+    // size, so the result does not depend on scheduling)
+    __syncthreads();
+    double *sh = reinterpret_cast<double *>(smem_raw);
+    for (int q = 0; q < a.rabi_ncomp * a.rabi_n; q++) {
+      sh[threadIdx.x] = rq[q];
+      __syncthreads();
+      for (int s = Cfg::NT / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        __syncthreads();
+      }
+      if (threadIdx.x == 0) a.rabi_partial[blockIdx.x * RED_MAXQ + q] = sh[0];
+      __syncthreads();
+    }
   }
 }
 

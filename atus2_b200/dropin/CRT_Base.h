@@ -155,6 +155,41 @@ class CRT_Base : public CRT_shared {
     (*step_fct)(this, seq);
     (*half_fct)(this, seq);
   }
+  // strang_block that also returns the Rabi sums of the block's final state
+  // (component comps[c] with centres k0[c], all lists of one length) when the
+  // block runs fused on the GPU: the sums are then taken inside its last
+  // kinetic pass.  Returns false (sums untouched) when the block ran
+  // otherwise; the caller computes them separately then.
+  bool strang_block_rabi(sequence_item &seq, int Nk, StepFunction step_fct, StepFunction half_fct,
+                         StepFunction full_fct, const std::vector<int> &comps,
+                         const std::vector<const std::vector<CPoint<dim>> *> &k0, double thr,
+                         std::vector<std::vector<double>> &sums) {
+    const int kind = gpu_kind(seq.name);
+    const size_t n = k0.empty() ? 0 : k0[0]->size();
+    bool ok = kind >= 0 && half_fct == &Do_FT_Step_half_Wrapper && full_fct == &Do_FT_Step_full_Wrapper && n > 0 &&
+              comps.size() * n <= 8;
+    for (auto *l : k0) ok = ok && l->size() == n;
+    if (!ok) {
+      strang_block(seq, Nk, step_fct, half_fct, full_fct);
+      return false;
+    }
+    upload_step_parameters(seq);
+    std::vector<double> F, kk, out(comps.size() * n);
+    pulse_amplitudes(seq, Nk, F);
+    for (auto *l : k0)
+      for (auto &p : *l)
+        for (int a = 0; a < dim; a++) kk.push_back(p[a]);
+    gpu_before();
+    atus_check(m_gpu,
+               atus_strang_block_rabi(m_gpu, Nk, kind, F.data(), (int)comps.size(), comps.data(), kk.data(), (int)n,
+                                      thr, out.data()),
+               "strang_block_rabi");
+    gpu_after();
+    sums.assign(comps.size(), std::vector<double>(n));
+    for (size_t c = 0; c < comps.size(); c++)
+      for (size_t m = 0; m < n; m++) sums[c][m] = out[c * n + m];
+    return true;
+  }
   // the registered step of a tag; as in the reference a tag nobody
   // registered ends the program (a GPU kind only speeds up a registered tag)
   StepFunction step_function(const std::string &tag) {

@@ -321,7 +321,17 @@ void CRT_Base_IF<T, dim, no_int_states>::run_sequence() {
       chirp_rate[0] = dw[s];
       if (seq.chirp_mode == 1) phase[0] = s * 2.0 * M_PI / (1.0 * seq.no_of_chirps);
       for (int i = 1; i <= Na; i++) {
-        this->strang_block(seq, Nk, step_fct, half_fct, full_fct);
+        // with Rabi output each block, the sums come out of the block's last
+        // kinetic pass where it runs fused on the GPU
+        bool rabi_done = false;
+        if (seq.rabi_output_freq == freq::each && nrm > 0) {
+          std::vector<std::vector<double>> sums;
+          rabi_done = this->strang_block_rabi(seq, Nk, step_fct, half_fct, full_fct, {0}, {&m_rabi_momentum_list},
+                                              m_rabi_threshold, sums);
+          if (rabi_done) m_rabi_freq_list.push_back(list<double>(sums[0].begin(), sums[0].end()));
+        } else {
+          this->strang_block(seq, Nk, step_fct, half_fct, full_fct);
+        }
         std::cout << "t = " << to_string(m_header.t) << std::endl;
         if (seq.output_freq == freq::each && s == 0)
           for (int k = 0; k < no_int_states; k++) {
@@ -336,7 +346,7 @@ void CRT_Base_IF<T, dim, no_int_states>::run_sequence() {
         if (seq.compute_pn_freq == freq::each)
           for (int c = 0; c < no_int_states; c++)
             std::cout << "N[" << c << "] = " << this->Get_Particle_Number(c) << std::endl;
-        if (seq.rabi_output_freq == freq::each) compute_rabi_integrals();
+        if (seq.rabi_output_freq == freq::each && !rabi_done) compute_rabi_integrals();
         if (seq.custom_freq == freq::each && m_custom_fct != nullptr) (*m_custom_fct)(this, seq);
       }
       if (seq.output_freq == freq::last && s == 0)

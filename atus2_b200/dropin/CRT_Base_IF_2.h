@@ -234,13 +234,27 @@ void CRT_Base_IF_2<T, dim, no_int_states>::run_sequence() {
       m_rabi_freq_list2.clear();
       chirp_rate[0] = 0.0;
       for (int i = 1; i <= Na; i++) {
-        this->strang_block(seq, Nk, step_fct, half_fct, full_fct);
+        // with Rabi output each block, both species' sums come out of the
+        // block's last kinetic pass where it runs fused on the GPU
+        bool rabi_done = false;
+        if (seq.rabi_output_freq == freq::each && nrm > 0 && !m_rabi_momentum_list2.empty()) {
+          std::vector<std::vector<double>> sums;
+          rabi_done = this->strang_block_rabi(seq, Nk, step_fct, half_fct, full_fct, {0, no_int_states / 2},
+                                              {&m_rabi_momentum_list, &m_rabi_momentum_list2}, m_rabi_threshold,
+                                              sums);
+          if (rabi_done) {
+            m_rabi_freq_list.push_back(list<double>(sums[0].begin(), sums[0].end()));
+            m_rabi_freq_list2.push_back(list<double>(sums[1].begin(), sums[1].end()));
+          }
+        } else {
+          this->strang_block(seq, Nk, step_fct, half_fct, full_fct);
+        }
         std::cout << "t = " << to_string(m_header.t) << std::endl;
         if (seq.output_freq == freq::each) save_all();
         if (seq.compute_pn_freq == freq::each)
           for (int c = 0; c < no_int_states; c++)
             std::cout << "N[" << c << "] = " << this->Get_Particle_Number(c) << std::endl;
-        if (seq.rabi_output_freq == freq::each) compute_rabi_integrals();
+        if (seq.rabi_output_freq == freq::each && !rabi_done) compute_rabi_integrals();
         if (seq.custom_freq == freq::each && m_custom_fct != nullptr) (*m_custom_fct)(this, seq);
       }
       if (seq.output_freq == freq::last) save_all();

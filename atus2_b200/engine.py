@@ -110,6 +110,7 @@ SIGNATURES = {
     "atus_ft_step": (_i, [_vp, _i]),
     "atus_nl_step": (_i, [_vp, _i, _d]),
     "atus_strang_block": (_i, [_vp, _i, _i, _dp]),
+    "atus_strang_block_rabi": (_i, [_vp, _i, _i, _dp, _i, C.POINTER(C.c_int), _dp, _i, C.c_double, _dp]),
     "atus_profile_passes": (_i, [_vp, _i, _i, _dp, _dp, _dp, C.POINTER(C.c_int)]),
     "atus_particle_number": (_i, [_vp, _i, _dp]),
     "atus_set_bragg_stable": (_i, [_vp, _i]),
@@ -331,6 +332,22 @@ class Solver:
                 raise ValueError("F needs one amplitude per potential step")
         self._ok(self._L.atus_strang_block(self._c, int(nk), int(kind), None if Fa is None else _dptr(Fa)),
                  "strang_block")
+
+    def block_rabi(self, nk: int, kind: int, comps, k0, thr: float, laser: Laser | None = None, F=None) -> np.ndarray:
+        """block() that also returns the Rabi sums of its final state for
+        components comps (one k0 list per component): shape (len(comps), n)."""
+        if laser is not None:
+            self.set_laser(laser)
+        Fa = None if F is None else np.ascontiguousarray(F, dtype=np.float64)
+        if Fa is not None and Fa.size < nk:
+            raise ValueError("F needs one amplitude per potential step")
+        cs = (C.c_int * len(comps))(*comps)
+        k = np.ascontiguousarray(k0, dtype=np.float64).reshape(len(comps), -1, self.dim)
+        out = np.zeros(k.shape[0] * k.shape[1])
+        self._ok(self._L.atus_strang_block_rabi(self._c, int(nk), int(kind), None if Fa is None else _dptr(Fa),
+                                                len(comps), cs, _dptr(k), k.shape[1], float(thr), _dptr(out)),
+                 "strang_block_rabi")
+        return out.reshape(k.shape[0], k.shape[1])
 
     # ------------------------------------------------------------ observables
     def particle_number(self, comp: int = 0) -> float:

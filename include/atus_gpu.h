@@ -31,7 +31,7 @@
  *                                   CRT_Base_IF::Do_NL_Step (CRT_Base_IF.h:380-419),
  *                                   Bragg_single::Do_Bragg_ad
  *                                   (source/interferometry/src/bragg.cpp:185-304)
- *   atus_strang_block               the inner loop of run_sequence,
+ *   atus_strang_block(_rabi)        the inner loop of run_sequence,
  *                                   half,(V,full)^(Nk-1),V,half
  *                                   (include/CRT_Base.h:776-786,
  *                                   CRT_Base_IF.h:779-789), fused on the GPU
@@ -187,6 +187,17 @@ ATUS_API int atus_nl_step(atus_ctx *ctx, int kind, double F);
 /* nk Strang steps: half, (V, full)^(nk-1), V, half.  F[j] is the pulse
  * amplitude of the j-th potential step (NULL: all 1). */
 ATUS_API int atus_strang_block(atus_ctx *ctx, int nk, int kind, const double *F);
+/* atus_strang_block with the Rabi sums of the block's final state:
+ * compute_rabi_integrals (include/CRT_Base_IF.h:207-281; both species of
+ * CRT_Base_IF_2, include/CRT_Base_IF_2.h:115-210) of components comps[c]
+ * (c < ncomp_r <= 2) for the centres k0[(c*n + m)*dim ..] (m < n, ncomp_r*n <=
+ * 8), radius thr, into out[c*n + m].  Where the block's last kinetic pass is
+ * the register-staged x pass (2D / 3D, 32 <= nx <= 256) the sums are taken
+ * inside it (every axis is in k-space there and |psi^|^2 does not see the
+ * kinetic phase); otherwise by a separate transform and reduction as
+ * atus_rabi_integrals_comp does. */
+ATUS_API int atus_strang_block_rabi(atus_ctx *ctx, int nk, int kind, const double *F, int ncomp_r, const int *comps,
+                                    const double *k0, int n, double thr, double *out);
 
 /* ------------------------------------------------------------ measurement */
 /* Device time of the fused passes that make up one Strang step of `kind`,

@@ -212,6 +212,38 @@ def test_primitives_match_oracle():
     np.testing.assert_allclose(s.rabi_integrals(k0, 1.0), o.rabi_integrals(k0, 1.0), rtol=1e-12, atol=1e-14)
 
 
+@pytest.mark.parametrize("grid,ncomp,comps", [([64, 32, 32], 2, [0]), ([64, 64], 2, [0, 1]), ([32, 16, 32], 4, [0, 2]),
+                                              ([16, 8, 16], 2, [0])])
+def test_block_rabi_fused_matches_oracle(grid, ncomp, comps):
+    """atus_strang_block_rabi: the Rabi sums taken inside the block's last
+    kinetic pass (register-staged x pass for nx in 32..256; the 16-point grid
+    takes the separate reduction) against the oracle's compute_rabi_integrals
+    of the state after the block, at 1e-12; the state itself is the plain
+    block's."""
+    dim = len(grid)
+    h = _grid(dim, grid, 16.0)
+    X = _coords(h)
+    r2 = sum(x * x for x in X)
+    rng = np.random.default_rng(11)
+    psi = [np.exp(-0.5 * r2) * (1 + 0.2 * rng.standard_normal(r2.shape)) * np.exp(1j * (c + 1) * X[0]) + 0j
+           for c in range(ncomp)]
+    gs = list(np.full(ncomp * ncomp, 20.0))
+    o, s = _setup_pair(h, ncomp, psi, [0.5] * dim, gs, None, 1e-3)
+    kw = dict(beta=[0.1, 0, 0], DeltaL=[0, 0.5, 0, 0.3], Amp=[3.0, 3.0], laser_k=[2.0, 0], laser_dk=[0, 0],
+              laser_domh=[4.0, 0], phase=[0, 0], chirp_rate=[0, 0], chirp=0.0)
+    kind = KIND_BRAGG_AD if ncomp == 2 else KIND_NL_IF_2
+    k0 = [[[0.0] * dim, [4.0] + [0.0] * (dim - 1), [-4.0] + [0.0] * (dim - 1)],
+          [[0.0] * dim, [2.0] + [0.0] * (dim - 1), [-2.0] + [0.0] * (dim - 1)]][: len(comps)]
+    F = np.full(10, 0.8)
+    o.block(10, kind, OLaser.make(**kw), F)
+    got = s.block_rabi(10, kind, comps, k0, 1.0, Laser.make(**kw), F)
+    state_close([s.psi(c) for c in range(ncomp)], [o.psi(c) for c in range(ncomp)], FP64_TOL)
+    for i, c in enumerate(comps):
+        ref = o.rabi_integrals(k0[i], 1.0, c)
+        assert ref[0] > 1e-6
+        np.testing.assert_allclose(got[i], ref, rtol=1e-12, atol=1e-14)
+
+
 @pytest.mark.parametrize("dim,n", [(1, [4096]), (2, [64, 256]), (3, [16, 32, 256])])
 def test_field_transform_matches_oracle(dim, n):
     """atus_ft (cft_Nd::ft: transform over all axes, then the reference's
