@@ -52,6 +52,12 @@ struct atus_ctx {
   cudaGraphExec_t sob_graph = nullptr;  // a chunk of device-side iterations
   double sob_graph_step = 0;            // stepsize the graph was captured with
   void *h_sob = nullptr;                // pinned host copy of the SobDev
+  // asynchronous output snapshots
+  void *snap = nullptr;                 // ncomp x N complex128 staging copy
+  cudaStream_t copy_stream = nullptr;   // its device->host copies
+  cudaEvent_t snap_taken = nullptr;     // the staging copy is complete
+  cudaEvent_t snap_done = nullptr;      // the host copies are complete
+  bool snap_pending = false;
 };
 
 // ------------------------------------------------------------------ errors

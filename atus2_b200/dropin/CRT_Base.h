@@ -34,6 +34,7 @@
 #include <sstream>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "CRT_shared.h"
@@ -91,6 +92,62 @@ class CRT_Base : public CRT_shared {
   std::array<vector<double>, no_int_states> m_Potential;
   std::map<std::string, StepFunction> m_map_stepfcts;
   StepFunction m_custom_fct;
+
+  // ---- asynchronous file output of run_sequence
+  // The files of an output point (Save_Phi / Append_Phi of every component)
+  // are written from a snapshot: the fields are copied into pinned host
+  // buffers on a copy stream while the next block runs, and a writer thread
+  // writes the files once the copies are done.  One output point is in flight
+  // at a time; finish_output() waits for it (before the next one, before any
+  // file is read back, and when run_sequence ends).  ATUS_SYNC_OUTPUT=1
+  // writes synchronously instead.
+  std::vector<double *> m_out_buf;
+  std::thread m_writer;
+  void finish_output() {
+    if (m_writer.joinable()) m_writer.join();
+  }
+  void output_point(const char *fmt_or_name, bool append, int seq_counter = 0) {
+    char filename[1024];
+    std::vector<std::string> names;
+    for (int k = 0; k < no_int_states; k++) {
+      if (append) snprintf(filename, sizeof filename, fmt_or_name, seq_counter, k + 1);
+      else snprintf(filename, sizeof filename, fmt_or_name, this->Get_t(), k + 1);
+      names.push_back(filename);
+    }
+    const char *sync = std::getenv("ATUS_SYNC_OUTPUT");
+    if (sync && sync[0] == '1') {
+      for (int k = 0; k < no_int_states; k++) append ? Append_Phi(names[k], k) : Save_Phi(names[k], k);
+      return;
+    }
+    finish_output();
+    if (m_out_buf.empty())
+      for (int k = 0; k < no_int_states; k++) {
+        void *p = nullptr;
+        atus_check(m_gpu, atus_host_alloc(sizeof(fftw_complex) * (size_t)m_no_of_pts, &p), "host_alloc");
+        m_out_buf.push_back(static_cast<double *>(p));
+      }
+    gpu_before();
+    atus_check(m_gpu, atus_snapshot_async(m_gpu, m_out_buf.data()), "snapshot");
+    const generic_header h = m_header;
+    const size_t bytes = sizeof(fftw_complex) * (size_t)m_no_of_pts;
+    atus_ctx *ctx = m_gpu;
+    std::vector<double *> bufs = m_out_buf;
+    m_writer = std::thread([ctx, h, bytes, bufs, names, append]() {
+      if (atus_snapshot_wait(ctx) != ATUS_OK) {
+        std::cerr << "GPU error in snapshot: " << atus_last_error(ctx) << std::endl;
+        exit(EXIT_FAILURE);
+      }
+      for (size_t k = 0; k < names.size(); k++) {
+        std::ofstream f(names[k], append ? (std::ofstream::binary | std::ofstream::app) : std::ofstream::binary);
+        if (f.fail()) {
+          std::cout << "File " << names[k] << " could not be opened. Failbit: " << f.rdstate() << std::endl;
+          exit(EXIT_FAILURE);
+        }
+        f.write(reinterpret_cast<const char *>(&h), sizeof(generic_header));
+        f.write(reinterpret_cast<const char *>(bufs[k]), bytes);
+      }
+    });
+  }
 
   // ---- GPU side
   atus_ctx *m_gpu = nullptr;
@@ -212,6 +269,7 @@ class CRT_Base : public CRT_shared {
   }
   // reads component k of a .bin file into its mirror (a restart point)
   void reload(const std::string &filename, int k) {
+    finish_output();
     std::ifstream f(filename, std::ifstream::binary);
     if (!f.is_open()) return;
     f.seekg(sizeof(generic_header), std::ifstream::beg);
@@ -266,6 +324,8 @@ CRT_Base<T, dim, no_int_states>::CRT_Base(ParameterHandler *params) {
 
 template <class T, int dim, int no_int_states>
 CRT_Base<T, dim, no_int_states>::~CRT_Base() {
+  finish_output();
+  for (double *p : m_out_buf) atus_host_free(p);
   for (int i = 0; i < no_int_states; i++) delete m_fields[i];
   atus_destroy(m_gpu);
 }
@@ -407,12 +467,14 @@ void CRT_Base<T, dim, no_int_states>::Save(fftw_complex *data, std::string filen
 // Save_Phi / Append_Phi (include/CRT_Base.h:606-641)
 template <class T, int dim, int no_int_states>
 void CRT_Base<T, dim, no_int_states>::Save_Phi(std::string filename, const int comp) {
+  finish_output();
   std::ofstream f(filename, std::ofstream::binary);
   f.write(reinterpret_cast<const char *>(&m_header), sizeof(generic_header));
   f.write(reinterpret_cast<const char *>(m_fields[comp]->host_view()), sizeof(fftw_complex) * m_no_of_pts);
 }
 template <class T, int dim, int no_int_states>
 void CRT_Base<T, dim, no_int_states>::Append_Phi(std::string filename, const int comp) {
+  finish_output();
   std::ofstream f(filename, std::ofstream::binary | std::ofstream::app);
   if (f.fail()) {
     std::cout << "File " << filename << " could not be opened. Failbit: " << f.rdstate() << std::endl;
@@ -464,6 +526,7 @@ void CRT_Base<T, dim, no_int_states>::run_sequence() {
     if (double(Na * Nk) * seq.dt != max_duration) std::cout << "FYI: double(Na*Nk)*seq.dt != max_duration\n";
     if (this->Get_dt() != seq.dt) this->Set_dt(seq.dt);
     StepFunction step_fct = step_function(seq.name);
+    finish_output();
     for (int k = 0; k < no_int_states; k++) {
       snprintf(filename, sizeof filename, "Seq_%d_%d.bin", seq_counter, k + 1);
       std::remove(filename);
@@ -471,32 +534,27 @@ void CRT_Base<T, dim, no_int_states>::run_sequence() {
     for (int i = 1; i <= Na; i++) {
       strang_block(seq, Nk, step_fct, half_fct, full_fct);
       std::cout << "t = " << std::to_string(m_header.t) << std::endl;
-      if (seq.output_freq == freq::each)
-        for (int k = 0; k < no_int_states; k++) {
-          snprintf(filename, sizeof filename, "%.3f_%d.bin", this->Get_t(), k + 1);
-          this->Save_Phi(filename, k);
-        }
-      if (seq.output_freq == freq::packed)
-        for (int k = 0; k < no_int_states; k++) {
-          snprintf(filename, sizeof filename, "Seq_%d_%d.bin", seq_counter, k + 1);
-          this->Append_Phi(filename, k);
-        }
+      if (seq.output_freq == freq::each) output_point("%.3f_%d.bin", false);
+      if (seq.output_freq == freq::packed) output_point("Seq_%d_%d.bin", true, seq_counter);
       if (seq.compute_pn_freq == freq::each)
         for (int c = 0; c < no_int_states; c++)
           std::cout << "N[" << c << "] = " << this->Get_Particle_Number(c) << std::endl;
-      if (seq.custom_freq == freq::each && m_custom_fct != nullptr) (*m_custom_fct)(this, seq);
-    }
-    if (seq.output_freq == freq::last)
-      for (int k = 0; k < no_int_states; k++) {
-        snprintf(filename, sizeof filename, "%.3f_%d.bin", this->Get_t(), k + 1);
-        this->Save_Phi(filename, k);
+      if (seq.custom_freq == freq::each && m_custom_fct != nullptr) {
+        finish_output();
+        (*m_custom_fct)(this, seq);
       }
+    }
+    if (seq.output_freq == freq::last) output_point("%.3f_%d.bin", false);
     if (seq.compute_pn_freq == freq::last)
       for (int c = 0; c < no_int_states; c++)
         std::cout << "N[" << c << "] = " << this->Get_Particle_Number(c) << std::endl;
-    if (seq.custom_freq == freq::last && m_custom_fct != nullptr) (*m_custom_fct)(this, seq);
+    if (seq.custom_freq == freq::last && m_custom_fct != nullptr) {
+      finish_output();
+      (*m_custom_fct)(this, seq);
+    }
     seq_counter++;
   }
+  finish_output();
 }
 
 #endif

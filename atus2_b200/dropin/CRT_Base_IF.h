@@ -300,6 +300,7 @@ void CRT_Base_IF<T, dim, no_int_states>::run_sequence() {
     if (seq.name == "freeprop") seq.no_of_chirps = 1;
     const double backup_t = m_header.t;
     double backup_end_t = m_header.t;
+    this->finish_output();
     for (int k = 0; k < no_int_states; k++) {
       snprintf(filename, sizeof filename, "Seq_%d_%d.bin", seq_counter, k + 1);
       std::remove(filename);
@@ -333,27 +334,18 @@ void CRT_Base_IF<T, dim, no_int_states>::run_sequence() {
           this->strang_block(seq, Nk, step_fct, half_fct, full_fct);
         }
         std::cout << "t = " << to_string(m_header.t) << std::endl;
-        if (seq.output_freq == freq::each && s == 0)
-          for (int k = 0; k < no_int_states; k++) {
-            snprintf(filename, sizeof filename, "%.3f_%d.bin", this->Get_t(), k + 1);
-            this->Save_Phi(filename, k);
-          }
-        if (seq.output_freq == freq::packed && s == 0)
-          for (int k = 0; k < no_int_states; k++) {
-            snprintf(filename, sizeof filename, "Seq_%d_%d.bin", seq_counter, k + 1);
-            this->Append_Phi(filename, k);
-          }
+        if (seq.output_freq == freq::each && s == 0) this->output_point("%.3f_%d.bin", false);
+        if (seq.output_freq == freq::packed && s == 0) this->output_point("Seq_%d_%d.bin", true, seq_counter);
         if (seq.compute_pn_freq == freq::each)
           for (int c = 0; c < no_int_states; c++)
             std::cout << "N[" << c << "] = " << this->Get_Particle_Number(c) << std::endl;
         if (seq.rabi_output_freq == freq::each && !rabi_done) compute_rabi_integrals();
-        if (seq.custom_freq == freq::each && m_custom_fct != nullptr) (*m_custom_fct)(this, seq);
-      }
-      if (seq.output_freq == freq::last && s == 0)
-        for (int k = 0; k < no_int_states; k++) {
-          snprintf(filename, sizeof filename, "%.3f_%d.bin", this->Get_t(), k + 1);
-          this->Save_Phi(filename, k);
+        if (seq.custom_freq == freq::each && m_custom_fct != nullptr) {
+          this->finish_output();
+          (*m_custom_fct)(this, seq);
         }
+      }
+      if (seq.output_freq == freq::last && s == 0) this->output_point("%.3f_%d.bin", false);
       if (seq.no_of_chirps > 1 && s == 0) {
         backup_end_t = this->Get_t();
         for (int k = 0; k < no_int_states; k++) {
@@ -364,7 +356,10 @@ void CRT_Base_IF<T, dim, no_int_states>::run_sequence() {
       if (seq.compute_pn_freq == freq::last)
         for (int c = 0; c < no_int_states; c++)
           std::cout << "N[" << c << "] = " << this->Get_Particle_Number(c) << std::endl;
-      if (seq.custom_freq == freq::last && m_custom_fct != nullptr) (*m_custom_fct)(this, seq);
+      if (seq.custom_freq == freq::last && m_custom_fct != nullptr) {
+        this->finish_output();
+        (*m_custom_fct)(this, seq);
+      }
       if (seq.rabi_output_freq == freq::last) {
         compute_rabi_integrals();
         cout << "Rabi output for timestep ";
@@ -418,6 +413,7 @@ void CRT_Base_IF<T, dim, no_int_states>::run_sequence() {
     }
     seq_counter++;
   }
+  this->finish_output();
 }
 
 #endif

@@ -183,13 +183,7 @@ class CRT_Base_IF_2 : public CRT_Base_2<T, dim, no_int_states> {
       t += dt_out;
     }
   }
-  void save_all() {
-    char filename[1024];
-    for (int k = 0; k < no_int_states; k++) {
-      snprintf(filename, sizeof filename, "%.3f_%d.bin", this->Get_t(), k + 1);
-      this->Save_Phi(filename, k);
-    }
-  }
+  void save_all() { this->output_point("%.3f_%d.bin", false); }
 };
 
 // CRT_Base_IF_2::run_sequence (include/CRT_Base_IF_2.h:420-593)
@@ -255,13 +249,19 @@ void CRT_Base_IF_2<T, dim, no_int_states>::run_sequence() {
           for (int c = 0; c < no_int_states; c++)
             std::cout << "N[" << c << "] = " << this->Get_Particle_Number(c) << std::endl;
         if (seq.rabi_output_freq == freq::each && !rabi_done) compute_rabi_integrals();
-        if (seq.custom_freq == freq::each && m_custom_fct != nullptr) (*m_custom_fct)(this, seq);
+        if (seq.custom_freq == freq::each && m_custom_fct != nullptr) {
+          this->finish_output();
+          (*m_custom_fct)(this, seq);
+        }
       }
       if (seq.output_freq == freq::last) save_all();
       if (seq.compute_pn_freq == freq::last)
         for (int c = 0; c < no_int_states; c++)
           std::cout << "N[" << c << "] = " << this->Get_Particle_Number(c) << std::endl;
-      if (seq.custom_freq == freq::last && m_custom_fct != nullptr) (*m_custom_fct)(this, seq);
+      if (seq.custom_freq == freq::last && m_custom_fct != nullptr) {
+        this->finish_output();
+        (*m_custom_fct)(this, seq);
+      }
       if (seq.rabi_output_freq == freq::last) {
         compute_rabi_integrals();
         cout << "Spezie 1" << endl;
@@ -306,6 +306,7 @@ void CRT_Base_IF_2<T, dim, no_int_states>::run_sequence() {
     }
     seq_counter++;
   }
+  this->finish_output();
 }
 
 #endif

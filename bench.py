@@ -709,6 +709,8 @@ def atus_arm(args, rank, ws, local, dist):
         barrier(dist)
         out["variants"]["config2_2d"] = run_config2(stream, args.steps, args.warmup, peak, peak_kind, cpu,
                                                     accuracy=not args.no_accuracy)
+    if not args.no_configs and rank == 0:
+        out["variants"]["file_output"] = run_output_overlap()
     if not args.no_batch:
         barrier(dist)
         out["variants"]["batch"] = run_batch()
@@ -720,6 +722,47 @@ def atus_arm(args, rank, ws, local, dist):
     barrier(dist)
     if rank == 0:
         print(json.dumps(out))
+
+
+# ------------------------------------------------------------------ file output during a run
+def run_output_overlap(blocks=5, nk=100):
+    """ATUS-2's bragg program built against the drop-in headers (host/bin/
+    bragg) on the 256^3 workload: `blocks` blocks of `nk` steps with every
+    component written after each block (output_freq="each", 537 MB per
+    output), against the same run without output, with the files written
+    from snapshots by a writer thread (the default) and synchronously
+    (ATUS_SYNC_OUTPUT=1).  Wall time of each whole program run."""
+    prog = os.path.join(ROOT, "atus2_b200", "host", "bin", "bragg")
+    if not os.path.exists(prog):
+        return {"unavailable": "host/bin/bragg is not built (needs the ATUS-2 source tree at build time)"}
+    from atus2_b200 import binfmt
+
+    def xml(freq):
+        return bragg_xml(nk).replace(f'Nk="{nk}" output_freq="none"', f'Nk="{nk}" output_freq="{freq}"').replace(
+            f">{nk * DT!r}</bragg_ad>", f">{blocks * nk * DT!r}</bragg_ad>")
+
+    out = {"grid": [N, N, N], "components": 2, "blocks": blocks, "steps_per_block": nk,
+           "bytes_per_output": 2 * 16 * N ** 3}
+    with tempfile.TemporaryDirectory() as tmp:
+        h = header()
+        psi1, psi2 = initial_state(h)
+        binfmt.write_bin(os.path.join(tmp, "inp_1.bin"), h, psi1)
+        binfmt.write_bin(os.path.join(tmp, "inp_2.bin"), h, psi2)
+        runs = {"no_output": ("none", {}), "async_output": ("each", {}), "sync_output": ("each", {"ATUS_SYNC_OUTPUT": "1"})}
+        for name, (freq, extra) in runs.items():
+            open(os.path.join(tmp, "run.xml"), "w").write(xml(freq))
+            env = dict(os.environ, **extra)
+            t0 = time.perf_counter()
+            r = subprocess.run([prog, "run.xml"], cwd=tmp, env=env, capture_output=True, text=True, timeout=600)
+            out[name + "_s"] = time.perf_counter() - t0
+            if r.returncode != 0:
+                return {"error": f"{name}: rc {r.returncode}: {r.stdout[-500:]} {r.stderr[-500:]}"}
+            for fn in os.listdir(tmp):
+                if fn.endswith(".bin") and not fn.startswith("inp_"):
+                    os.remove(os.path.join(tmp, fn))
+    out["output_cost_async_s"] = out["async_output_s"] - out["no_output_s"]
+    out["output_cost_sync_s"] = out["sync_output_s"] - out["no_output_s"]
+    return out
 
 
 # ------------------------------------------------------------------ batched sweep
