@@ -137,7 +137,7 @@ class CRT_Base : public CRT_shared {
         std::cerr << "GPU error in snapshot: " << atus_last_error(ctx) << std::endl;
         exit(EXIT_FAILURE);
       }
-      for (size_t k = 0; k < names.size(); k++) {
+      auto write = [&](size_t k) {
         std::ofstream f(names[k], append ? (std::ofstream::binary | std::ofstream::app) : std::ofstream::binary);
         if (f.fail()) {
           std::cout << "File " << names[k] << " could not be opened. Failbit: " << f.rdstate() << std::endl;
@@ -145,7 +145,12 @@ class CRT_Base : public CRT_shared {
         }
         f.write(reinterpret_cast<const char *>(&h), sizeof(generic_header));
         f.write(reinterpret_cast<const char *>(bufs[k]), bytes);
-      }
+      };
+      // one file per component, written side by side
+      std::vector<std::thread> more;
+      for (size_t k = 1; k < names.size(); k++) more.emplace_back(write, k);
+      write(0);
+      for (auto &t : more) t.join();
     });
   }
 

@@ -725,7 +725,7 @@ def atus_arm(args, rank, ws, local, dist):
 
 
 # ------------------------------------------------------------------ file output during a run
-def run_output_overlap(blocks=5, nk=100):
+def run_output_overlap(blocks=3, nk=1000):
     """ATUS-2's bragg program built against the drop-in headers (host/bin/
     bragg) on the 256^3 workload: `blocks` blocks of `nk` steps with every
     component written after each block (output_freq="each", 537 MB per
