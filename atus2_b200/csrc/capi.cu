@@ -603,7 +603,7 @@ void atus_destroy(atus_ctx *ctx) {
   if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
   cudaFree(ctx->snap);
   if (ctx->snap_taken) cudaEventDestroy(ctx->snap_taken);
-  if (ctx->snap_done) cudaEventDestroy(ctx->snap_done);
+  if (ctx->snap_read) cudaEventDestroy(ctx->snap_read);
   if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
   cudaFree(ctx->scratch);
   cudaFree(ctx->pipe);
@@ -747,19 +747,19 @@ int atus_download_psi(atus_ctx *ctx, int comp, double *psi) {
 
 // ------------------------------------------------------------------ asynchronous output
 // The copy into the staging buffer runs on the context's stream (ordered after
-// the steps before it); the device->host copies run on a copy stream of the
-// context after that, so the steps enqueued next overlap them.
-int atus_snapshot_async(atus_ctx *ctx, double *const *host_dst) {
-  if (!ctx || !host_dst) return ATUS_E_ARG;
-  for (int c = 0; c < ctx->ncomp; c++)
-    if (!host_dst[c]) return ATUS_E_ARG;
-  RUN(atus_snapshot_wait(ctx));
+// the steps before it) and returns at once; the device->host copies run on a
+// copy stream of the context, from whichever host thread asks for them, so the
+// steps enqueued next overlap them.
+int atus_snapshot(atus_ctx *ctx) {
+  if (!ctx) return ATUS_E_ARG;
   if (!ctx->snap) {
     CK(cudaMalloc(&ctx->snap, (size_t)16 * ctx->npts * ctx->ncomp));
     CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&ctx->snap_taken, cudaEventDisableTiming));
-    CK(cudaEventCreateWithFlags(&ctx->snap_done, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ctx->snap_read, cudaEventDisableTiming));
   }
+  // the staging buffer may still be read by the copies of the last snapshot
+  CK(cudaStreamWaitEvent(ctx->stream, ctx->snap_read, 0));
   for (int c = 0; c < ctx->ncomp; c++) {
     double2 *dst = static_cast<double2 *>(ctx->snap) + (size_t)c * ctx->npts;
     if (ctx->prec == ATUS_PREC_FP64) {
@@ -770,35 +770,20 @@ int atus_snapshot_async(atus_ctx *ctx, double *const *host_dst) {
     }
   }
   CK(cudaEventRecord(ctx->snap_taken, ctx->stream));
-  CK(cudaStreamWaitEvent(ctx->copy_stream, ctx->snap_taken, 0));
-  for (int c = 0; c < ctx->ncomp; c++)
-    CK(cudaMemcpyAsync(host_dst[c], static_cast<double2 *>(ctx->snap) + (size_t)c * ctx->npts, 16 * ctx->npts,
-                       cudaMemcpyDeviceToHost, ctx->copy_stream));
-  CK(cudaEventRecord(ctx->snap_done, ctx->copy_stream));
-  ctx->snap_pending = true;
   return ATUS_OK;
 }
 
-int atus_snapshot_wait(atus_ctx *ctx) {
-  if (!ctx) return ATUS_E_ARG;
-  if (!ctx->snap_pending) return ATUS_OK;
-  ctx->snap_pending = false;
-  CK(cudaEventSynchronize(ctx->snap_done));
-  return ATUS_OK;
-}
-
-int atus_host_alloc(size_t bytes, void **out) {
-  if (!out) return ATUS_E_ARG;
-  *out = nullptr;
-  if (cudaHostAlloc(out, bytes ? bytes : 1, cudaHostAllocDefault) != cudaSuccess) {
-    *out = nullptr;
-    return ATUS_E_NOMEM;
-  }
-  return ATUS_OK;
-}
-
-void atus_host_free(void *p) {
-  if (p) cudaFreeHost(p);
+int atus_snapshot_read(atus_ctx *ctx, int comp, double *host_dst) {
+  if (!ctx || !host_dst || comp < 0 || comp >= ctx->ncomp) return ATUS_E_ARG;
+  if (!ctx->snap) return fail(ctx, ATUS_E_ARG, "no snapshot taken");
+  cudaStream_t s = ctx->copy_stream;
+  cudaError_t e = cudaStreamWaitEvent(s, ctx->snap_taken, 0);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(host_dst, static_cast<double2 *>(ctx->snap) + (size_t)comp * ctx->npts, 16 * ctx->npts,
+                        cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->snap_read, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  return e == cudaSuccess ? ATUS_OK : ATUS_E_CUDA;
 }
 
 int atus_device_psi(atus_ctx *ctx, int comp, void **dptr) {

@@ -56,8 +56,7 @@ struct atus_ctx {
   void *snap = nullptr;                 // ncomp x N complex128 staging copy
   cudaStream_t copy_stream = nullptr;   // its device->host copies
   cudaEvent_t snap_taken = nullptr;     // the staging copy is complete
-  cudaEvent_t snap_done = nullptr;      // the host copies are complete
-  bool snap_pending = false;
+  cudaEvent_t snap_read = nullptr;      // the last host copy from it is complete
 };
 
 // ------------------------------------------------------------------ errors

@@ -95,23 +95,25 @@ class CRT_Base : public CRT_shared {
 
   // ---- asynchronous file output of run_sequence
   // The files of an output point (Save_Phi / Append_Phi of every component)
-  // are written from a snapshot: the fields are copied into pinned host
-  // buffers on a copy stream while the next block runs, and a writer thread
-  // writes the files once the copies are done.  One output point is in flight
-  // at a time; finish_output() waits for it (before the next one, before any
-  // file is read back, and when run_sequence ends).  ATUS_SYNC_OUTPUT=1
+  // are written from a snapshot: the fields are copied into a device staging
+  // buffer (microseconds, on the compute stream), and a writer thread per
+  // component copies its field to the host and writes its file while the next
+  // block runs.  One output point is in flight at a time; finish_output()
+  // waits for it (before the next one, before any file is read back, before a
+  // custom function runs, and when run_sequence ends).  ATUS_SYNC_OUTPUT=1
   // writes synchronously instead.
-  std::vector<double *> m_out_buf;
-  std::thread m_writer;
+  std::vector<std::vector<double>> m_out_buf;
+  std::vector<std::thread> m_writers;
   void finish_output() {
-    if (m_writer.joinable()) m_writer.join();
+    for (auto &t : m_writers) t.join();
+    m_writers.clear();
   }
-  void output_point(const char *fmt_or_name, bool append, int seq_counter = 0) {
+  void output_point(const char *fmt, bool append, int seq_counter = 0) {
     char filename[1024];
     std::vector<std::string> names;
     for (int k = 0; k < no_int_states; k++) {
-      if (append) snprintf(filename, sizeof filename, fmt_or_name, seq_counter, k + 1);
-      else snprintf(filename, sizeof filename, fmt_or_name, this->Get_t(), k + 1);
+      if (append) snprintf(filename, sizeof filename, fmt, seq_counter, k + 1);
+      else snprintf(filename, sizeof filename, fmt, this->Get_t(), k + 1);
       names.push_back(filename);
     }
     const char *sync = std::getenv("ATUS_SYNC_OUTPUT");
@@ -120,38 +122,28 @@ class CRT_Base : public CRT_shared {
       return;
     }
     finish_output();
-    if (m_out_buf.empty())
-      for (int k = 0; k < no_int_states; k++) {
-        void *p = nullptr;
-        atus_check(m_gpu, atus_host_alloc(sizeof(fftw_complex) * (size_t)m_no_of_pts, &p), "host_alloc");
-        m_out_buf.push_back(static_cast<double *>(p));
-      }
+    m_out_buf.resize(no_int_states);
     gpu_before();
-    atus_check(m_gpu, atus_snapshot_async(m_gpu, m_out_buf.data()), "snapshot");
+    atus_check(m_gpu, atus_snapshot(m_gpu), "snapshot");
     const generic_header h = m_header;
-    const size_t bytes = sizeof(fftw_complex) * (size_t)m_no_of_pts;
-    atus_ctx *ctx = m_gpu;
-    std::vector<double *> bufs = m_out_buf;
-    m_writer = std::thread([ctx, h, bytes, bufs, names, append]() {
-      if (atus_snapshot_wait(ctx) != ATUS_OK) {
-        std::cerr << "GPU error in snapshot: " << atus_last_error(ctx) << std::endl;
-        exit(EXIT_FAILURE);
-      }
-      auto write = [&](size_t k) {
-        std::ofstream f(names[k], append ? (std::ofstream::binary | std::ofstream::app) : std::ofstream::binary);
+    const size_t n = 2 * (size_t)m_no_of_pts;
+    for (int k = 0; k < no_int_states; k++) {
+      std::vector<double> *buf = &m_out_buf[k];
+      m_writers.emplace_back([this, k, h, n, buf, name = names[k], append]() {
+        buf->resize(n);
+        if (atus_snapshot_read(m_gpu, k, buf->data()) != ATUS_OK) {
+          std::cerr << "GPU error reading an output snapshot" << std::endl;
+          exit(EXIT_FAILURE);
+        }
+        std::ofstream f(name, append ? (std::ofstream::binary | std::ofstream::app) : std::ofstream::binary);
         if (f.fail()) {
-          std::cout << "File " << names[k] << " could not be opened. Failbit: " << f.rdstate() << std::endl;
+          std::cout << "File " << name << " could not be opened. Failbit: " << f.rdstate() << std::endl;
           exit(EXIT_FAILURE);
         }
         f.write(reinterpret_cast<const char *>(&h), sizeof(generic_header));
-        f.write(reinterpret_cast<const char *>(bufs[k]), bytes);
-      };
-      // one file per component, written side by side
-      std::vector<std::thread> more;
-      for (size_t k = 1; k < names.size(); k++) more.emplace_back(write, k);
-      write(0);
-      for (auto &t : more) t.join();
-    });
+        f.write(reinterpret_cast<const char *>(buf->data()), sizeof(double) * n);
+      });
+    }
   }
 
   // ---- GPU side
@@ -330,7 +322,6 @@ CRT_Base<T, dim, no_int_states>::CRT_Base(ParameterHandler *params) {
 template <class T, int dim, int no_int_states>
 CRT_Base<T, dim, no_int_states>::~CRT_Base() {
   finish_output();
-  for (double *p : m_out_buf) atus_host_free(p);
   for (int i = 0; i < no_int_states; i++) delete m_fields[i];
   atus_destroy(m_gpu);
 }

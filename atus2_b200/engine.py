@@ -111,10 +111,8 @@ SIGNATURES = {
     "atus_nl_step": (_i, [_vp, _i, _d]),
     "atus_strang_block": (_i, [_vp, _i, _i, _dp]),
     "atus_strang_block_rabi": (_i, [_vp, _i, _i, _dp, _i, C.POINTER(C.c_int), _dp, _i, C.c_double, _dp]),
-    "atus_snapshot_async": (_i, [_vp, C.POINTER(_dp)]),
-    "atus_snapshot_wait": (_i, [_vp]),
-    "atus_host_alloc": (_i, [C.c_size_t, C.POINTER(C.c_void_p)]),
-    "atus_host_free": (None, [_vp]),
+    "atus_snapshot": (_i, [_vp]),
+    "atus_snapshot_read": (_i, [_vp, _i, _dp]),
     "atus_profile_passes": (_i, [_vp, _i, _i, _dp, _dp, _dp, C.POINTER(C.c_int)]),
     "atus_particle_number": (_i, [_vp, _i, _dp]),
     "atus_set_bragg_stable": (_i, [_vp, _i]),

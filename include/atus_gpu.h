@@ -24,9 +24,8 @@
  *                                   (include/CRT_Base_IF.h:65-77, 144-168)
  *   atus_upload_psi/atus_download_psi  m_fields[c]->Getp2In() contents
  *                                   (source/libs/lib_myutils/cft_base.h:175)
- *   atus_snapshot_async/_wait       Save_Phi / Append_Phi of run_sequence written from a
- *                                   snapshot (include/CRT_Base.h:606-641); atus_host_alloc/free
- *                                   its pinned buffers
+ *   atus_snapshot/_read             Save_Phi / Append_Phi of run_sequence written from a
+ *                                   snapshot (include/CRT_Base.h:606-641)
  *   atus_ft                         cft_Nd::ft (source/libs/lib_myutils/cft_3d.cpp:58-74)
  *   atus_ft_step                    Do_FT_Step_full / Do_FT_Step_half
  *                                   (include/CRT_Base.h:336-392)
@@ -177,19 +176,19 @@ ATUS_API int atus_download_psi(atus_ctx *ctx, int comp, double *psi);
 /* Device pointer of component comp (complex128 or complex64 per precision). */
 ATUS_API int atus_device_psi(atus_ctx *ctx, int comp, void **dptr);
 /* Output without stalling the steps (Save_Phi / Append_Phi of run_sequence,
- * include/CRT_Base.h:606-641, written from a snapshot): copies every
- * component into a device staging buffer of the context, ordered after the
- * steps enqueued before, then into host_dst[c] (N complex128 values each;
- * pinned memory from atus_host_alloc for the copy to overlap the next steps)
- * on a copy stream of the context, and returns at once.  atus_snapshot_wait
- * blocks until the host buffers hold the snapshot; a second snapshot first
- * waits for the one before.  The staging buffer (ncomp x N x 16 bytes) is
- * allocated by the first call. */
-ATUS_API int atus_snapshot_async(atus_ctx *ctx, double *const *host_dst /* ncomp */);
-ATUS_API int atus_snapshot_wait(atus_ctx *ctx);
-/* Page-locked host memory for snapshots (cudaHostAlloc) and its release. */
-ATUS_API int atus_host_alloc(size_t bytes, void **out);
-ATUS_API void atus_host_free(void *p);
+ * include/CRT_Base.h:606-641, written from a snapshot).  atus_snapshot
+ * copies every component into a device staging buffer of the context
+ * (complex128), ordered after the steps enqueued before, and returns at once;
+ * the steps enqueued next run while the snapshot is read.  The first call
+ * allocates the staging buffer (ncomp x N x 16 bytes); a snapshot waits on the
+ * device for the reads of the one before.
+ * atus_snapshot_read copies component comp of the last snapshot into host_dst
+ * (N complex128 values) on a copy stream of the context and returns when it
+ * is there.  It may be called from other host threads (one per component)
+ * while the context's own thread goes on with other calls; the caller makes
+ * sure the reads of one snapshot finish before it takes the next. */
+ATUS_API int atus_snapshot(atus_ctx *ctx);
+ATUS_API int atus_snapshot_read(atus_ctx *ctx, int comp, double *host_dst);
 /* cft_Nd::ft(isign) on component comp, in place (source/libs/lib_myutils/
  * cft_1d.cpp:61-77, cft_2d.cpp:58-74, cft_3d.cpp:58-74): the transform over
  * every axis with FFTW's sign convention (isign -1 forward, +1 backward),
