@@ -709,7 +709,7 @@ def atus_arm(args, rank, ws, local, dist):
         barrier(dist)
         out["variants"]["config2_2d"] = run_config2(stream, args.steps, args.warmup, peak, peak_kind, cpu,
                                                     accuracy=not args.no_accuracy)
-    if not args.no_configs and rank == 0:
+    if args.file_output and rank == 0:
         out["variants"]["file_output"] = run_output_overlap()
     if not args.no_batch:
         barrier(dist)
@@ -725,13 +725,14 @@ def atus_arm(args, rank, ws, local, dist):
 
 
 # ------------------------------------------------------------------ file output during a run
-def run_output_overlap(blocks=3, nk=1000):
+def run_output_overlap(blocks=4, nk=1000, reps=3):
     """ATUS-2's bragg program built against the drop-in headers (host/bin/
     bragg) on the 256^3 workload: `blocks` blocks of `nk` steps with every
     component written after each block (output_freq="each", 537 MB per
     output), against the same run without output, with the files written
     from snapshots by a writer thread (the default) and synchronously
-    (ATUS_SYNC_OUTPUT=1).  Wall time of each whole program run."""
+    (ATUS_SYNC_OUTPUT=1).  Median wall time of `reps` runs of each whole
+    program, the three kinds interleaved."""
     prog = os.path.join(ROOT, "atus2_b200", "host", "bin", "bragg")
     if not os.path.exists(prog):
         return {"unavailable": "host/bin/bragg is not built (needs the ATUS-2 source tree at build time)"}
@@ -749,17 +750,22 @@ def run_output_overlap(blocks=3, nk=1000):
         binfmt.write_bin(os.path.join(tmp, "inp_1.bin"), h, psi1)
         binfmt.write_bin(os.path.join(tmp, "inp_2.bin"), h, psi2)
         runs = {"no_output": ("none", {}), "async_output": ("each", {}), "sync_output": ("each", {"ATUS_SYNC_OUTPUT": "1"})}
-        for name, (freq, extra) in runs.items():
-            open(os.path.join(tmp, "run.xml"), "w").write(xml(freq))
-            env = dict(os.environ, **extra)
-            t0 = time.perf_counter()
-            r = subprocess.run([prog, "run.xml"], cwd=tmp, env=env, capture_output=True, text=True, timeout=600)
-            out[name + "_s"] = time.perf_counter() - t0
-            if r.returncode != 0:
-                return {"error": f"{name}: rc {r.returncode}: {r.stdout[-500:]} {r.stderr[-500:]}"}
-            for fn in os.listdir(tmp):
-                if fn.endswith(".bin") and not fn.startswith("inp_"):
-                    os.remove(os.path.join(tmp, fn))
+        times = {k: [] for k in runs}
+        for _ in range(reps):
+            for name, (freq, extra) in runs.items():
+                open(os.path.join(tmp, "run.xml"), "w").write(xml(freq))
+                env = dict(os.environ, **extra)
+                t0 = time.perf_counter()
+                r = subprocess.run([prog, "run.xml"], cwd=tmp, env=env, capture_output=True, text=True, timeout=600)
+                times[name].append(time.perf_counter() - t0)
+                if r.returncode != 0:
+                    return {"error": f"{name}: rc {r.returncode}: {r.stdout[-500:]} {r.stderr[-500:]}"}
+                for fn in os.listdir(tmp):
+                    if fn.endswith(".bin") and not fn.startswith("inp_"):
+                        os.remove(os.path.join(tmp, fn))
+        for name in runs:
+            out[name + "_s"] = statistics.median(times[name])
+            out[name + "_all_s"] = times[name]
     out["output_cost_async_s"] = out["async_output_s"] - out["no_output_s"]
     out["output_cost_sync_s"] = out["sync_output_s"] - out["no_output_s"]
     return out
@@ -1057,6 +1063,8 @@ def main():
     ap.add_argument("--no-sobmin", action="store_true", help="skip the ground-state variant")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the 10^4-step accuracy runs")
     ap.add_argument("--no-configs", action="store_true", help="skip the 1D and 2D workloads")
+    ap.add_argument("--file-output", action="store_true",
+                    help="also time the drop-in bragg program with output every block (async vs sync files)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, ws, local, dist = dist_init()
