@@ -777,7 +777,9 @@ int atus_snapshot_read(atus_ctx *ctx, int comp, double *host_dst) {
   if (!ctx || !host_dst || comp < 0 || comp >= ctx->ncomp) return ATUS_E_ARG;
   if (!ctx->snap) return fail(ctx, ATUS_E_ARG, "no snapshot taken");
   cudaStream_t s = ctx->copy_stream;
-  cudaError_t e = cudaStreamWaitEvent(s, ctx->snap_taken, 0);
+  // wait on the host until the staging copy is done: a copy into pageable
+  // memory queued behind it would hold up the context's other launches
+  cudaError_t e = cudaEventSynchronize(ctx->snap_taken);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(host_dst, static_cast<double2 *>(ctx->snap) + (size_t)comp * ctx->npts, 16 * ctx->npts,
                         cudaMemcpyDeviceToHost, s);
