@@ -477,6 +477,38 @@ static int scratch_forward(atus_ctx *ctx) {
   return r;
 }
 
+// Spectral prolongation: the unscaled spectrum C of a coarse field (FP64
+// scratch of the coarse context) into the spectrum of a finer grid on the same
+// box, F(m) = C(m) / Nc for every wavenumber |m| < nc/2 on each axis (the
+// coarse Nyquist plane has no partner on the fine grid and is dropped), zero
+// elsewhere; the inverse unscaled transform on the fine grid is then the
+// trigonometric interpolant of the coarse values.
+struct ProlongArgs {
+  const double2 *src;
+  double2 *dst;
+  int nc[3], nf[3];
+  double inv_nc;
+  int64_t npts_c;
+};
+__global__ void prolong_kernel(ProlongArgs a) {
+  for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < a.npts_c; l += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i2 = l % a.nc[2], i1 = (l / a.nc[2]) % a.nc[1], i0 = l / ((int64_t)a.nc[2] * a.nc[1]);
+    const int64_t ic[3] = {i0, i1, i2};
+    int64_t f = 0;
+    bool keep = true;
+    for (int ax = 0; ax < 3; ax++) {
+      const int64_t n = a.nc[ax];
+      if (n > 1 && 2 * ic[ax] == n) keep = false;           // Nyquist index
+      const int64_t m = (2 * ic[ax] < n) ? ic[ax] : ic[ax] - n;  // signed wavenumber
+      f = f * a.nf[ax] + ((m + a.nf[ax]) % a.nf[ax]);
+    }
+    if (keep) {
+      const double2 c = a.src[l];
+      a.dst[f] = make_double2(c.x * a.inv_nc, c.y * a.inv_nc);
+    }
+  }
+}
+
 // psi *= fak in FP64 (the scale pass of cft_Nd::ft)
 template <typename R>
 __global__ void ft_scale_kernel(void *psi, double fak, int64_t n) {
@@ -809,6 +841,49 @@ int atus_ft(atus_ctx *ctx, int comp, int isign) {
   else
     ft_scale_kernel<float><<<grid_blocks(ctx->npts, 256), 256, 0, ctx->stream>>>(ctx->psi[comp], fak, ctx->npts);
   LAUNCHED(ctx);
+  return ATUS_OK;
+}
+
+int atus_prolong(atus_ctx *coarse, int comp_c, atus_ctx *fine, int comp_f) {
+  if (!coarse || !fine || comp_c < 0 || comp_c >= coarse->ncomp || comp_f < 0 || comp_f >= fine->ncomp)
+    return ATUS_E_ARG;
+  atus_ctx *ctx = fine;
+  if (coarse->prec != ATUS_PREC_FP64 || fine->prec != ATUS_PREC_FP64)
+    return fail(fine, ATUS_E_UNSUPPORTED, "prolongation needs FP64 contexts");
+  if (coarse->dim != fine->dim) return fail(fine, ATUS_E_ARG, "grids of different dimension");
+  for (int ax = 0; ax < coarse->dim; ax++) {
+    if (fine->n[ax] < coarse->n[ax]) return fail(fine, ATUS_E_ARG, "the fine grid has fewer points");
+    const double Lc = coarse->d[ax] * coarse->n[ax], Lf = fine->d[ax] * fine->n[ax];
+    if (fabs(Lc - Lf) > 1e-12 * Lf) return fail(fine, ATUS_E_ARG, "grids on different boxes");
+  }
+  {  // coarse spectrum in the coarse context's scratch, on its stream
+    atus_ctx *c = coarse;
+    const int r1 = to_scratch(c, comp_c);
+    if (r1 != ATUS_OK) return r1;
+    const int r2 = scratch_forward(c);
+    if (r2 != ATUS_OK) return r2;
+    cudaEvent_t ev;
+    CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    CK(cudaEventRecord(ev, c->stream));
+    CK(cudaStreamWaitEvent(fine->stream, ev, 0));
+    cudaEventDestroy(ev);
+  }
+  CK(cudaMemsetAsync(fine->psi[comp_f], 0, 16 * fine->npts, fine->stream));
+  ProlongArgs a;
+  a.src = static_cast<const double2 *>(coarse->scratch);
+  a.dst = static_cast<double2 *>(fine->psi[comp_f]);
+  for (int ax = 0; ax < 3; ax++) {
+    a.nc[ax] = (int)coarse->n[ax];
+    a.nf[ax] = (int)fine->n[ax];
+  }
+  a.inv_nc = 1.0 / (double)coarse->npts;
+  a.npts_c = coarse->npts;
+  prolong_kernel<<<grid_blocks(coarse->npts, 256), 256, 0, fine->stream>>>(a);
+  LAUNCHED(fine);
+  void *f[1] = {fine->psi[comp_f]};
+  for (int ax = fine->dim - 1; ax >= 0; ax--) RUN(run_pass(fine, ax, T_INV, OP_NONE, T_NONE, nullptr, 0, f, 1));
+  // the coarse scratch is read by the fine stream: keep it until then
+  CK(cudaStreamSynchronize(fine->stream));
   return ATUS_OK;
 }
 

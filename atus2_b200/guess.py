@@ -148,6 +148,53 @@ def solve(n, wy, wz, g, coef=None, eps=EPS, max_iter=200000):
     return psi, it, res, dt, mu
 
 
+def solve_cascade(n, wy, wz, g, coef=None, levels=None, eps=EPS, eps_coarse=None, max_iter=400000):
+    """Coarse-to-fine sobmin: the guess (Thomas-Fermi, or the learned one when
+    coef is given) on the coarsest grid of `levels` (default n/4, n/2, n, same
+    box), the descent there to eps_coarse, then the spectral interpolant of
+    each level's converged state (atus_prolong) seeds the next finer grid; the
+    finest runs to eps with the fixed step of plain sobmin.  The slow modes of
+    the fixed-step descent are smooth, global ones, which the coarse grids
+    resolve at a fraction of the cost; what the finer grids add is fine-scale
+    structure, which the Sobolev-preconditioned descent removes quickly.
+    Returns (psi, iterations per level, residual, seconds, mu); the seconds
+    cover the descents and the interpolations (the grids and potentials are
+    set up before the clock starts, as in solve())."""
+    levels = list(levels or [n // 4, n // 2, n])
+    eps_coarse = eps if eps_coarse is None else eps_coarse
+    solvers = []
+    for k, nl in enumerate(levels):
+        h = header(nl)
+        V = potential(h, wy, wz)
+        s = Solver(h, 1, PREC_FP64)
+        if k == 0:
+            if coef is None:
+                s.set_psi(0, tf_guess(h, V, g))
+            else:
+                s.guess_decode(0, coef, scales(wy, wz, g))
+        s.set_potential(0, V)
+        s.set_gs([g])
+        s.sob_init([ALPHA], STEP)
+        solvers.append(s)
+    for s in solvers:
+        s.synchronize()
+    t0 = time.perf_counter()
+    iters = []
+    res = 0.0
+    for k, s in enumerate(solvers):
+        if k > 0:
+            s.prolong_from(solvers[k - 1])
+        it, res = s.sob_run(eps if k == len(solvers) - 1 else eps_coarse, max_iter)
+        iters.append(it)
+    solvers[-1].synchronize()
+    dt = time.perf_counter() - t0
+    mu = float(solvers[-1].sob_mu()[0])
+    psi = solvers[-1].psi(0)
+    for s in solvers:
+        s.close()
+    return psi, iters, res, dt, mu
+
+
 def generate(count: int, seed: int, n: int = 64, workers: int = 8):
     """Training set: plain-sobmin ground states of `count` draws at n^3,
     projected on their bases."""
