@@ -477,35 +477,20 @@ static int scratch_forward(atus_ctx *ctx) {
   return r;
 }
 
-// Spectral prolongation: the unscaled spectrum C of a coarse field (FP64
-// scratch of the coarse context) into the spectrum of a finer grid on the same
-// box, F(m) = C(m) / Nc for every wavenumber |m| < nc/2 on each axis (the
-// coarse Nyquist plane has no partner on the fine grid and is dropped), zero
-// elsewhere; the inverse unscaled transform on the fine grid is then the
-// trigonometric interpolant of the coarse values.
-struct ProlongArgs {
+// Embedding: a field on a smaller grid with the same spacing, centred in a
+// larger one (index offsets (nd - ns) / 2 per axis, both grids centred at
+// x = 0), zero outside.
+struct EmbedArgs {
   const double2 *src;
   double2 *dst;
-  int nc[3], nf[3];
-  double inv_nc;
-  int64_t npts_c;
+  int ns[3], nd[3], off[3];
+  int64_t npts_s;
 };
-__global__ void prolong_kernel(ProlongArgs a) {
-  for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < a.npts_c; l += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t i2 = l % a.nc[2], i1 = (l / a.nc[2]) % a.nc[1], i0 = l / ((int64_t)a.nc[2] * a.nc[1]);
-    const int64_t ic[3] = {i0, i1, i2};
-    int64_t f = 0;
-    bool keep = true;
-    for (int ax = 0; ax < 3; ax++) {
-      const int64_t n = a.nc[ax];
-      if (n > 1 && 2 * ic[ax] == n) keep = false;           // Nyquist index
-      const int64_t m = (2 * ic[ax] < n) ? ic[ax] : ic[ax] - n;  // signed wavenumber
-      f = f * a.nf[ax] + ((m + a.nf[ax]) % a.nf[ax]);
-    }
-    if (keep) {
-      const double2 c = a.src[l];
-      a.dst[f] = make_double2(c.x * a.inv_nc, c.y * a.inv_nc);
-    }
+__global__ void embed_kernel(EmbedArgs a) {
+  for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < a.npts_s; l += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i2 = l % a.ns[2], i1 = (l / a.ns[2]) % a.ns[1], i0 = l / ((int64_t)a.ns[2] * a.ns[1]);
+    const int64_t f = ((i0 + a.off[0]) * a.nd[1] + (i1 + a.off[1])) * a.nd[2] + (i2 + a.off[2]);
+    a.dst[f] = a.src[l];
   }
 }
 
@@ -844,46 +829,35 @@ int atus_ft(atus_ctx *ctx, int comp, int isign) {
   return ATUS_OK;
 }
 
-int atus_prolong(atus_ctx *coarse, int comp_c, atus_ctx *fine, int comp_f) {
-  if (!coarse || !fine || comp_c < 0 || comp_c >= coarse->ncomp || comp_f < 0 || comp_f >= fine->ncomp)
-    return ATUS_E_ARG;
-  atus_ctx *ctx = fine;
-  if (coarse->prec != ATUS_PREC_FP64 || fine->prec != ATUS_PREC_FP64)
-    return fail(fine, ATUS_E_UNSUPPORTED, "prolongation needs FP64 contexts");
-  if (coarse->dim != fine->dim) return fail(fine, ATUS_E_ARG, "grids of different dimension");
-  for (int ax = 0; ax < coarse->dim; ax++) {
-    if (fine->n[ax] < coarse->n[ax]) return fail(fine, ATUS_E_ARG, "the fine grid has fewer points");
-    const double Lc = coarse->d[ax] * coarse->n[ax], Lf = fine->d[ax] * fine->n[ax];
-    if (fabs(Lc - Lf) > 1e-12 * Lf) return fail(fine, ATUS_E_ARG, "grids on different boxes");
+int atus_embed(atus_ctx *src, int comp_s, atus_ctx *dst, int comp_d) {
+  if (!src || !dst || comp_s < 0 || comp_s >= src->ncomp || comp_d < 0 || comp_d >= dst->ncomp) return ATUS_E_ARG;
+  atus_ctx *ctx = dst;
+  if (src->prec != ATUS_PREC_FP64 || dst->prec != ATUS_PREC_FP64)
+    return fail(dst, ATUS_E_UNSUPPORTED, "embedding needs FP64 contexts");
+  if (src->dim != dst->dim) return fail(dst, ATUS_E_ARG, "grids of different dimension");
+  EmbedArgs a;
+  for (int ax = 0; ax < 3; ax++) {
+    if (dst->n[ax] < src->n[ax]) return fail(dst, ATUS_E_ARG, "the target grid has fewer points");
+    if (ax < src->dim && fabs(src->d[ax] - dst->d[ax]) > 1e-12 * dst->d[ax])
+      return fail(dst, ATUS_E_ARG, "grids of different spacing");
+    a.ns[ax] = (int)src->n[ax];
+    a.nd[ax] = (int)dst->n[ax];
+    a.off[ax] = (int)((dst->n[ax] - src->n[ax]) / 2);
   }
-  {  // coarse spectrum in the coarse context's scratch, on its stream
-    atus_ctx *c = coarse;
-    const int r1 = to_scratch(c, comp_c);
-    if (r1 != ATUS_OK) return r1;
-    const int r2 = scratch_forward(c);
-    if (r2 != ATUS_OK) return r2;
+  {  // the source field must be complete before the target stream reads it
     cudaEvent_t ev;
     CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-    CK(cudaEventRecord(ev, c->stream));
-    CK(cudaStreamWaitEvent(fine->stream, ev, 0));
+    CK(cudaEventRecord(ev, src->stream));
+    CK(cudaStreamWaitEvent(dst->stream, ev, 0));
     cudaEventDestroy(ev);
   }
-  CK(cudaMemsetAsync(fine->psi[comp_f], 0, 16 * fine->npts, fine->stream));
-  ProlongArgs a;
-  a.src = static_cast<const double2 *>(coarse->scratch);
-  a.dst = static_cast<double2 *>(fine->psi[comp_f]);
-  for (int ax = 0; ax < 3; ax++) {
-    a.nc[ax] = (int)coarse->n[ax];
-    a.nf[ax] = (int)fine->n[ax];
-  }
-  a.inv_nc = 1.0 / (double)coarse->npts;
-  a.npts_c = coarse->npts;
-  prolong_kernel<<<grid_blocks(coarse->npts, 256), 256, 0, fine->stream>>>(a);
-  LAUNCHED(fine);
-  void *f[1] = {fine->psi[comp_f]};
-  for (int ax = fine->dim - 1; ax >= 0; ax--) RUN(run_pass(fine, ax, T_INV, OP_NONE, T_NONE, nullptr, 0, f, 1));
-  // the coarse scratch is read by the fine stream: keep it until then
-  CK(cudaStreamSynchronize(fine->stream));
+  CK(cudaMemsetAsync(dst->psi[comp_d], 0, 16 * dst->npts, dst->stream));
+  a.src = static_cast<const double2 *>(src->psi[comp_s]);
+  a.dst = static_cast<double2 *>(dst->psi[comp_d]);
+  a.npts_s = src->npts;
+  embed_kernel<<<grid_blocks(src->npts, 256), 256, 0, dst->stream>>>(a);
+  LAUNCHED(dst);
+  CK(cudaStreamSynchronize(dst->stream));
   return ATUS_OK;
 }
 

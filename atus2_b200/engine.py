@@ -106,7 +106,7 @@ SIGNATURES = {
     "atus_upload_psi": (_i, [_vp, _i, _dp]),
     "atus_download_psi": (_i, [_vp, _i, _dp]),
     "atus_device_psi": (_i, [_vp, _i, C.POINTER(C.c_void_p)]),
-    "atus_prolong": (_i, [_vp, _i, _vp, _i]),
+    "atus_embed": (_i, [_vp, _i, _vp, _i]),
     "atus_ft": (_i, [_vp, _i, _i]),
     "atus_ft_step": (_i, [_vp, _i]),
     "atus_nl_step": (_i, [_vp, _i, _d]),
@@ -406,10 +406,10 @@ class Solver:
         sc = np.ascontiguousarray(scale, dtype=np.float64)
         self._ok(self._L.atus_guess_decode(self._c, comp, _dptr(c), _dptr(sc)), "guess_decode")
 
-    def prolong_from(self, coarse: "Solver", comp: int = 0, comp_coarse: int = 0) -> None:
-        """Component comp := the spectral interpolant of `coarse`'s component
-        comp_coarse (same box, at least as many points per axis, FP64)."""
-        self._ok(self._L.atus_prolong(coarse._c, int(comp_coarse), self._c, int(comp)), "prolong")
+    def embed_from(self, small: "Solver", comp: int = 0, comp_small: int = 0) -> None:
+        """Component comp := `small`'s component comp_small (same spacing,
+        fewer points) centred in this grid, zero elsewhere (FP64)."""
+        self._ok(self._L.atus_embed(small._c, int(comp_small), self._c, int(comp)), "embed")
 
     def sob_mu(self) -> np.ndarray:
         mu = np.zeros(MAX_COMP)

@@ -148,51 +148,70 @@ def solve(n, wy, wz, g, coef=None, eps=EPS, max_iter=200000):
     return psi, it, res, dt, mu
 
 
-def solve_cascade(n, wy, wz, g, coef=None, levels=None, eps=EPS, eps_coarse=None, max_iter=400000):
-    """Coarse-to-fine sobmin: the guess (Thomas-Fermi, or the learned one when
-    coef is given) on the coarsest grid of `levels` (default n/4, n/2, n, same
-    box), the descent there to eps_coarse, then the spectral interpolant of
-    each level's converged state (atus_prolong) seeds the next finer grid; the
-    finest runs to eps with the fixed step of plain sobmin.  The slow modes of
-    the fixed-step descent are smooth, global ones, which the coarse grids
-    resolve at a fraction of the cost; what the finer grids add is fine-scale
-    structure, which the Sobolev-preconditioned descent removes quickly.
-    Returns (psi, iterations per level, residual, seconds, mu); the seconds
-    cover the descents and the interpolations (the grids and potentials are
-    set up before the clock starts, as in solve())."""
-    levels = list(levels or [n // 4, n // 2, n])
-    eps_coarse = eps if eps_coarse is None else eps_coarse
-    solvers = []
-    for k, nl in enumerate(levels):
-        h = header(nl)
-        V = potential(h, wy, wz)
-        s = Solver(h, 1, PREC_FP64)
-        if k == 0:
-            if coef is None:
-                s.set_psi(0, tf_guess(h, V, g))
-            else:
-                s.guess_decode(0, coef, scales(wy, wz, g))
-        s.set_potential(0, V)
+def small_box(n: int, wy: float, wz: float, g: float, margin: float = 2.0):
+    """Points per axis of the smallest grid with the full grid's spacing that
+    holds the condensate of a draw: twice its Thomas-Fermi radius plus
+    `margin` oscillator lengths on each side, rounded up to a power of two
+    (at least 16, at most n)."""
+    mu = mu_tf(wy, wz, g)
+    dx = L_BOX / n
+    out = []
+    for w in (1.0, wy, wz):
+        half = math.sqrt(2.0 * mu) / w + margin / math.sqrt(w)
+        m = 16
+        while m < n and m * dx < 2.0 * half:
+            m *= 2
+        out.append(min(m, n))
+    return out
+
+
+def solve_learned(n, wy, wz, g, coef, eps=EPS, margin=2.0, max_iter=400000):
+    """sobmin seeded by the learned guess: the guess decoded on the small box
+    of the draw (small_box: the full grid's spacing, just large enough for the
+    condensate), the descent there to eps, the converged state embedded in
+    the full box (atus_embed), and the descent on the full box to eps from
+    there.  The slow modes of the fixed-step descent are the condensate's own
+    low modes, which the small box holds exactly at a fraction of the cost
+    per iteration; on the full box only the tails outside the small box are
+    left.  A draw whose small box is the full box runs plain sobmin from the
+    learned guess.  Returns (psi, [iterations small, full], residual, seconds,
+    mu, small-box points); the seconds cover both descents and the embedding
+    (the grids and potentials are set up before the clock starts, as in
+    solve())."""
+    ns = small_box(n, wy, wz, g, margin)
+    hf = header(n)
+    f = Solver(hf, 1, PREC_FP64)
+    f.set_potential(0, potential(hf, wy, wz))
+    f.set_gs([g])
+    f.sob_init([ALPHA], STEP)
+    s = None
+    if ns != [n, n, n]:
+        hs = binfmt.make_header(3, ns, [-0.5 * m * L_BOX / n for m in ns], [0.5 * m * L_BOX / n for m in ns])
+        s = Solver(hs, 1, PREC_FP64)
+        s.guess_decode(0, coef, scales(wy, wz, g))
+        s.set_potential(0, potential(hs, wy, wz))
         s.set_gs([g])
         s.sob_init([ALPHA], STEP)
-        solvers.append(s)
-    for s in solvers:
         s.synchronize()
+    else:
+        f.guess_decode(0, coef, scales(wy, wz, g))
+    f.synchronize()
     t0 = time.perf_counter()
-    iters = []
-    res = 0.0
-    for k, s in enumerate(solvers):
-        if k > 0:
-            s.prolong_from(solvers[k - 1])
-        it, res = s.sob_run(eps if k == len(solvers) - 1 else eps_coarse, max_iter)
-        iters.append(it)
-    solvers[-1].synchronize()
+    iters = [0]
+    if s is not None:
+        it, _ = s.sob_run(eps, max_iter)
+        iters = [it]
+        f.embed_from(s)
+    it, res = f.sob_run(eps, max_iter)
+    iters.append(it)
+    f.synchronize()
     dt = time.perf_counter() - t0
-    mu = float(solvers[-1].sob_mu()[0])
-    psi = solvers[-1].psi(0)
-    for s in solvers:
+    mu = float(f.sob_mu()[0])
+    psi = f.psi(0)
+    f.close()
+    if s is not None:
         s.close()
-    return psi, iters, res, dt, mu
+    return psi, iters, res, dt, mu, ns
 
 
 def generate(count: int, seed: int, n: int = 64, workers: int = 8):

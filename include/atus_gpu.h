@@ -45,8 +45,8 @@
  *   atus_sob_*                      CSOB_Base (include/CSOB_Base.h:96-543)
  *   atus_particle_number_noalloc    no counterpart in the reference (see its
  *                                   declaration below)
- *   atus_prolong                    no counterpart in the reference: coarse-to-fine
- *                                   seeding of the Sobolev descent
+ *   atus_embed                      no counterpart in the reference: seeding the
+ *                                   Sobolev descent from a smaller grid
  *   atus_guess_*                    no counterpart in the reference: a learned
  *                                   initial state for CSOB_Base::run (the
  *                                   reference starts from a muParser guess,
@@ -269,14 +269,12 @@ ATUS_API int atus_rabi_integrals(atus_ctx *ctx, const double *k0, int n, double 
 ATUS_API int atus_rabi_integrals_comp(atus_ctx *ctx, int comp, const double *k0, int n, double thr, double *out);
 
 /* ------------------------------------------------------------ Sobolev gradient */
-/* Spectral interpolation of component comp_c of a coarse context onto
- * component comp_f of a context with at least as many points per axis on the
- * same box (both FP64): the trigonometric interpolant of the coarse values,
- * by the coarse transform, zero padding (the coarse Nyquist plane dropped)
- * and the fine inverse transform.  No counterpart in the reference: it seeds
- * a Sobolev descent on a fine grid with the converged state of a coarser one
- * (coarse-to-fine ground states). */
-ATUS_API int atus_prolong(atus_ctx *coarse, int comp_c, atus_ctx *fine, int comp_f);
+/* Component comp_s of a context on a smaller grid with the same spacing,
+ * centred in component comp_d of a larger one (index offset (n_dst - n_src)/2
+ * per axis), zero elsewhere; both FP64.  No counterpart in the reference: it
+ * carries a ground state solved on a box that just holds the condensate into
+ * the full box, as the start of the Sobolev descent there. */
+ATUS_API int atus_embed(atus_ctx *src, int comp_s, atus_ctx *dst, int comp_d);
 /* Ground-state descent of CSOB_Base on the context's grid: alpha per
  * component (Alpha_i[0] on every axis), gs already scaled by sqrt(N_i N_j),
  * fixed stepsize.  The potential comes from atus_set_potential and the start
