@@ -19,12 +19,19 @@ Thomas-Fermi guess stays the fallback; the converged residual and chemical
 potential tell how good the learned guess was.
 
     python -m atus2_b200.guess generate --count 256 --out atus2_b200/data/sob_train_64.npz
+    python -m atus2_b200.guess evaluate --held-out 200 --seed 2 --out <file.json>
+
+The guess seeds sobmin through a small box (solve_learned): the descent runs
+first on a box with the full grid's spacing that just holds the condensate,
+from the decoded guess, and its converged state, embedded in the full box,
+starts the descent there.
 """
 from __future__ import annotations
 
 import argparse
 import ctypes as C
 import concurrent.futures as cf
+import json
 import math
 import os
 import time
@@ -148,7 +155,7 @@ def solve(n, wy, wz, g, coef=None, eps=EPS, max_iter=200000):
     return psi, it, res, dt, mu
 
 
-def small_box(n: int, wy: float, wz: float, g: float, margin: float = 2.0):
+def small_box(n: int, wy: float, wz: float, g: float, margin: float = 3.0):
     """Points per axis of the smallest grid with the full grid's spacing that
     holds the condensate of a draw: twice its Thomas-Fermi radius plus
     `margin` oscillator lengths on each side, rounded up to a power of two
@@ -165,7 +172,7 @@ def small_box(n: int, wy: float, wz: float, g: float, margin: float = 2.0):
     return out
 
 
-def solve_learned(n, wy, wz, g, coef, eps=EPS, margin=2.0, max_iter=400000):
+def solve_learned(n, wy, wz, g, coef, eps=EPS, margin=3.0, max_iter=400000):
     """sobmin seeded by the learned guess: the guess decoded on the small box
     of the draw (small_box: the full grid's spacing, just large enough for the
     condensate), the descent there to eps, the converged state embedded in
@@ -280,15 +287,52 @@ def coef_stats(coef):
     return coef.mean(axis=0), coef.std(axis=0) + 1e-12
 
 
+def evaluate(count: int, seed: int, n: int = 128, train_epochs: int = 20000):
+    """The learned guess on `count` held-out draws (seed `seed`): plain sobmin
+    from the Thomas-Fermi guess against solve_learned, both to EPS; per draw
+    iterations, seconds, mu and the particle number of the final state
+    (the reference's descent renormalises only when |N - 1| > 1e-5, so two
+    converged runs end at slightly different N and mu)."""
+    d = np.load(TRAIN_FILE)
+    m, sd = coef_stats(d["coef"])
+    params, hist = train(features(d["params"]), (d["coef"] - m) / sd, epochs=train_epochs, lr=2e-3)
+    H = draw(count, seed)
+    pred = predict(params, features(H)) * sd + m
+    rows = []
+    dv = (L_BOX / n) ** 3
+    for k, (wy, wz, g) in enumerate(H):
+        psi_p, it_p, res_p, t_p, mu_p = solve(n, wy, wz, g)
+        psi_l, it_l, res_l, t_l, mu_l, ns = solve_learned(n, wy, wz, g, pred[k])
+        rows.append(dict(w_y=float(wy), w_z=float(wz), g=float(g), iters_plain=int(it_p), s_plain=t_p, mu_plain=mu_p,
+                         N_plain=float(dv * np.vdot(psi_p, psi_p).real), iters_learned=[int(i) for i in it_l],
+                         s_learned=t_l, mu_learned=mu_l, N_learned=float(dv * np.vdot(psi_l, psi_l).real),
+                         small_box=ns, speedup=t_p / t_l, dmu=abs(mu_l - mu_p),
+                         rel_l2=float(np.linalg.norm(psi_l - psi_p) / np.linalg.norm(psi_p))))
+        print(json.dumps(rows[-1]), flush=True)
+    sp = np.array([r["speedup"] for r in rows])
+    return dict(count=count, seed=seed, n=n, rows=rows, mean_speedup=float(sp.mean()),
+                total_speedup=float(sum(r["s_plain"] for r in rows) / sum(r["s_learned"] for r in rows)),
+                min_speedup=float(sp.min()), frac_ge_3=float((sp >= 3).mean()),
+                max_dmu=float(max(r["dmu"] for r in rows)), training_loss=[float(hist[0]), float(hist[-1])])
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("cmd", choices=["generate"])
+    ap.add_argument("cmd", choices=["generate", "evaluate"])
     ap.add_argument("--count", type=int, default=256)
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--n", type=int, default=64)
     ap.add_argument("--workers", type=int, default=8)
     ap.add_argument("--out", default=TRAIN_FILE)
+    ap.add_argument("--held-out", type=int, default=200, help="evaluate: number of held-out draws (seed --seed)")
     a = ap.parse_args()
+    if a.cmd == "evaluate":
+        out = evaluate(a.held_out, a.seed)
+        with open(a.out, "w") as f:
+            json.dump(out, f)
+        print(f"{a.held_out} draws: mean speed-up {out['mean_speedup']:.2f}, total {out['total_speedup']:.2f}, "
+              f"min {out['min_speedup']:.2f}, >= 3x for {100 * out['frac_ge_3']:.0f} %, max |dmu| {out['max_dmu']:.2e}")
+        return
     t0 = time.perf_counter()
     d = generate(a.count, a.seed, a.n, a.workers)
     os.makedirs(os.path.dirname(a.out), exist_ok=True)
