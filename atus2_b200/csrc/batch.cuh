@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(Tile2<R>::NT, Tile2<R>::MINB) batch_pass2_kern
       setup = true;
       __syncthreads();  // twiddle rows visible to every warp before the first exchange
     }
-    p2_item<R, N, TC, MODE, STRIDED, false>(sa, tile_geo<Cfg::B, N>(sa, w % bp.items), smem_raw, false, s_om, s_ec,
+    p2_item<R, N, TC, MODE, STRIDED>(sa, tile_geo<Cfg::B, N>(sa, w % bp.items), smem_raw, false, s_om, s_ec,
                                             s_es);
     __syncthreads();  // sa is rewritten by the next item
   }
@@ -257,7 +257,7 @@ __global__ void __launch_bounds__(P5Cfg<R, TC>::NT, 4) batch_pass512_kernel(BPas
       p5_setup<R, TC>(sa, smem_raw);
       setup = true;
     }
-    p5_item<R, TC, MODE, STRIDED, false>(sa, tile_geo<Cfg::B, 512>(sa, w % bp.items), smem_raw, s_om, s_ec, s_es);
+    p5_item<R, TC, MODE, STRIDED>(sa, tile_geo<Cfg::B, 512>(sa, w % bp.items), smem_raw, s_om, s_ec, s_es);
     __syncthreads();
   }
 }

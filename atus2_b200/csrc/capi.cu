@@ -210,38 +210,9 @@ static int run_pass(atus_ctx *ctx, int axis, int t1, int op, int t2, const NLArg
     if (_r != ATUS_OK) return _r; \
   } while (0)
 
-// One cluster slab pass over the context's fields (3D); ATUS_E_UNSUPPORTED
-// when the grid has no slab kernel, after which the axis passes are used.
-static int slab_pass(atus_ctx *ctx, int load_rows, int inv_y, int inv_z, const NLArgs *nl, int fwd_z, int fwd_y,
-                     int store_rows) {
-  if (!ctx->use_slab || ctx->dim != 3 || ctx->ncomp > 2) return ATUS_E_UNSUPPORTED;
-  SlabArgs a;
-  memset(&a, 0, sizeof(a));
-  for (int c = 0; c < MAXC; c++) a.psi[c] = ctx->psi[c];
-  a.nc = ctx->ncomp;
-  a.load_rows = load_rows;
-  a.inv_y = inv_y;
-  a.inv_z = inv_z;
-  a.fwd_z = fwd_z;
-  a.fwd_y = fwd_y;
-  a.store_rows = store_rows;
-  if (nl) {
-    a.nl = *nl;
-    a.do_nl = 1;
-  }
-  const int tc = tc_for(ctx->ncomp);
-  const int r = (ctx->prec == ATUS_PREC_FP64) ? launch_slab_d(ctx, a, tc) : launch_slab_f(ctx, a, tc);
-  if (r == ATUS_E_UNSUPPORTED) ctx->use_slab = false;
-  return r;
-}
-
 // Forward (dir -1) or inverse (+1) transform of the axes other than 0.
 static int transform_inner(atus_ctx *ctx, int dir, void *const *f = nullptr, int nf = -1) {
   if (ctx->dim == 2) return run_pass(ctx, 1, dir, OP_NONE, T_NONE, nullptr, 0, f, nf);
-  if (ctx->dim == 3 && f == nullptr) {
-    const int r = (dir == T_FWD) ? slab_pass(ctx, 1, 0, 0, nullptr, 1, 1, 0) : slab_pass(ctx, 0, 1, 1, nullptr, 0, 0, 1);
-    if (r != ATUS_E_UNSUPPORTED) return r;
-  }
   if (ctx->dim == 3) {
     if (dir == T_FWD) {
       RUN(run_pass(ctx, 2, T_FWD, OP_NONE, T_NONE, nullptr, 0, f, nf));
@@ -309,98 +280,8 @@ static int kinetic_pass_rabi(atus_ctx *ctx, int half, const RabiReq &rr, double 
   return ATUS_OK;
 }
 
-// Arguments of one pass over the context's fields, with the geometry the
-// launchers fill in (the plane pipeline takes three of them as they are).
-static PassArgs pass_args(const atus_ctx *ctx, int axis, int t1, int op, int t2, const NLArgs *nl) {
-  PassArgs a;
-  memset(&a, 0, sizeof(a));
-  for (int c = 0; c < MAXC; c++) a.psi[c] = (c < ctx->ncomp) ? ctx->psi[c] : nullptr;
-  a.t1 = t1;
-  a.op = op;
-  a.t2 = t2;
-  a.per_comp = (op != OP_NL) ? 1 : 0;
-  a.nc = (op == OP_NL) ? ctx->ncomp : 1;
-  a.s_f = scale_fak(ctx->dim, ctx->d);
-  a.s_b = scale_fak(ctx->dim, ctx->dk);
-  if (nl) a.nl = *nl;
-  int64_t sa = 1;
-  for (int b = axis + 1; b < 3; b++) sa *= ctx->n[b];
-  a.sa = sa;
-  a.x_along = (axis == 0);
-  a.axis = axis;
-  a.g = geo(ctx);
-  a.tw = (ctx->prec == ATUS_PREC_FP64) ? ctx->tw64 : ctx->tw;
-  for (int ax = 0; ax < 3; ax++) {
-    a.dk[ax] = ctx->dk[ax];
-    a.n[ax] = (int)ctx->n[ax];
-  }
-  a.ncomp_grid = ctx->ncomp;
-  return a;
-}
-
-// 3D real-space half step as one plane pipeline (pipe.cuh):
-// IFFT_y, IFFT_z -> potential -> FFT_z, FFT_y with the planes in flight held
-// in L2.  ATUS_E_UNSUPPORTED when the grid has no pipeline instantiation.
-static int pipe_pass(atus_ctx *ctx, const NLArgs &nl) {
-  if (!ctx->use_pipe || ctx->dim != 3 || ctx->ncomp > 2 || ctx->n[0] > PIPE_MAX_PLANES) return ATUS_E_UNSUPPORTED;
-  // complex64 fields: the three separate passes measured faster on B200
-  if (ctx->prec != ATUS_PREC_FP64 && !ctx->pipe_mixed) return ATUS_E_UNSUPPORTED;
-  if (ctx->n[1] != ctx->n[2] || ctx->n[1] < 32 || ctx->n[1] > 256) return ATUS_E_UNSUPPORTED;
-  if (!ctx->pipe) {
-    CK(cudaMalloc(&ctx->pipe, sizeof(PipeQueue)));
-    CK(cudaMemsetAsync(ctx->pipe, 0, sizeof(PipeQueue), ctx->stream));
-    ctx->pipe_epoch = 0;
-  }
-  if (ctx->pipe_epoch >= (1u << 20)) {  // keep epoch * items below 2^32
-    CK(cudaMemsetAsync(ctx->pipe, 0, sizeof(PipeQueue), ctx->stream));
-    ctx->pipe_epoch = 0;
-  }
-  PipeArgs a;
-  memset(&a, 0, sizeof(a));
-  a.pa = pass_args(ctx, 1, T_INV, OP_NONE, T_NONE, nullptr);
-  a.pb = pass_args(ctx, 2, T_INV, OP_NL, T_FWD, &nl);
-  a.pc = pass_args(ctx, 1, T_FWD, OP_NONE, T_NONE, nullptr);
-  a.q = ctx->pipe;
-  a.epoch = ctx->pipe_epoch + 1;
-  a.P = (int)ctx->n[0];
-  a.n1 = (int)ctx->n[1];
-  a.n2 = (int)ctx->n[2];
-  const int tc = tc_for(ctx->ncomp);
-  const int r = (ctx->prec == ATUS_PREC_FP64) ? launch_pipe_d(ctx, a, tc) : launch_pipe_f(ctx, a, tc);
-  if (r == ATUS_OK) {
-    ctx->pipe_epoch++;
-    ctx->pipe_pending = true;
-  }
-  return r;
-}
-
-// Reads the pipeline's error flag after the launches of a call (one small
-// copy and a stream synchronisation); a wait that gave up is a CUDA error.
-static int pipe_check(atus_ctx *ctx) {
-  if (!ctx->pipe_pending) return ATUS_OK;
-  ctx->pipe_pending = false;
-  unsigned *h = reinterpret_cast<unsigned *>(ctx->h_red);
-  CK(cudaMemcpyAsync(h, &ctx->pipe->err, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
-  if (*h != 0) {
-    CK(cudaMemsetAsync(ctx->pipe, 0, sizeof(PipeQueue), ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    ctx->pipe_epoch = 0;
-    return fail(ctx, ATUS_E_CUDA, "plane pipeline: a wait for another tile's results gave up");
-  }
-  return ATUS_OK;
-}
-
 // Real-space potential pass: 2D one pass over rows; 3D inverse y, rows, forward y.
 static int potential_pass(atus_ctx *ctx, const NLArgs &nl) {
-  if (ctx->dim == 3) {
-    const int r = slab_pass(ctx, 0, 1, 1, &nl, 1, 1, 0);
-    if (r != ATUS_E_UNSUPPORTED) return r;
-  }
-  if (ctx->dim == 3) {
-    const int r = pipe_pass(ctx, nl);
-    if (r != ATUS_E_UNSUPPORTED) return r;
-  }
   const int last = ctx->dim - 1;
   if (ctx->dim == 3) RUN(run_pass(ctx, 1, T_INV, OP_NONE, T_NONE, nullptr, 0));
   RUN(run_pass(ctx, last, T_INV, OP_NL, T_FWD, &nl, 0));
@@ -538,21 +419,9 @@ int atus_create(const atus_grid *grid, int ncomp, int precision, atus_ctx **out)
   else { ctx->ar = ctx->d[0] * ctx->d[1] * ctx->d[2]; ctx->ar_k = ctx->dk[0] * ctx->dk[1] * ctx->dk[2]; }
   ctx->t = grid->t;
   {
-    // ATUS_SLAB=1: 3D real-space passes as one cluster slab pass instead of
-    // three axis passes (measured slower on B200 so far; kept for A/B runs)
-    const char *e = getenv("ATUS_SLAB");
-    ctx->use_slab = (e && e[0] == '1');
     // ATUS_PASS2=0: tile kernel only (A/B comparisons of the two pass kernels)
     const char *p2 = getenv("ATUS_PASS2");
     ctx->use_pass2 = !(p2 && p2[0] == '0');
-    // ATUS_PIPE=1: 3D real-space half step as one plane pipeline (both
-    // precisions) instead of three axis passes.  Since the strided passes
-    // prefetch their next tile into L2 the three passes are faster on B200
-    // (FP64 256^3 Bragg: 1.159 against 1.181 ms per step on one box), so the
-    // pipeline is kept for A/B runs only.
-    const char *pp = getenv("ATUS_PIPE");
-    ctx->use_pipe = ctx->use_pass2 && (pp && pp[0] == '1');
-    ctx->pipe_mixed = ctx->use_pipe;
   }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) { delete ctx; return ATUS_E_CUDA; }
@@ -623,7 +492,6 @@ void atus_destroy(atus_ctx *ctx) {
   if (ctx->snap_read) cudaEventDestroy(ctx->snap_read);
   if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
   cudaFree(ctx->scratch);
-  cudaFree(ctx->pipe);
   cudaFree(ctx->sob_dev);
   if (ctx->sob_graph) cudaGraphExecDestroy(ctx->sob_graph);
   if (ctx->h_sob) cudaFreeHost(ctx->h_sob);
@@ -1015,8 +883,7 @@ static int strang_block(atus_ctx *ctx, int nk, int kind, const double *F, const 
     RUN(r);
     ctx->t += last ? 0.5 * dt : dt;
   }
-  RUN(transform_inner(ctx, T_INV));
-  return pipe_check(ctx);
+  return transform_inner(ctx, T_INV);
 }
 
 int atus_profile_passes(atus_ctx *ctx, int kind, int reps, double *ms, double *lps, double *bytes, int *npass) {
@@ -1056,40 +923,15 @@ int atus_profile_passes(atus_ctx *ctx, int kind, int reps, double *ms, double *l
     auto kin = [&]() { return kinetic_pass(ctx, 0); };
     r = timed(kin, 1.0, fb);
     const int last = ctx->dim - 1;
-    bool slab_done = false;
-    if (r == ATUS_OK && ctx->dim == 3) {  // the fused (y,z) cluster pass, when the grid has one
-      const int probe = slab_pass(ctx, 0, 1, 1, &nl, 1, 1, 0);
-      if (probe == ATUS_OK) {
-        auto slab = [&]() { return slab_pass(ctx, 0, 1, 1, &nl, 1, 1, 0); };
-        r = timed(slab, 1.0, fb + vb);
-        slab_done = true;
-      } else if (probe != ATUS_E_UNSUPPORTED) {
-        r = probe;
-      }
-    }
-    if (!slab_done && r == ATUS_OK && ctx->dim == 3) {  // the plane pipeline, when the grid has one
-      const int probe = pipe_pass(ctx, nl);
-      if (probe == ATUS_OK) {
-        r = pipe_check(ctx);
-        auto pipe = [&]() { return pipe_pass(ctx, nl); };
-        if (r == ATUS_OK) r = timed(pipe, 1.0, fb + vb);
-        if (r == ATUS_OK) r = pipe_check(ctx);
-        slab_done = true;
-      } else if (probe != ATUS_E_UNSUPPORTED) {
-        r = probe;
-      }
-    }
-    if (slab_done) {
-      // one fused launch replaces the three axis passes below
-    } else if (r == ATUS_OK && ctx->dim == 3) {
+    if (r == ATUS_OK && ctx->dim == 3) {
       auto yinv = [&]() { return run_pass(ctx, 1, T_INV, OP_NONE, T_NONE, nullptr, 0); };
       r = timed(yinv, 1.0, fb);
     }
-    if (r == ATUS_OK && !slab_done) {
+    if (r == ATUS_OK) {
       auto pot = [&]() { return run_pass(ctx, last, T_INV, OP_NL, T_FWD, &nl, 0); };
       r = timed(pot, 1.0, fb + vb);
     }
-    if (r == ATUS_OK && ctx->dim == 3 && !slab_done) {
+    if (r == ATUS_OK && ctx->dim == 3) {
       auto yfwd = [&]() { return run_pass(ctx, 1, T_FWD, OP_NONE, T_NONE, nullptr, 0); };
       r = timed(yfwd, 1.0, fb);
     }

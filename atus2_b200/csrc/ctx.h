@@ -8,7 +8,6 @@
 #include "../../include/atus_gpu.h"
 #include "kernels.cuh"
 
-namespace atus { struct PipeQueue; }
 using namespace atus;
 
 struct atus_ctx {
@@ -34,13 +33,7 @@ struct atus_ctx {
   double *red_partial = nullptr, *red_out = nullptr, *h_red = nullptr;
   cudaStream_t own_stream = nullptr, stream = nullptr;
   int64_t launches = 0;
-  bool use_slab = true;         // 3D: fused (y,z) cluster pass when available
   bool use_pass2 = true;        // register-staged passes for pencils of 32..256 points
-  bool use_pipe = false;        // 3D: real-space half step as one plane pipeline (ATUS_PIPE=1)
-  bool pipe_mixed = false;      // ... also for complex64 fields
-  PipeQueue *pipe = nullptr;    // its device-resident work queue
-  unsigned pipe_epoch = 0;      // pipeline launches since the queue was zeroed
-  bool pipe_pending = false;    // a launch whose error flag is not read yet
   int bragg_stable = 0;         // FP64 Bragg step in the eigenvalue-free form
   std::string err;
   // Sobolev state

@@ -3,7 +3,7 @@
 // combination, so the kernels compile in parallel.
 #pragma once
 #include "ctx.h"
-#include "pipe.cuh"
+#include "pass2.cuh"
 
 template <typename R, int N, int TC>
 static inline int launch_pass_t(atus_ctx *ctx, PassArgs &a, int axis) {
@@ -175,47 +175,3 @@ static inline int launch_pass2_n(atus_ctx *ctx, PassArgs &a, int axis) {
   }
 }
 
-// ------------------------------------------------------------ plane pipeline
-template <typename R, int N, int TC>
-static inline int launch_pipe_t(atus_ctx *ctx, PipeArgs &a) {
-  using CT = P2Cfg<R, N, 1>;
-  using CZ = P2Cfg<R, N, TC>;
-  constexpr size_t smem = PipeCfg<R, N, TC>::smem;
-  static int resident = 0;
-  static int nsm = 0;
-  if (!resident) {
-    CK(cudaFuncSetAttribute(pipe_kernel<R, N, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    CK(cudaFuncSetAttribute(pipe_kernel<R, N, TC>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                            cudaSharedmemCarveoutMaxShared));
-    int dev = 0;
-    CK(cudaGetDevice(&dev));
-    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, pipe_kernel<R, N, TC>, CT::NT, smem));
-    if (resident < 1) return fail(ctx, ATUS_E_UNSUPPORTED, "pipeline kernel does not fit on an SM");
-  }
-  const int grid = nsm * resident;
-  a.tpcA = (a.n2 + CT::B - 1) / CT::B;
-  a.nA = a.tpcA * ctx->ncomp;
-  a.nB = (a.n1 + CZ::B - 1) / CZ::B;
-  const int per_slot = 2 * a.nA + a.nB;
-  // lag: the IFFT_y items of a plane are handed out at least one full grid of
-  // items before its z items
-  a.L = (grid + per_slot - 1) / per_slot + 1;
-  a.total = (long long)(a.P + 2 * a.L) * per_slot;
-  CK(cudaMemsetAsync(&a.q->next, 0, sizeof(unsigned long long), ctx->stream));
-  pipe_kernel<R, N, TC><<<grid, CT::NT, smem, ctx->stream>>>(a);
-  LAUNCHED(ctx);
-  return ATUS_OK;
-}
-
-template <typename R, int TC>
-static inline int launch_pipe_n(atus_ctx *ctx, PipeArgs &a) {
-  if (a.n1 != a.n2) return ATUS_E_UNSUPPORTED;
-  switch (a.n1) {
-    case 32: return launch_pipe_t<R, 32, TC>(ctx, a);
-    case 64: return launch_pipe_t<R, 64, TC>(ctx, a);
-    case 128: return launch_pipe_t<R, 128, TC>(ctx, a);
-    case 256: return launch_pipe_t<R, 256, TC>(ctx, a);
-    default: return ATUS_E_UNSUPPORTED;
-  }
-}

@@ -1,8 +1,7 @@
 // launch.h -- exported launchers, one per precision and tile component count.
 #pragma once
 #include "ctx.h"
-#include "pipe.cuh"
-#include "slab.cuh"
+#include "pass2.cuh"
 
 int launch_pass_d1(atus_ctx *ctx, PassArgs &a, int axis);
 int launch_pass_d2(atus_ctx *ctx, PassArgs &a, int axis);
@@ -28,12 +27,3 @@ int launch_pass2_d_kr(atus_ctx *ctx, PassArgs &a, int axis);
 int launch_pass2_f_kr(atus_ctx *ctx, PassArgs &a, int axis);
 int launch_pass2_d_nl(atus_ctx *ctx, PassArgs &a, int axis, int tc);
 int launch_pass2_f_nl(atus_ctx *ctx, PassArgs &a, int axis, int tc);
-// Plane pipeline of the 3D real-space half step (pipe.cuh) for n1 == n2 in
-// 32..256 and tc = 1 or 2; fills the item counts and lag of a, zeroes the
-// queue counter and launches.  ATUS_E_UNSUPPORTED when it does not apply.
-int launch_pipe_d(atus_ctx *ctx, atus::PipeArgs &a, int tc);
-int launch_pipe_f(atus_ctx *ctx, atus::PipeArgs &a, int tc);
-// Returns ATUS_E_UNSUPPORTED (without touching the fields) when the grid has
-// no slab instantiation or the cluster cannot be scheduled.
-int launch_slab_d(atus_ctx *ctx, atus::SlabArgs &a, int tc);
-int launch_slab_f(atus_ctx *ctx, atus::SlabArgs &a, int tc);

@@ -125,9 +125,7 @@ __device__ __forceinline__ bool p2_setup(const PassArgs &a, unsigned char *smem_
   return kt_shared;
 }
 
-// One work item: the tile g of the pass described by a.  Field loads go
-// through L2 only (ld.global.cg) when L2LOAD is set -- the fused plane
-// pipeline reads data that other CTAs of the same launch wrote.
+// One work item: the tile g of the pass described by a.
 // Rabi sums of one thread's 16 values (k-space points j + R2 m of the pencil
 // whose point 0 has axis indices p0) into rq, with the ball rule of
 // compute_rabi_integrals (include/CRT_Base_IF.h:231-257): a point inside a
@@ -164,7 +162,7 @@ __device__ __forceinline__ void p2_rabi(const PassArgs &a, int ci, const int *p0
   }
 }
 
-template <typename R, int N, int TC, int MODE, bool STRIDED, bool L2LOAD>
+template <typename R, int N, int TC, int MODE, bool STRIDED>
 __device__ __forceinline__ void p2_item(const PassArgs &a, const TileGeo &g, unsigned char *smem_raw, bool kt_shared,
                                         double *s_om, double *s_ec, double *s_es, double *rq = nullptr) {
   using C = cplx<R>;
@@ -205,7 +203,7 @@ __device__ __forceinline__ void p2_item(const PassArgs &a, const TileGeo &g, uns
 
   C v[16];
   #pragma unroll
-  for (int r = 0; r < 16; r++) v[r] = live ? (L2LOAD ? __ldcg(&src[r * step]) : src[r * step]) : mk<R>(0, 0);
+  for (int r = 0; r < 16; r++) v[r] = live ? src[r * step] : mk<R>(0, 0);
 
   if constexpr (MODE == M2_FWD) {
     p2_transform<R, N, -1, !STRIDED>(v, my, twS, j);
@@ -344,7 +342,7 @@ __device__ __forceinline__ void p2_item(const PassArgs &a, const TileGeo &g, uns
 // Strided tiles: asks L2 for the CTA's next tile (one prefetch per 128-byte
 // line; the B pencils of a row are adjacent, the N rows sa apart) while this
 // one is transformed, so that its loads wait on L2 rather than HBM.  (The
-// same for contiguous tiles and for the plane pipeline measured slower.)
+// same for contiguous tiles measured slower.)
 template <typename R, int N, int TC>
 __device__ __forceinline__ void p2_prefetch_l2(const PassArgs &a, const TileGeo &g) {
   using Cfg = P2Cfg<R, N, TC>;
@@ -374,7 +372,7 @@ __global__ void __launch_bounds__(Tile2<R>::NT, Tile2<R>::MINB) pass2_kernel(Pas
   for (int q = 0; q < (MODE == M2_KIN_RABI ? RED_MAXQ : 1); q++) rq[q] = 0.0;
   for (int64_t w = blockIdx.x; w < W; w += gridDim.x) {
     if (STRIDED && w + gridDim.x < W) p2_prefetch_l2<R, N, TC>(a, tile_geo<Cfg::B, N>(a, w + gridDim.x));
-    p2_item<R, N, TC, MODE, STRIDED, false>(a, tile_geo<Cfg::B, N>(a, w), smem_raw, kt_shared, s_om, s_ec, s_es, rq);
+    p2_item<R, N, TC, MODE, STRIDED>(a, tile_geo<Cfg::B, N>(a, w), smem_raw, kt_shared, s_om, s_ec, s_es, rq);
   }
   if constexpr (MODE == M2_KIN_RABI) {
     // per-CTA sums in a fixed tree (the tiles of a CTA are fixed by the grid

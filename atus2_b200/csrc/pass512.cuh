@@ -117,7 +117,7 @@ __device__ __forceinline__ void p5_setup(const PassArgs &a, unsigned char *smem_
 }
 
 // One work item (tile g) of a pass over 512-point pencils; as p2_item.
-template <typename R, int TC, int MODE, bool STRIDED, bool L2LOAD>
+template <typename R, int TC, int MODE, bool STRIDED>
 __device__ __forceinline__ void p5_item(const PassArgs &a, const TileGeo &g, unsigned char *smem_raw, double *s_om,
                                         double *s_ec, double *s_es) {
   using C = cplx<R>;
@@ -154,7 +154,7 @@ __device__ __forceinline__ void p5_item(const PassArgs &a, const TileGeo &g, uns
 
   C v[32];
   #pragma unroll
-  for (int m = 0; m < 32; m++) v[m] = live ? (L2LOAD ? __ldcg(&src[m * step]) : src[m * step]) : mk<R>(0, 0);
+  for (int m = 0; m < 32; m++) v[m] = live ? src[m * step] : mk<R>(0, 0);
 
   if constexpr (MODE == M2_FWD) {
     p5_transform<R, -1>(v, my, twS, j);
