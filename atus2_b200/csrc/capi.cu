@@ -569,6 +569,62 @@ int atus_set_gs(atus_ctx *ctx, const double *gs) {
   return ATUS_OK;
 }
 
+int atus_clone(const atus_ctx *src, atus_ctx **out) {
+  if (!src || !out) return ATUS_E_ARG;
+  *out = nullptr;
+  atus_grid g{};
+  g.dim = src->dim;
+  for (int ax = 0; ax < 3; ax++) {
+    g.n[ax] = src->n[ax];
+    g.d[ax] = src->d[ax];
+    g.dk[ax] = src->dk[ax];
+  }
+  g.t = src->t;
+  atus_ctx *ctx = nullptr;
+  const int r = atus_create(&g, src->ncomp, src->prec, &ctx);
+  if (r != ATUS_OK) return r;
+  // the source's work must be complete before its buffers are read
+  if (cudaStreamSynchronize(src->stream) != cudaSuccess) {
+    atus_destroy(ctx);
+    return ATUS_E_CUDA;
+  }
+  ctx->t = src->t;
+  ctx->dt = src->dt;
+  memcpy(ctx->alpha, src->alpha, sizeof(ctx->alpha));
+  memcpy(ctx->gs, src->gs, sizeof(ctx->gs));
+  ctx->laser = src->laser;
+  ctx->laser2 = src->laser2;
+  ctx->win_t0 = src->win_t0;
+  ctx->win_dur[0] = src->win_dur[0];
+  ctx->win_dur[1] = src->win_dur[1];
+  ctx->bragg_stable = src->bragg_stable;
+  ctx->use_pass2 = src->use_pass2;
+  int e = ATUS_OK;
+  auto copy = [&](void *dst, const void *from, size_t bytes) {
+    if (e == ATUS_OK && cudaMemcpyAsync(dst, from, bytes, cudaMemcpyDeviceToDevice, ctx->stream) != cudaSuccess)
+      e = fail(ctx, ATUS_E_CUDA, "clone copy");
+  };
+  for (int c = 0; c < src->ncomp; c++) {
+    copy(ctx->psi[c], src->psi[c], src->csize * src->npts);
+    if (src->V[c]) {
+      if (cudaMalloc(&ctx->V[c], sizeof(double) * src->npts) != cudaSuccess) e = ATUS_E_NOMEM;
+      else copy(ctx->V[c], src->V[c], sizeof(double) * src->npts);
+    }
+    // the kinetic phases as the source holds them (built for its dt and the
+    // alpha it had then)
+    for (int hf = 0; hf < 2; hf++)
+      for (int ax = 0; ax < 3; ax++)
+        if (src->kt[hf][c][ax]) copy(ctx->kt[hf][c][ax], src->kt[hf][c][ax], sizeof(double2) * src->n[ax]);
+  }
+  if (e == ATUS_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess) e = ATUS_E_CUDA;
+  if (e != ATUS_OK) {
+    atus_destroy(ctx);
+    return e;
+  }
+  *out = ctx;
+  return ATUS_OK;
+}
+
 int atus_set_potential(atus_ctx *ctx, int comp, const double *V) {
   if (!ctx || comp < 0 || comp >= ctx->ncomp) return ATUS_E_ARG;
   if (!V) {

@@ -18,7 +18,9 @@
 #include <cmath>
 #include <cstring>
 #include <list>
+#include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "CRT_Base.h"
@@ -73,6 +75,10 @@ class CRT_Base_IF : public CRT_Base<T, dim, no_int_states> {
   // ---- GPU side
   void upload_step_parameters(const sequence_item &) override { upload_laser(); }
   void upload_laser() {
+    const atus_laser L = make_laser();
+    atus_check(this->m_gpu, atus_set_laser(this->m_gpu, &L), "set_laser");
+  }
+  atus_laser make_laser() const {
     atus_laser L{};
     for (int i = 0; i < dim; i++) L.beta[i] = beta[i];
     for (int i = 0; i < no_int_states; i++) L.DeltaL[i] = DeltaL[i];
@@ -85,7 +91,7 @@ class CRT_Base_IF : public CRT_Base<T, dim, no_int_states> {
       L.chirp_rate[i] = chirp_rate[i];
     }
     L.chirp = chirp;
-    atus_check(this->m_gpu, atus_set_laser(this->m_gpu, &L), "set_laser");
+    return L;
   }
   // AMP_T at t + dt/2 of every potential step of the coming block, with the
   // header-time additions of the block (include/CRT_Base_IF.h:170-198)
@@ -105,6 +111,108 @@ class CRT_Base_IF : public CRT_Base<T, dim, no_int_states> {
       t += dt;
     }
   }
+  // ---- phase scans side by side
+  // One scan s >= 1 of a phase scan (chirp_mode 1) on its own clone of the
+  // sequence's start state: Na fused blocks with the scan's laser, the
+  // per-block and per-scan observables of run_sequence, its Rabi file; the
+  // console lines go to `text` (printed in scan order by the caller) and the
+  // scan's entry of the chirp list to `entry`.
+  struct ScanJob {
+    atus_ctx *ctx = nullptr;
+    atus_laser laser{};
+    int s = 0, kind = 0, Na = 0, Nk = 0, seq_counter = 0;
+    const std::vector<std::vector<double>> *F = nullptr;
+    std::vector<double> k0;
+    int nrm = 0;
+    double thr = 0, dt = 0, phase = 0;
+    int rabi_freq = 0, pn_freq = 0;
+    std::string rabi_header;
+    std::string text;
+    list<double> entry;
+    int err = 0;
+    std::string errmsg;
+  };
+  static void run_scan(ScanJob *j) {
+    std::ostringstream out;
+    list<list<double>> rabi;
+    auto fail = [&](int r) {
+      j->err = r;
+      j->errmsg = atus_last_error(j->ctx);
+    };
+    auto sums = [&](std::vector<double> &v) {
+      v.assign(j->nrm, 0.0);
+      const int r = atus_rabi_integrals(j->ctx, j->k0.data(), j->nrm, j->thr, v.data());
+      if (r != ATUS_OK) fail(r);
+    };
+    int r = atus_set_laser(j->ctx, &j->laser);
+    if (r != ATUS_OK) return fail(r);
+    for (int i = 0; i < j->Na && !j->err; i++) {
+      const double *F = (*j->F)[i].data();
+      if (j->rabi_freq == freq::each && j->nrm > 0) {
+        std::vector<double> v(j->nrm);
+        const int c0 = 0;
+        r = atus_strang_block_rabi(j->ctx, j->Nk, j->kind, F, 1, &c0, j->k0.data(), j->nrm, j->thr, v.data());
+        if (r != ATUS_OK) return fail(r);
+        rabi.push_back(list<double>(v.begin(), v.end()));
+      } else {
+        r = atus_strang_block(j->ctx, j->Nk, j->kind, F);
+        if (r != ATUS_OK) return fail(r);
+      }
+      double t = 0;
+      atus_get_time(j->ctx, &t);
+      out << "t = " << to_string(t) << std::endl;
+      if (j->pn_freq == freq::each)
+        for (int c = 0; c < no_int_states; c++) {
+          double n = 0;
+          atus_particle_number(j->ctx, c, &n);
+          out << "N[" << c << "] = " << n << std::endl;
+        }
+      if (j->rabi_freq == freq::each && j->nrm == 0)
+        std::cerr << "WARNING: Rabi momentum list is empty. Cannot compute rabi frquencies." << endl;
+    }
+    if (j->err) return;
+    double t_end = 0;
+    atus_get_time(j->ctx, &t_end);
+    if (j->pn_freq == freq::last)
+      for (int c = 0; c < no_int_states; c++) {
+        double n = 0;
+        atus_particle_number(j->ctx, c, &n);
+        out << "N[" << c << "] = " << n << std::endl;
+      }
+    if (j->rabi_freq == freq::last && j->nrm > 0) {
+      std::vector<double> v;
+      sums(v);
+      rabi.push_back(list<double>(v.begin(), v.end()));
+      out << "Rabi output for timestep ";
+      for (auto &row : rabi) {
+        out << t_end << "\n";
+        for (double x : row) out << x << "\t";
+        out << endl;
+      }
+    }
+    if (j->rabi_freq == freq::each) {
+      char filename[1024];
+      snprintf(filename, sizeof filename, "Rabi_%d_%d.txt", j->seq_counter, j->s);
+      ofstream txt(filename);
+      double t = 0;
+      txt << j->rabi_header << endl;
+      for (auto &row : rabi) {
+        txt << t << "\t";
+        for (double x : row) txt << x << "\t";
+        txt << endl;
+        t += j->dt * double(j->Nk);
+      }
+    }
+    if (j->nrm > 0) {
+      std::vector<double> v;
+      sums(v);
+      j->entry = list<double>(v.begin(), v.end());
+      j->entry.push_front(j->phase);
+      j->entry.push_front(j->s);
+    }
+    j->text = out.str();
+  }
+
   // one potential step of GPU kind `kind` at the current header time
   void gpu_potential_step(int kind) {
     upload_laser();
@@ -317,7 +425,64 @@ void CRT_Base_IF<T, dim, no_int_states>::run_sequence() {
     } else {
       dw[0] = 0;
     }
-    for (int s = 0; s < seq.no_of_chirps; ++s) {
+    // A phase scan (chirp_mode 1) has independent scans: each starts from this
+    // state, with phase s 2 pi / n and chirp rates that do not depend on the
+    // results (dw[s + 1] = (dw[s] + dw[s - 1]) / 2; the swap on dphi only
+    // applies to the chirp scan).  Where the blocks run fused on the GPU and
+    // no custom function touches the solver, scans 1..n-1 run side by side on
+    // clones of the context while scan 0 runs here with all its outputs.
+    const int gkind = this->gpu_kind(seq.name);
+    const bool side = seq.no_of_chirps > 1 && seq.chirp_mode == 1 && gkind >= 0 &&
+                      half_fct == &CRT_Base<T, dim, no_int_states>::Do_FT_Step_half_Wrapper &&
+                      full_fct == &CRT_Base<T, dim, no_int_states>::Do_FT_Step_full_Wrapper &&
+                      m_custom_fct == nullptr && !std::getenv("ATUS_SEQUENTIAL_SCANS");
+    std::vector<ScanJob> jobs;
+    std::vector<std::thread> workers;
+    std::vector<std::vector<double>> Fs;
+    if (side) {
+      for (int s = 1; s + 1 < seq.no_of_chirps; s++) dw[s + 1] = (dw[s] + dw[s - 1]) / 2;
+      // pulse amplitudes of every block, with the header-time additions of the blocks
+      const double save_t = m_header.t, dt = this->Get_dt();
+      double t = m_header.t;
+      Fs.resize(Na);
+      for (int i = 0; i < Na; i++) {
+        m_header.t = t;
+        this->pulse_amplitudes(seq, Nk, Fs[i]);
+        t += 0.5 * dt;
+        for (int j = 0; j < Nk; j++) t += (j == Nk - 1) ? 0.5 * dt : dt;
+      }
+      m_header.t = save_t;
+      this->upload_step_parameters(seq);
+      this->gpu_before();
+      std::ostringstream hdr;
+      hdr << "# time \t";
+      for (auto &p : m_rabi_momentum_list) hdr << p << "\t";
+      jobs.resize(seq.no_of_chirps - 1);
+      for (int s = 1; s < seq.no_of_chirps; s++) {
+        ScanJob &j = jobs[s - 1];
+        atus_check(this->m_gpu, atus_clone(this->m_gpu, &j.ctx), "clone");
+        j.laser = make_laser();
+        j.phase = s * 2.0 * M_PI / (1.0 * seq.no_of_chirps);
+        j.laser.phase[0] = j.phase;
+        j.laser.chirp_rate[0] = dw[s];
+        j.s = s;
+        j.kind = gkind;
+        j.Na = Na;
+        j.Nk = Nk;
+        j.seq_counter = seq_counter;
+        j.F = &Fs;
+        for (auto &p : m_rabi_momentum_list)
+          for (int a = 0; a < dim; a++) j.k0.push_back(p[a]);
+        j.nrm = nrm;
+        j.thr = m_rabi_threshold;
+        j.dt = m_header.dt;
+        j.rabi_freq = seq.rabi_output_freq;
+        j.pn_freq = seq.compute_pn_freq;
+        j.rabi_header = hdr.str();
+      }
+      for (auto &j : jobs) workers.emplace_back(&CRT_Base_IF::run_scan, &j);
+    }
+    for (int s = 0; s < (side ? 1 : seq.no_of_chirps); ++s) {
       m_rabi_freq_list.clear();
       chirp_rate[0] = dw[s];
       if (seq.chirp_mode == 1) phase[0] = s * 2.0 * M_PI / (1.0 * seq.no_of_chirps);
@@ -386,20 +551,32 @@ void CRT_Base_IF<T, dim, no_int_states>::run_sequence() {
           tmp.push_front(s);
           m_chirps_list.push_back(tmp);
         }
-        if (s < seq.no_of_chirps - 1) {
+        if (s < seq.no_of_chirps - 1 && !side) {
           for (int k = 0; k < no_int_states; k++) {
             snprintf(filename, sizeof filename, "%.3f_%d.bin", backup_t, k + 1);
             this->reload(filename, k);
           }
           m_header.t = backup_t;
         }
-        if (s > 0 && s < seq.no_of_chirps - 1) {
+        if (s > 0 && s < seq.no_of_chirps - 1 && !side) {
           dw[s + 1] = (dw[s] + dw[s - 1]) / 2;
           if (dphi[s] - dphi[s - 1] < 0) {
             dw[s] = dw[s - 1];
             dphi[s] = dphi[s - 1];
           }
         }
+      }
+    }
+    if (side) {  // the other scans, in scan order
+      for (auto &w : workers) w.join();
+      for (auto &j : jobs) {
+        atus_destroy(j.ctx);
+        if (j.err) {
+          std::cerr << "GPU error in scan " << j.s << ": " << j.errmsg << " (code " << j.err << ")" << endl;
+          exit(EXIT_FAILURE);
+        }
+        std::cout << j.text;
+        if (nrm > 0) m_chirps_list.push_back(j.entry);
       }
     }
     if (seq.no_of_chirps > 1) {

@@ -88,6 +88,7 @@ class BatchInstance(C.Structure):
 _vp, _dp, _i, _d = C.c_void_p, C.POINTER(C.c_double), C.c_int, C.c_double
 SIGNATURES = {
     "atus_create": (_i, [C.POINTER(Grid), _i, _i, C.POINTER(C.c_void_p)]),
+    "atus_clone": (_i, [_vp, C.POINTER(C.c_void_p)]),
     "atus_destroy": (None, [_vp]),
     "atus_last_error": (C.c_char_p, [_vp]),
     "atus_set_stream": (_i, [_vp, _vp]),

@@ -45,6 +45,8 @@
  *   atus_sob_*                      CSOB_Base (include/CSOB_Base.h:96-543)
  *   atus_particle_number_noalloc    no counterpart in the reference (see its
  *                                   declaration below)
+ *   atus_clone                      no counterpart in the reference: a copy of a
+ *                                   context's state (the scans of a phase scan side by side)
  *   atus_embed                      no counterpart in the reference: seeding the
  *                                   Sobolev descent from a smaller grid
  *   atus_guess_*                    no counterpart in the reference: a learned
@@ -132,6 +134,13 @@ typedef struct {
 /* ------------------------------------------------------------ context */
 ATUS_API int atus_create(const atus_grid *grid, int ncomp, int precision, atus_ctx **out);
 ATUS_API void atus_destroy(atus_ctx *ctx);
+/* A new context with the state of src: grid, precision, fields, potentials,
+ * kinetic phases as src holds them, alpha, g, lasers, pulse windows, time and
+ * dt, on a stream of its own.  No counterpart in the reference: the chirp /
+ * phase scan of CRT_Base_IF::run_sequence (include/CRT_Base_IF.h:755-921)
+ * reruns a sequence from one start state per scan; clones let the scans of
+ * a phase scan run side by side. */
+ATUS_API int atus_clone(const atus_ctx *src, atus_ctx **out);
 ATUS_API const char *atus_last_error(const atus_ctx *ctx);
 /* Kernels run on this CUDA stream (a cudaStream_t; NULL = the context's own). */
 ATUS_API int atus_set_stream(atus_ctx *ctx, void *stream);

@@ -150,6 +150,19 @@ NUM_CASES = [
               dict(name="freeprop", dt=0.001, Nk=10, duration=0.02, rabi=True)]),
 ]
 
+# phase scans (CRT_Base_IF::run_sequence, chirp_mode 1): no_of_chirps runs of
+# the same sequence from the same start, scan s with laser phase s 2 pi / n
+# and the chirp rates chirp_min, chirp_max, then midpoints (include/
+# CRT_Base_IF.h:755-921)
+PHASESCAN_CASES = [
+    dict(name="scan1d", dim=1, n=[256], lo=[-32.0], hi=[32.0], laser_k=2.0, laser_domh=8.0, Amp=4.0,
+         tc=0.02, two_sigma2=2 * 0.008 ** 2, g=[100.0, 90.0, 90.0, 100.0], Delta_L=[0.0, 0.2], Beta=[0.05],
+         chirps=5, chirp_min=-2.0, chirp_max=3.0),
+    dict(name="scan2d", dim=2, n=[64, 32], lo=[-16.0, -8.0], hi=[16.0, 8.0], laser_k=2.0, laser_domh=8.0,
+         Amp=4.0, tc=0.02, two_sigma2=2 * 0.008 ** 2, g=[100.0] * 4, Delta_L=[0.0, 0.5], Beta=[0.1, 0.0],
+         chirps=4, chirp_min=-1.0, chirp_max=1.0),
+]
+
 SOB_CASES = [
     dict(name="sob1d", dim=1, n=[64], lo=[-8.0], hi=[8.0], g=50.0, Nparticles=1.0, alpha=0.5, stepsize=0.01,
          epsilon=1e-7, V_expr="0.5*x*x", guess_expr="exp(-0.5*x*x)"),
@@ -480,6 +493,58 @@ def make_numerical(case, tmp):
                 xml=xml)
 
 
+def make_phasescan(case, tmp):
+    """The bragg program with a phase scan on its bragg_ad sequence
+    (no_of_chirps, chirp_mode 1), Rabi sums every block, then freeprop:
+    every .bin output, the Rabi file of each scan and the Chirp file."""
+    rng = np.random.default_rng(5)
+    dim = case["dim"]
+    h = binfmt.make_header(dim, case["n"], case["lo"], case["hi"], dt=0.001)
+    X = grid(h)
+    r2 = sum(x * x for x in X)
+    psi1 = (np.sqrt(np.maximum(0.0, 1.0 - 0.1 * r2)) * (1 + 0.01 * rng.standard_normal(r2.shape))).astype(np.complex128)
+    psi2 = np.zeros_like(psi1)
+    binfmt.write_bin(os.path.join(tmp, "inp_1.bin"), h, psi1)
+    binfmt.write_bin(os.path.join(tmp, "inp_2.bin"), h, psi2)
+    nc = case["chirps"]
+    xml = f"""<SIMULATION>
+  <DIM>{dim}</DIM>
+  <FILENAME>inp_1.bin</FILENAME>
+  <FILENAME_2>inp_2.bin</FILENAME_2>
+  <AMP_T>exp(-(t-{case['tc']!r})*(t-{case['tc']!r})/{case['two_sigma2']!r})</AMP_T>
+  <CONSTANTS>
+    <laser_k>{case['laser_k']!r}</laser_k><laser_dk>0</laser_dk><laser_domh>{case['laser_domh']!r}</laser_domh>
+    <rabi_threshold>1.0</rabi_threshold><chirp>0</chirp>
+  </CONSTANTS>
+  <VCONSTANTS>
+    <Amp_1>{case['Amp']!r},{case['Amp']!r}</Amp_1>
+    <Alpha_1>{xml_vec([0.5] * dim)}</Alpha_1>
+    <Delta_L>{xml_vec(case['Delta_L'])}</Delta_L>
+    <GS_1>{xml_vec(case['g'][:2])}</GS_1><GS_2>{xml_vec(case['g'][2:])}</GS_2>
+    <Beta>{xml_vec(case['Beta'])}</Beta>
+  </VCONSTANTS>
+  <ALGORITHM><DT>1</DT></ALGORITHM>
+  <SEQUENCE>
+    <bragg_ad dt="0.001" Nk="10" output_freq="each" pn_freq="none" rabi_output_freq="each" no_of_chirps="{nc}"
+      chirp_mode="1" chirp_min="{case['chirp_min']!r}" chirp_max="{case['chirp_max']!r}">0.04</bragg_ad>
+    <freeprop dt="0.001" Nk="10" output_freq="each" pn_freq="none" rabi_output_freq="each">0.02</freeprop>
+  </SEQUENCE>
+</SIMULATION>"""
+    open(os.path.join(tmp, "run.xml"), "w").write(xml)
+    run("bragg", tmp)
+    t, psi = collect_outputs(tmp, 2, [])
+
+    def rows(path):
+        return np.array([[float(v) for v in ln.split()] for ln in open(path) if not ln.startswith("#") and ln.split()])
+
+    rabi = np.stack([rows(os.path.join(tmp, f"Rabi_1_{k}.txt")) for k in range(nc)])
+    rabi_free = rows(os.path.join(tmp, "Rabi_2_0.txt"))
+    chirp = rows(os.path.join(tmp, "Chirp_1.txt"))
+    params = dict(program="bragg", dim=dim, ncomp=2, chirps=nc, laser_k=case["laser_k"])
+    return dict(header=h.tobytes(), psi0=np.stack([psi1, psi2]), t=t, psi=psi, rabi_scans=rabi,
+                rabi_free=rabi_free, chirp=chirp, params=json.dumps(params), xml=xml)
+
+
 def make_sob(case, tmp):
     dim = case["dim"]
     ax = "XYZ"[:dim]
@@ -517,8 +582,14 @@ def main():
     CASES, BRAGG_CASES = [c for c in CASES if keep(c)], [c for c in BRAGG_CASES if keep(c)]
     DBRAGG_CASES, SOB_CASES = [c for c in DBRAGG_CASES if keep(c)], [c for c in SOB_CASES if keep(c)]
     BRAGGDS_CASES = [c for c in BRAGGDS_CASES if keep(c)]
-    global NUM_CASES
+    global NUM_CASES, PHASESCAN_CASES
     NUM_CASES = [c for c in NUM_CASES if keep(c)]
+    PHASESCAN_CASES = [c for c in PHASESCAN_CASES if keep(c)]
+    for case in PHASESCAN_CASES:
+        with tempfile.TemporaryDirectory() as tmp:
+            d = make_phasescan(case, tmp)
+            np.savez_compressed(os.path.join(HERE, case["name"] + ".npz"), **d)
+            print("wrote", case["name"])
     for case in CASES:
         with tempfile.TemporaryDirectory() as tmp:
             d = make_rt(case, tmp)

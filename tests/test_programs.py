@@ -137,6 +137,40 @@ def _realtime_program(name, env=None):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("name", ["scan1d", "scan2d"])
+@pytest.mark.parametrize("sequential", [False, True])
+def test_phase_scan_matches_reference(name, sequential):
+    """A phase scan (bragg_ad with no_of_chirps scans, chirp_mode 1) then
+    freeprop, through ATUS-2's bragg program on the drop-in headers: scans
+    1..n-1 side by side on clones of the context (default) or one after
+    another (ATUS_SEQUENTIAL_SCANS=1); the .bin outputs (scan 0), the Rabi
+    file of every scan and the Chirp file against the reference program."""
+    from test_gpu_parity import FP64_TOL, state_close
+
+    g = load(name)
+    nc = int(g["params"]["chirps"])
+
+    def rows(path):
+        return np.array([[float(v) for v in ln.split()] for ln in open(path) if not ln.startswith("#") and ln.split()])
+
+    with tempfile.TemporaryDirectory() as tmp:
+        _write_inputs(g, tmp)
+        run("bragg", tmp, env={"ATUS_SEQUENTIAL_SCANS": "1"} if sequential else None)
+        outs = _outputs(tmp, 2)
+        rabi = np.stack([rows(os.path.join(tmp, f"Rabi_1_{k}.txt")) for k in range(nc)])
+        rabi_free = rows(os.path.join(tmp, "Rabi_2_0.txt"))
+        chirp = rows(os.path.join(tmp, "Chirp_1.txt"))
+    assert len(outs) == len(g["t"])
+    for (t, psi), t_ref, psi_ref in zip(outs, g["t"], g["psi"]):
+        assert t == t_ref
+        state_close(list(psi), list(psi_ref), FP64_TOL)
+    # six significant digits in the text files
+    np.testing.assert_allclose(rabi, g["rabi_scans"], rtol=5e-6, atol=1e-10)
+    np.testing.assert_allclose(rabi_free, g["rabi_free"], rtol=5e-6, atol=1e-10)
+    np.testing.assert_allclose(chirp, g["chirp"], rtol=5e-6, atol=1e-10)
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("name", SOB_CASES)
 def test_sobmin_program_matches_reference(name):
     g = load(name)
