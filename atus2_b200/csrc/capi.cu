@@ -224,8 +224,151 @@ static int transform_inner(atus_ctx *ctx, int dir, void *const *f = nullptr, int
   return ATUS_OK;
 }
 
-// k-space kinetic pass along axis 0: FFT_x, phase, IFFT_x.
+static int grid_blocks(int64_t n, int threads) {
+  int64_t b = (n + threads - 1) / threads;
+  return (int)(b < 148 * 16 ? b : 148 * 16);
+}
+
+// ------------------------------------------------------------------ long 1D axes (four-step)
+// x[n], n = n2c * r + c (r < n1 along view axis 0, stride n2c; c < n2c along
+// view axis 1, contiguous).  Forward: transform along r, times W_N^{r' c}
+// (r' the transformed index), transform along c; element (k1, k2) then holds
+// X[k1 + n1 k2].  Inverse: the same steps backwards with conjugate twiddles.
+template <typename R>
+__global__ void fs_twiddle_kernel(void *psi, const double2 *tw, int64_t n2c, int64_t N, int conj_) {
+  cplx<R> *p = static_cast<cplx<R> *>(psi);
+  for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < N; l += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = l / n2c, c = l % n2c;
+    double2 w = tw[(r * c) % N];
+    if (conj_) w.y = -w.y;
+    p[l] = from_d<R>(cmul(to_d<R>(p[l]), w));
+  }
+}
+
+// Kinetic factor of the four-step spectrum: element (k1, k2) is wavenumber
+// index k1 + n1 k2 of the 1D table, with the transform scales applied as in
+// the passes: ((u s_f) K) s_b in FP64.
+template <typename R>
+__global__ void fs_kin_kernel(void *psi, const double2 *kt, int64_t n1, int64_t n2c, double s_f, double s_b) {
+  cplx<R> *p = static_cast<cplx<R> *>(psi);
+  const int64_t N = n1 * n2c;
+  for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < N; l += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k1 = l / n2c, k2 = l % n2c;
+    const double2 K = kt[k1 + n1 * k2];
+    double2 u = to_d<R>(p[l]);
+    u.x *= s_f;
+    u.y *= s_f;
+    u = cmul(u, K);
+    u.x *= s_b;
+    u.y *= s_b;
+    p[l] = from_d<R>(u);
+  }
+}
+
+// Four-step spectrum <-> natural wavenumber order, FP64 buffers:
+// to_natural: dst[k1 + n1 k2] = src[k1 n2c + k2]; else the inverse.
+__global__ void fs_reorder_kernel(const double2 *src, double2 *dst, int64_t n1, int64_t n2c, int to_natural) {
+  const int64_t N = n1 * n2c;
+  for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < N; l += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k1 = l / n2c, k2 = l % n2c;
+    if (to_natural) dst[k1 + n1 * k2] = src[l];
+    else dst[l] = src[k1 + n1 * k2];
+  }
+}
+
+// The context seen as its n1 x n2c four-step grid while plain transforms run.
+struct FsView {
+  atus_ctx *c;
+  int dim;
+  int64_t n[3];
+  int lg[3];
+  explicit FsView(atus_ctx *ctx) : c(ctx), dim(ctx->dim) {
+    for (int a = 0; a < 3; a++) {
+      n[a] = ctx->n[a];
+      lg[a] = ctx->lg[a];
+    }
+    ctx->dim = 2;
+    ctx->n[0] = ctx->fs_n1;
+    ctx->n[1] = ctx->fs_n2;
+    ctx->n[2] = 1;
+    ctx->lg[0] = ilog2(ctx->fs_n1);
+    ctx->lg[1] = ilog2(ctx->fs_n2);
+    ctx->lg[2] = 0;
+  }
+  ~FsView() {
+    c->dim = dim;
+    for (int a = 0; a < 3; a++) {
+      c->n[a] = n[a];
+      c->lg[a] = lg[a];
+    }
+  }
+};
+
+static int fs_twiddle(atus_ctx *ctx, void *const *f, int nf, int conj_, bool fp64) {
+  for (int i = 0; i < nf; i++) {
+    if (fp64)
+      fs_twiddle_kernel<double><<<grid_blocks(ctx->npts, 256), 256, 0, ctx->stream>>>(f[i], ctx->fs_tw, ctx->fs_n2,
+                                                                                       ctx->npts, conj_);
+    else
+      fs_twiddle_kernel<float><<<grid_blocks(ctx->npts, 256), 256, 0, ctx->stream>>>(f[i], ctx->fs_tw, ctx->fs_n2,
+                                                                                      ctx->npts, conj_);
+    LAUNCHED(ctx);
+  }
+  return ATUS_OK;
+}
+
+// Unscaled forward / inverse transform of nf fields (four-step order in k).
+static int fs_forward(atus_ctx *ctx, void *const *f, int nf) {
+  const bool fp64 = ctx->prec == ATUS_PREC_FP64;
+  {
+    FsView v(ctx);
+    RUN(run_pass(ctx, 0, T_FWD, OP_NONE, T_NONE, nullptr, 0, f, nf));
+  }
+  RUN(fs_twiddle(ctx, f, nf, 0, fp64));
+  FsView v(ctx);
+  return run_pass(ctx, 1, T_FWD, OP_NONE, T_NONE, nullptr, 0, f, nf);
+}
+static int fs_inverse(atus_ctx *ctx, void *const *f, int nf) {
+  const bool fp64 = ctx->prec == ATUS_PREC_FP64;
+  {
+    FsView v(ctx);
+    RUN(run_pass(ctx, 1, T_INV, OP_NONE, T_NONE, nullptr, 0, f, nf));
+  }
+  RUN(fs_twiddle(ctx, f, nf, 1, fp64));
+  FsView v(ctx);
+  return run_pass(ctx, 0, T_INV, OP_NONE, T_NONE, nullptr, 0, f, nf);
+}
+
+// An FP64 four-step spectrum (scratch-sized buffer) into / out of natural order.
+static int fs_reorder(atus_ctx *ctx, void *&buf, int to_natural) {
+  if (!ctx->fs_tmp) CK(cudaMalloc(&ctx->fs_tmp, 16 * ctx->npts));
+  fs_reorder_kernel<<<grid_blocks(ctx->npts, 256), 256, 0, ctx->stream>>>(
+      static_cast<const double2 *>(buf), static_cast<double2 *>(ctx->fs_tmp), ctx->fs_n1, ctx->fs_n2, to_natural);
+  LAUNCHED(ctx);
+  void *t = buf;
+  buf = ctx->fs_tmp;
+  ctx->fs_tmp = t;
+  return ATUS_OK;
+}
+
+// k-space kinetic pass along axis 0: FFT_x, phase, IFFT_x (a long 1D axis:
+// four-step transforms around the factor of each wavenumber).
 static int kinetic_pass(atus_ctx *ctx, int half) {
+  if (ctx->fs_tw) {
+    RUN(fs_forward(ctx, ctx->psi, ctx->ncomp));
+    const double s_f = scale_fak(ctx->dim, ctx->d), s_b = scale_fak(ctx->dim, ctx->dk);
+    for (int c = 0; c < ctx->ncomp; c++) {
+      const double2 *kt = ctx->kt[half ? 0 : 1][c][0];
+      if (ctx->prec == ATUS_PREC_FP64)
+        fs_kin_kernel<double><<<grid_blocks(ctx->npts, 256), 256, 0, ctx->stream>>>(ctx->psi[c], kt, ctx->fs_n1,
+                                                                                    ctx->fs_n2, s_f, s_b);
+      else
+        fs_kin_kernel<float><<<grid_blocks(ctx->npts, 256), 256, 0, ctx->stream>>>(ctx->psi[c], kt, ctx->fs_n1,
+                                                                                   ctx->fs_n2, s_f, s_b);
+      LAUNCHED(ctx);
+    }
+    return fs_inverse(ctx, ctx->psi, ctx->ncomp);
+  }
   return run_pass(ctx, 0, T_FWD, OP_KIN, T_INV, nullptr, half);
 }
 
@@ -329,11 +472,6 @@ static int reduce_dev(atus_ctx *ctx, RedArgs &a, double *dst) {
   return ATUS_OK;
 }
 
-static int grid_blocks(int64_t n, int threads) {
-  int64_t b = (n + threads - 1) / threads;
-  return (int)(b < 148 * 16 ? b : 148 * 16);
-}
-
 // Copy component comp into the FP64 scratch buffer (complex128).
 static int to_scratch(atus_ctx *ctx, int comp) {
   if (ctx->prec == ATUS_PREC_FP64) {
@@ -353,7 +491,13 @@ static int scratch_forward(atus_ctx *ctx) {
   ctx->prec = ATUS_PREC_FP64;
   void *f[1] = {ctx->scratch};
   int r = ATUS_OK;
-  for (int ax = ctx->dim - 1; ax >= 0 && r == ATUS_OK; ax--) r = run_pass(ctx, ax, T_FWD, OP_NONE, T_NONE, nullptr, 0, f, 1);
+  if (ctx->fs_tw) {
+    r = fs_forward(ctx, f, 1);
+    if (r == ATUS_OK) r = fs_reorder(ctx, ctx->scratch, 1);
+  } else {
+    for (int ax = ctx->dim - 1; ax >= 0 && r == ATUS_OK; ax--)
+      r = run_pass(ctx, ax, T_FWD, OP_NONE, T_NONE, nullptr, 0, f, 1);
+  }
   ctx->prec = saved;
   return r;
 }
@@ -403,7 +547,10 @@ int atus_create(const atus_grid *grid, int ncomp, int precision, atus_ctx **out)
     ctx->n[a] = (a < grid->dim) ? grid->n[a] : 1;
     ctx->d[a] = (a < grid->dim) ? grid->d[a] : 0.0;
     ctx->dk[a] = (a < grid->dim) ? grid->dk[a] : 0.0;
-    if (ctx->n[a] < 1 || (ctx->n[a] & (ctx->n[a] - 1)) != 0 || ctx->n[a] > 8192) {  // longest pass instantiation
+    // the longest pass instantiation is 8192 points; a 1D axis up to 2^26
+    // points runs as four-step transforms over two such passes
+    const int64_t nmax = (grid->dim == 1 && a == 0) ? (int64_t(1) << 26) : 8192;
+    if (ctx->n[a] < 1 || (ctx->n[a] & (ctx->n[a] - 1)) != 0 || ctx->n[a] > nmax) {
       delete ctx;
       return ATUS_E_UNSUPPORTED;
     }
@@ -465,6 +612,26 @@ int atus_create(const atus_grid *grid, int ncomp, int precision, atus_ctx **out)
     return ATUS_E_NOMEM;
   }
   // CRT_Base's constructor builds the tables once (alpha still zero).
+  if (ok && ctx->dim == 1 && ctx->n[0] > 8192) {
+    // four-step view n1 x n2 (n2 >= n1, both powers of two <= 8192) and the
+    // exact twiddles W_N^m = exp(-2 pi i m / N) rounded once from long double
+    const int l = ctx->lg[0];
+    ctx->fs_n1 = int64_t(1) << (l / 2);
+    ctx->fs_n2 = ctx->n[0] / ctx->fs_n1;
+    std::vector<double2> t(ctx->n[0]);
+    const long double two_pi = 6.283185307179586476925286766559005768L;
+    for (int64_t m = 0; m < ctx->n[0]; m++) {
+      const long double th = two_pi * (long double)m / (long double)ctx->n[0];
+      t[m].x = (double)cosl(th);
+      t[m].y = (double)(-sinl(th));
+    }
+    ok = cudaMalloc(&ctx->fs_tw, sizeof(double2) * ctx->n[0]) == cudaSuccess &&
+         cudaMemcpy(ctx->fs_tw, t.data(), sizeof(double2) * ctx->n[0], cudaMemcpyHostToDevice) == cudaSuccess;
+    if (!ok) {
+      atus_destroy(ctx);
+      return ATUS_E_NOMEM;
+    }
+  }
   int r = build_kinetic(ctx);
   if (r != ATUS_OK) {
     atus_destroy(ctx);
@@ -491,6 +658,8 @@ void atus_destroy(atus_ctx *ctx) {
   if (ctx->snap_taken) cudaEventDestroy(ctx->snap_taken);
   if (ctx->snap_read) cudaEventDestroy(ctx->snap_read);
   if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+  cudaFree(ctx->fs_tw);
+  cudaFree(ctx->fs_tmp);
   cudaFree(ctx->scratch);
   cudaFree(ctx->sob_dev);
   if (ctx->sob_graph) cudaGraphExecDestroy(ctx->sob_graph);
@@ -743,7 +912,20 @@ int atus_ft(atus_ctx *ctx, int comp, int isign) {
   if (!ctx || comp < 0 || comp >= ctx->ncomp || (isign != -1 && isign != 1)) return ATUS_E_ARG;
   void *f[1] = {ctx->psi[comp]};
   const int dir = (isign < 0) ? T_FWD : T_INV;
-  for (int ax = ctx->dim - 1; ax >= 0; ax--) RUN(run_pass(ctx, ax, dir, OP_NONE, T_NONE, nullptr, 0, f, 1));
+  if (ctx->fs_tw) {
+    // the spectrum in natural wavenumber order, as cft_1d::ft leaves it
+    if (ctx->prec != ATUS_PREC_FP64) return fail(ctx, ATUS_E_UNSUPPORTED, "ft of a long complex64 1D field");
+    if (isign < 0) {
+      RUN(fs_forward(ctx, f, 1));
+      RUN(fs_reorder(ctx, ctx->psi[comp], 1));
+    } else {
+      RUN(fs_reorder(ctx, ctx->psi[comp], 0));
+      void *g[1] = {ctx->psi[comp]};
+      RUN(fs_inverse(ctx, g, 1));
+    }
+  } else {
+    for (int ax = ctx->dim - 1; ax >= 0; ax--) RUN(run_pass(ctx, ax, dir, OP_NONE, T_NONE, nullptr, 0, f, 1));
+  }
   const double fak = scale_fak(ctx->dim, isign < 0 ? ctx->d : ctx->dk);
   if (ctx->prec == ATUS_PREC_FP64)
     ft_scale_kernel<double><<<grid_blocks(ctx->npts, 256), 256, 0, ctx->stream>>>(ctx->psi[comp], fak, ctx->npts);
@@ -861,10 +1043,14 @@ static int strang_block(atus_ctx *ctx, int nk, int kind, const double *F, const 
   if (!ctx || nk < 1) return ATUS_E_ARG;
   RUN(check_kind(ctx, kind));
   const double dt = ctx->dt;
-  if (ctx->dim == 1 && (ctx->ncomp > 2 || kind == K_NUM_BRAGG)) {
-    // more components than the resident 1D kernel holds, or a step that reads
-    // the header time itself: per step one kinetic pass (FFT, phase, IFFT per
-    // component) and one point-wise potential step
+  // shared memory of the resident 1D kernel (padded pencils, Pad<N>)
+  const int64_t n0 = ctx->n[0];
+  const int64_t np1d = ((n0 >= 16) ? (n0 + n0 / 16) : n0) | 1;
+  const bool fits1d = (int64_t)ctx->csize * tc_for(ctx->ncomp) * np1d <= 227 * 1024;
+  if (ctx->dim == 1 && (ctx->ncomp > 2 || kind == K_NUM_BRAGG || ctx->fs_tw || !fits1d)) {
+    // more components or points than the resident 1D kernel holds, or a step
+    // that reads the header time itself: per step one kinetic pass (FFT,
+    // phase, IFFT per component) and one point-wise potential step
     RUN(kinetic_pass(ctx, 1));
     ctx->t += 0.5 * dt;
     for (int j = 0; j < nk; j++) {
@@ -1087,6 +1273,7 @@ int atus_rabi_integrals_comp(atus_ctx *ctx, int comp, const double *k0, int n, d
 // Real k-space filter of an FP64 buffer over all axes: forward transforms,
 // filter inside the axis-0 pass, inverse transforms.
 static int sob_filter_n(atus_ctx *ctx, void *const *bufs, int nb, int mode, double alpha) {
+  if (ctx->fs_tw) return fail(ctx, ATUS_E_UNSUPPORTED, "the Sobolev filter takes 1D grids of at most 8192 points");
   const int saved = ctx->prec;
   ctx->prec = ATUS_PREC_FP64;
   int r = ATUS_OK;

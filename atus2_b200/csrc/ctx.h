@@ -45,6 +45,12 @@ struct atus_ctx {
   cudaGraphExec_t sob_graph = nullptr;  // a chunk of device-side iterations
   double sob_graph_step = 0;            // stepsize the graph was captured with
   void *h_sob = nullptr;                // pinned host copy of the SobDev
+  // 1D fields longer than the longest pass (four-step transforms): the field
+  // viewed as fs_n1 x fs_n2 (n = fs_n2 * n1 + n2), W_N^m for m < N, and a
+  // second N-point FP64 buffer for reordering spectra into natural k order
+  int64_t fs_n1 = 0, fs_n2 = 0;
+  double2 *fs_tw = nullptr;
+  void *fs_tmp = nullptr;
   // asynchronous output snapshots
   void *snap = nullptr;                 // ncomp x N complex128 staging copy
   cudaStream_t copy_stream = nullptr;   // its device->host copies

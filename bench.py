@@ -780,11 +780,9 @@ def run_batch(stream_unused=None):
     (atus2_b200.sweep), complex64 fields with FP64 phase arguments, autotuned,
     BATCH_STEPS steps as one graph launch.  Against it: the same instances one
     by one in plain FP64, timed on one representative instance per size class
-    over the full BATCH_STEPS -- a context where one exists, a single-instance
-    FP64 batch for 1D 8192 (no FP64 context fits one SM), and for 1D 16384
-    (no FP64 kernel at all) the 8192 time scaled by 2 * 14/13, the FFT work
-    ratio -- which also gives the accuracy of each class after BATCH_STEPS
-    steps."""
+    over the full BATCH_STEPS in one FP64 context (1D 8192 with two
+    components runs as per-step passes, 1D 16384 as four-step transforms),
+    which also gives the accuracy of each class after BATCH_STEPS steps."""
     import torch
 
     from atus2_b200 import PREC_FP64, PREC_MIXED, STEP_BRAGG_AD, Batch, Solver, sweep
@@ -807,25 +805,9 @@ def run_batch(stream_unused=None):
     seq_ms = {}
     errs = {}
     for key, ids in sorted(classes.items()):
-        if key == (1, 16384):
-            continue
         i = ids[0]
         d = insts[i]
         h = d["header"]
-        if key == (1, 8192):
-            # two complex128 components of 8192 points exceed one SM's shared
-            # memory for a context: a single-instance FP64 batch (one component
-            # resident) is the plain FP64 run of this instance
-            one = Batch([dict(d, bragg_stable=True)], PREC_FP64, DT)
-            p = sweep.initial_state(h)
-            one.set_psi(0, 0, p)
-            one.set_psi(0, 1, np.zeros_like(p))
-            seq_ms[key] = one.run(BATCH_STEPS)
-            ref = np.stack([one.psi(0, 0), one.psi(0, 1)])
-            got = np.stack([b.psi(i, 0), b.psi(i, 1)])
-            errs[f"{key[0]}D-{key[1]}"] = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
-            one.close()
-            continue
         s = Solver(h, 2, PREC_FP64)
         s.set_bragg_stable(True)  # the reference's eigen-form diverges in this sweep's pulse tails
         p = sweep.initial_state(h)
@@ -864,8 +846,6 @@ def run_batch(stream_unused=None):
         s.block(BATCH_STEPS, STEP_BRAGG_AD, d["laser"], sweep.pulse_values(0.0, BATCH_STEPS, *d["pulse"], DT))
         ref_norms[f"1D-{key[1]}"] = s.particle_number(0) + s.particle_number(1)
         s.close()
-    if (1, 16384) in classes and (1, 8192) in classes:
-        seq_ms[(1, 16384)] = seq_ms[(1, 8192)] * 2 * 14 / 13
     seq_total = sum(seq_ms[k] * len(v) for k, v in classes.items())
     work = BATCH_COUNT * BATCH_STEPS
     sched = b.schedule()

@@ -244,7 +244,7 @@ def test_block_rabi_fused_matches_oracle(grid, ncomp, comps):
         np.testing.assert_allclose(got[i], ref, rtol=1e-12, atol=1e-14)
 
 
-@pytest.mark.parametrize("dim,n", [(1, [4096]), (2, [64, 256]), (3, [16, 32, 256])])
+@pytest.mark.parametrize("dim,n", [(1, [4096]), (1, [32768]), (2, [64, 256]), (3, [16, 32, 256])])
 def test_field_transform_matches_oracle(dim, n):
     """atus_ft (cft_Nd::ft: transform over all axes, then the reference's
     scale) forward and back against the oracle's cft restatement, FP64."""
@@ -260,6 +260,39 @@ def test_field_transform_matches_oracle(dim, n):
         o.ft(ref, isign)
         assert rel_l2(s.psi(0), ref) < 1e-13, isign
     assert rel_l2(s.psi(0), a) < 1e-13  # a round trip is the identity (dk = 2 pi / L)
+
+
+@pytest.mark.parametrize("n,prec,tol", [(16384, PREC_FP64, FP64_TOL), (131072, PREC_FP64, FP64_TOL),
+                                        (16384, PREC_MIXED, MIXED_TOL)])
+def test_long_1d_matches_oracle(n, prec, tol):
+    """1D grids longer than one pass (four-step transforms over an n1 x n2
+    view with exact W_N twiddles): a two-state Bragg pulse then free steps
+    with g = 20, N points on [-N/128, N/128); state, particle numbers,
+    <p> and the Rabi integrals (spectrum in natural wavenumber order)
+    against the oracle."""
+    h = _grid(1, [n], n / 64.0)
+    (x,) = _coords(h)
+    psi0 = np.exp(-x * x / 32.0).astype(np.complex128)
+    psi0 /= math.sqrt(float(h["dx"]) * np.sum(np.abs(psi0) ** 2))
+    o, s = _setup_pair(h, 2, [psi0, np.zeros_like(psi0)], [0.5], [20.0, 15.0, 15.0, 18.0], 0.01 * x * x, 1e-3, prec)
+    kw = dict(beta=[0.2, 0, 0], DeltaL=[0, 0.5, 0, 0], Amp=[3.0, 3.0], laser_k=[4.0, 0], laser_dk=[0, 0],
+              laser_domh=[4.0, 0], phase=[0, 0], chirp_rate=[0, 0], chirp=0.0)
+    Lo, Ls = OLaser.make(**kw), Laser.make(**kw)
+    F = np.full(40, 0.9)
+    for _ in range(2):
+        o.block(40, KIND_BRAGG_AD, Lo, F)
+        s.block(40, KIND_BRAGG_AD, Ls, F)
+    o.block(40, KIND_NL_IF, Lo)
+    s.block(40, KIND_NL_IF, Ls)
+    assert s.t == o.t
+    state_close([s.psi(c) for c in range(2)], [o.psi(c) for c in range(2)], tol)
+    assert o.particle_number(1) > 1e-3
+    q = 1e-11 if prec == PREC_FP64 else 1e-5
+    for c in range(2):
+        np.testing.assert_allclose(s.particle_number(c), o.particle_number(c), rtol=q)
+        np.testing.assert_allclose(s.expval_momentum(c), o.expval_momentum(c), rtol=q, atol=q)
+    k0 = [[0.0], [8.0], [-8.0]]
+    np.testing.assert_allclose(s.rabi_integrals(k0, 1.0, 1), o.rabi_integrals(k0, 1.0, 1), rtol=q, atol=1e-14)
 
 
 def test_sobmin_mu_matches_oracle():
