@@ -155,6 +155,20 @@ def solve(n, wy, wz, g, coef=None, eps=EPS, max_iter=200000):
     return psi, it, res, dt, mu
 
 
+def mu_normalized(n, wy, wz, g, psi):
+    """mu (the descent's formula) of `psi` scaled to particle number 1."""
+    h = header(n)
+    s = Solver(h, 1, PREC_FP64)
+    nrm = (L_BOX / n) ** 3 * np.vdot(psi, psi).real
+    s.set_psi(0, psi / math.sqrt(nrm))
+    s.set_potential(0, potential(h, wy, wz))
+    s.set_gs([g])
+    s.sob_init([ALPHA], STEP)
+    mu = float(s.sob_mu()[0])
+    s.close()
+    return mu
+
+
 def small_box(n: int, wy: float, wz: float, g: float, margin: float = 3.0):
     """Points per axis of the smallest grid with the full grid's spacing that
     holds the condensate of a draw: twice its Thomas-Fermi radius plus
@@ -292,7 +306,8 @@ def evaluate(count: int, seed: int, n: int = 128, train_epochs: int = 20000):
     from the Thomas-Fermi guess against solve_learned, both to EPS; per draw
     iterations, seconds, mu and the particle number of the final state
     (the reference's descent renormalises only when |N - 1| > 1e-5, so two
-    converged runs end at slightly different N and mu)."""
+    converged runs end at slightly different N and mu; dmu_normalized
+    compares the two states scaled to N = 1)."""
     d = np.load(TRAIN_FILE)
     m, sd = coef_stats(d["coef"])
     params, hist = train(features(d["params"]), (d["coef"] - m) / sd, epochs=train_epochs, lr=2e-3)
@@ -307,13 +322,16 @@ def evaluate(count: int, seed: int, n: int = 128, train_epochs: int = 20000):
                          N_plain=float(dv * np.vdot(psi_p, psi_p).real), iters_learned=[int(i) for i in it_l],
                          s_learned=t_l, mu_learned=mu_l, N_learned=float(dv * np.vdot(psi_l, psi_l).real),
                          small_box=ns, speedup=t_p / t_l, dmu=abs(mu_l - mu_p),
+                         dmu_normalized=abs(mu_normalized(n, wy, wz, g, psi_l) - mu_normalized(n, wy, wz, g, psi_p)),
                          rel_l2=float(np.linalg.norm(psi_l - psi_p) / np.linalg.norm(psi_p))))
         print(json.dumps(rows[-1]), flush=True)
     sp = np.array([r["speedup"] for r in rows])
     return dict(count=count, seed=seed, n=n, rows=rows, mean_speedup=float(sp.mean()),
                 total_speedup=float(sum(r["s_plain"] for r in rows) / sum(r["s_learned"] for r in rows)),
                 min_speedup=float(sp.min()), frac_ge_3=float((sp >= 3).mean()),
-                max_dmu=float(max(r["dmu"] for r in rows)), training_loss=[float(hist[0]), float(hist[-1])])
+                max_dmu=float(max(r["dmu"] for r in rows)),
+                max_dmu_normalized=float(max(r["dmu_normalized"] for r in rows)),
+                training_loss=[float(hist[0]), float(hist[-1])])
 
 
 def main():
@@ -331,7 +349,8 @@ def main():
         with open(a.out, "w") as f:
             json.dump(out, f)
         print(f"{a.held_out} draws: mean speed-up {out['mean_speedup']:.2f}, total {out['total_speedup']:.2f}, "
-              f"min {out['min_speedup']:.2f}, >= 3x for {100 * out['frac_ge_3']:.0f} %, max |dmu| {out['max_dmu']:.2e}")
+              f"min {out['min_speedup']:.2f}, >= 3x for {100 * out['frac_ge_3']:.0f} %, max |dmu| {out['max_dmu']:.2e}, "
+              f"at N = 1 {out['max_dmu_normalized']:.2e}")
         return
     t0 = time.perf_counter()
     d = generate(a.count, a.seed, a.n, a.workers)

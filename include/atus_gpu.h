@@ -132,6 +132,9 @@ typedef struct {
 } atus_laser;
 
 /* ------------------------------------------------------------ context */
+/* Axis lengths: powers of two, 2..8192 per axis in 2D and 3D; a 1D grid up to
+ * 2^26 points (above 8192 the transforms run four-step over an n1 x n2 view;
+ * the Sobolev descent keeps the 8192 limit).  Else ATUS_E_UNSUPPORTED. */
 ATUS_API int atus_create(const atus_grid *grid, int ncomp, int precision, atus_ctx **out);
 ATUS_API void atus_destroy(atus_ctx *ctx);
 /* A new context with the state of src: grid, precision, fields, potentials,
