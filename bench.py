@@ -607,7 +607,7 @@ def run_cpu_baseline(n_short=1, n_long=5, repeats=3):
 # FP64 256^3 x 2 kernels, each from one ncu capture of that kernel on this
 # workload on a B200 (a profiler cannot run inside the timed bench, so the
 # capture's figure is carried here).
-NCU_TRAFFIC_FP64 = {"pass2_kernel M2_NL (z)": 1.0769e9, "pass2_kernel M2_KIN": 1.0433e9}
+NCU_TRAFFIC_FP64 = {"pass2_kernel M2_NL (z)": 1.0941e9, "pass2_kernel M2_KIN": 1.0433e9}
 
 
 def roofline(s, kind, peak, peak_kind, fp64=True):
@@ -710,6 +710,8 @@ def atus_arm(args, rank, ws, local, dist):
                                                     accuracy=not args.no_accuracy)
     if args.file_output and rank == 0:
         out["variants"]["file_output"] = run_output_overlap()
+    if args.phase_scans and rank == 0:
+        out["variants"]["phase_scans"] = run_phase_scans()
     if not args.no_batch:
         barrier(dist)
         out["variants"]["batch"] = run_batch()
@@ -767,6 +769,59 @@ def run_output_overlap(blocks=4, nk=1000, reps=3):
             out[name + "_all_s"] = times[name]
     out["output_cost_async_s"] = out["async_output_s"] - out["no_output_s"]
     out["output_cost_sync_s"] = out["sync_output_s"] - out["no_output_s"]
+    return out
+
+
+def run_phase_scans(reps=3):
+    """ATUS-2's bragg program on the drop-in headers with a phase scan
+    (no_of_chirps scans of a bragg_ad sequence, chirp_mode 1, Rabi sums every
+    block): scans 1..n-1 side by side on cloned contexts (the default)
+    against one after another (ATUS_SEQUENTIAL_SCANS=1).  Median wall time
+    of `reps` runs of the whole program, the two kinds interleaved."""
+    prog = os.path.join(ROOT, "atus2_b200", "host", "bin", "bragg")
+    if not os.path.exists(prog):
+        return {"unavailable": "host/bin/bragg is not built (needs the ATUS-2 source tree at build time)"}
+    from atus2_b200 import binfmt
+
+    cases = [dict(name="1D-4096", dim=1, n=[4096], L=[128.0], scans=16, nk=100, blocks=4),
+             dict(name="2D-512", dim=2, n=[512, 512], L=[32.0, 32.0], scans=8, nk=100, blocks=2)]
+    out = {}
+    for c in cases:
+        dim = c["dim"]
+        h = binfmt.make_header(dim, c["n"], [-0.5 * L for L in c["L"]], [0.5 * L for L in c["L"]], dt=DT)
+        X = np.meshgrid(*[binfmt.x_coords(h, a) for a in range(dim)], indexing="ij")
+        r2 = sum(x * x for x in X)
+        psi1 = np.sqrt(np.maximum(0.0, 1.0 - r2 / (0.1 * c["L"][0]) ** 2)).astype(np.complex128)
+        vec = lambda v: ",".join(repr(float(a)) for a in v)
+        xml = f"""<SIMULATION>
+  <DIM>{dim}</DIM><FILENAME>inp_1.bin</FILENAME><FILENAME_2>inp_2.bin</FILENAME_2>
+  <AMP_T>exp(-(t-0.2)*(t-0.2)/0.005)</AMP_T>
+  <CONSTANTS><laser_k>4</laser_k><laser_dk>0</laser_dk><laser_domh>16</laser_domh>
+    <rabi_threshold>1</rabi_threshold><chirp>0</chirp></CONSTANTS>
+  <VCONSTANTS><Amp_1>4,4</Amp_1><Alpha_1>{vec([0.5] * dim)}</Alpha_1><Delta_L>0,0</Delta_L>
+    <GS_1>100,100</GS_1><GS_2>100,100</GS_2><Beta>{vec([0.05] * dim)}</Beta></VCONSTANTS>
+  <ALGORITHM><DT>1</DT></ALGORITHM>
+  <SEQUENCE><bragg_ad dt="{DT!r}" Nk="{c['nk']}" output_freq="none" pn_freq="none" rabi_output_freq="each"
+    no_of_chirps="{c['scans']}" chirp_mode="1" chirp_min="-2" chirp_max="2">{c['blocks'] * c['nk'] * DT!r}</bragg_ad>
+  </SEQUENCE>
+</SIMULATION>"""
+        times = {"side_by_side": [], "sequential": []}
+        with tempfile.TemporaryDirectory() as tmp:
+            binfmt.write_bin(os.path.join(tmp, "inp_1.bin"), h, psi1)
+            binfmt.write_bin(os.path.join(tmp, "inp_2.bin"), h, np.zeros_like(psi1))
+            open(os.path.join(tmp, "run.xml"), "w").write(xml)
+            for _ in range(reps):
+                for kind, extra in (("side_by_side", {}), ("sequential", {"ATUS_SEQUENTIAL_SCANS": "1"})):
+                    t0 = time.perf_counter()
+                    r = subprocess.run([prog, "run.xml"], cwd=tmp, env=dict(os.environ, **extra), capture_output=True,
+                                       text=True, timeout=600)
+                    times[kind].append(time.perf_counter() - t0)
+                    if r.returncode != 0:
+                        return {"error": f"{c['name']} {kind}: rc {r.returncode}: {r.stdout[-500:]} {r.stderr[-500:]}"}
+        out[c["name"]] = {"scans": c["scans"], "steps_per_scan": c["blocks"] * c["nk"],
+                          "side_by_side_s": statistics.median(times["side_by_side"]),
+                          "sequential_s": statistics.median(times["sequential"]), "all_s": times,
+                          "speedup": statistics.median(times["sequential"]) / statistics.median(times["side_by_side"])}
     return out
 
 
@@ -1030,6 +1085,21 @@ def reference_arm(args, rank, ws, dist):
     print(json.dumps(out))
 
 
+def profile_block(which):
+    """One block of 2 Strang steps on the 256^3 two-component Bragg state, no
+    warm-up: pass2_kernel launches in order FFT_z, FFT_y, x kinetic (half),
+    IFFT_y, z potential, FFT_y, x kinetic, IFFT_y, z potential, FFT_y, x
+    kinetic (half), IFFT_y, IFFT_z."""
+    import torch
+
+    from atus2_b200 import PREC_FP64, PREC_MIXED
+
+    stream = torch.cuda.Stream()
+    s, ms, launches, _ = run_gpu(PREC_FP64 if which == "fp64" else PREC_MIXED, 2, 0, stream)
+    s.close()
+    print(json.dumps({"profile_block": which, "ms": ms, "launches": launches}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1043,7 +1113,15 @@ def main():
     ap.add_argument("--no-configs", action="store_true", help="skip the 1D and 2D workloads")
     ap.add_argument("--file-output", action="store_true",
                     help="also time the drop-in bragg program with output every block (async vs sync files)")
+    ap.add_argument("--phase-scans", action="store_true",
+                    help="also time the drop-in bragg program's phase scans side by side against one by one")
+    ap.add_argument("--profile-block", choices=["fp64", "mixed"],
+                    help="run one 2-step block of the 256^3 Bragg workload and exit (for profiler captures; "
+                         "the fifth pass2_kernel launch is the z potential pass)")
     args = ap.parse_args()
+    if args.profile_block:
+        profile_block(args.profile_block)
+        return
     args.warmup = max(args.warmup, 3)
     rank, ws, local, dist = dist_init()
     try:

@@ -170,3 +170,21 @@ def test_double_slit_2048_against_oracle(slit_oracle, prec, tol):
         # (measured over 10^4 steps: |drift| <= 6e-7)
         assert abs(s.particle_number(0) - n_ref) < (1e-12 if prec == PREC_FP64 else 1e-6)
     s.close()
+
+
+def test_mixed_error_after_10k_steps_256():
+    """The 256^3 Bragg workload at full length (5000 bragg_ad steps with the
+    pulse, then 5000 freeprop steps), mixed against FP64 on the GPU: the
+    measured bound of the complex64 form.  FP32 transform rounding random-
+    walks at ~2-3.5e-7 per step (3.9e-5 after 10^4 steps), so the bar is
+    5e-5 of the state and a norm drift below 1e-6; FP64 keeps the norm to
+    1e-8 (the reference's eigen-form of the 2x2 step is unitary to ~1e-10
+    per block here)."""
+    import torch
+
+    import bench
+
+    res = bench.run_accuracy3(torch.cuda.Stream())
+    assert res["mixed"]["rel_l2_vs_fp64"]["state"] < 5e-5, res
+    assert abs(res["mixed"]["norm_drift"]) < 1e-6, res
+    assert abs(res["fp64"]["norm_drift"]) < 1e-8, res
