@@ -423,81 +423,8 @@ static int kinetic_pass_rabi(atus_ctx *ctx, int half, const RabiReq &rr, double 
   return ATUS_OK;
 }
 
-// ------------------------------------------------------------------ x slabs
-// The 3D real-space half step (IFFT_y, z pass, FFT_y) acts on every x plane
-// on its own.  With ctx->slabs = S > 1 the field is cut into S slabs of
-// n0 / S planes whose three passes run on ctx->slab_streams side streams, a
-// slab starting once its predecessor's IFFT_y is done, so that the
-// FP64-bound z pass of one slab shares the SMs with the HBM-bound y passes
-// of its neighbours.  zcap / ycap cap the persistent grids (CTAs per SM) so
-// that two passes fit on an SM side by side.
-struct SlabView {
-  atus_ctx *c;
-  int64_t n0, npts;
-  int lg0;
-  void *psi[MAXC];
-  cudaStream_t st;
-  SlabView(atus_ctx *ctx, int64_t x0, int64_t nx, cudaStream_t s) : c(ctx) {
-    n0 = ctx->n[0];
-    npts = ctx->npts;
-    lg0 = ctx->lg[0];
-    st = ctx->stream;
-    const int64_t plane = ctx->n[1] * ctx->n[2];
-    for (int i = 0; i < MAXC; i++) {
-      psi[i] = ctx->psi[i];
-      if (i < ctx->ncomp) ctx->psi[i] = static_cast<char *>(ctx->psi[i]) + x0 * plane * (int64_t)ctx->csize;
-    }
-    ctx->n[0] = nx;
-    ctx->lg[0] = ilog2(nx);
-    ctx->npts = nx * plane;
-    ctx->stream = s;
-  }
-  ~SlabView() {
-    for (int i = 0; i < MAXC; i++) c->psi[i] = psi[i];
-    c->n[0] = n0;
-    c->lg[0] = lg0;
-    c->npts = npts;
-    c->stream = st;
-    c->cta_cap = 0;
-  }
-};
-
-static int potential_pass_slabs(atus_ctx *ctx, const NLArgs &nl) {
-  const int S = ctx->slabs, NS = ctx->slab_streams;
-  const int64_t nx = ctx->n[0] / S, plane = ctx->n[1] * ctx->n[2];
-  if (!ctx->slab_st[0]) {
-    for (int s = 0; s < NS; s++) CK(cudaStreamCreateWithFlags(&ctx->slab_st[s], cudaStreamNonBlocking));
-    for (int e = 0; e < 1 + S + NS; e++) CK(cudaEventCreateWithFlags(&ctx->slab_ev[e], cudaEventDisableTiming));
-  }
-  cudaEvent_t *const ev_in = &ctx->slab_ev[0], *const ev_y = &ctx->slab_ev[1], *const ev_out = &ctx->slab_ev[1 + S];
-  CK(cudaEventRecord(*ev_in, ctx->stream));
-  for (int s = 0; s < NS; s++) CK(cudaStreamWaitEvent(ctx->slab_st[s], *ev_in, 0));
-  for (int k = 0; k < S; k++) {
-    cudaStream_t st = ctx->slab_st[k % NS];
-    if (k > 0 && NS > 1) CK(cudaStreamWaitEvent(st, ev_y[k - 1], 0));
-    NLArgs sl = nl;
-    sl.shift0 = nl.shift0 - (int)(k * nx);
-    for (int c = 0; c < MAXC; c++)
-      if (sl.V[c]) sl.V[c] += k * nx * plane;
-    SlabView v(ctx, k * nx, nx, st);
-    ctx->cta_cap = ctx->ycap;
-    RUN(run_pass(ctx, 1, T_INV, OP_NONE, T_NONE, nullptr, 0));
-    CK(cudaEventRecord(ev_y[k], st));
-    ctx->cta_cap = ctx->zcap;
-    RUN(run_pass(ctx, 2, T_INV, OP_NL, T_FWD, &sl, 0));
-    ctx->cta_cap = ctx->ycap;
-    RUN(run_pass(ctx, 1, T_FWD, OP_NONE, T_NONE, nullptr, 0));
-  }
-  for (int s = 0; s < NS; s++) {
-    CK(cudaEventRecord(ev_out[s], ctx->slab_st[s]));
-    CK(cudaStreamWaitEvent(ctx->stream, ev_out[s], 0));
-  }
-  return ATUS_OK;
-}
-
 // Real-space potential pass: 2D one pass over rows; 3D inverse y, rows, forward y.
 static int potential_pass(atus_ctx *ctx, const NLArgs &nl) {
-  if (ctx->dim == 3 && ctx->slabs > 1) return potential_pass_slabs(ctx, nl);
   const int last = ctx->dim - 1;
   if (ctx->dim == 3) RUN(run_pass(ctx, 1, T_INV, OP_NONE, T_NONE, nullptr, 0));
   RUN(run_pass(ctx, last, T_INV, OP_NL, T_FWD, &nl, 0));
@@ -642,20 +569,6 @@ int atus_create(const atus_grid *grid, int ncomp, int precision, atus_ctx **out)
     // ATUS_PASS2=0: tile kernel only (A/B comparisons of the two pass kernels)
     const char *p2 = getenv("ATUS_PASS2");
     ctx->use_pass2 = !(p2 && p2[0] == '0');
-    // x slabs of the 3D real-space half step: ATUS_SLABS=S (power of two),
-    // ATUS_SLAB_STREAMS (1..4), ATUS_ZCAP / ATUS_YCAP (CTAs per SM, 0: all)
-    auto env_int = [](const char *k, int dflt) {
-      const char *v = getenv(k);
-      return v ? atoi(v) : dflt;
-    };
-    ctx->slabs = env_int("ATUS_SLABS", 1);
-    ctx->slab_streams = env_int("ATUS_SLAB_STREAMS", 2);
-    ctx->zcap = env_int("ATUS_ZCAP", 0);
-    ctx->ycap = env_int("ATUS_YCAP", 0);
-    if (ctx->slab_streams < 1 || ctx->slab_streams > 4) ctx->slab_streams = 2;
-    if (ctx->slabs < 1 || ctx->slabs > 16 || (ctx->slabs & (ctx->slabs - 1)) != 0 || grid->dim != 3 ||
-        ctx->n[0] % ctx->slabs != 0)
-      ctx->slabs = 1;
   }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) { delete ctx; return ATUS_E_CUDA; }
@@ -747,10 +660,6 @@ void atus_destroy(atus_ctx *ctx) {
   if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
   cudaFree(ctx->fs_tw);
   cudaFree(ctx->fs_tmp);
-  for (int i = 0; i < 4; i++)
-    if (ctx->slab_st[i]) cudaStreamDestroy(ctx->slab_st[i]);
-  for (int i = 0; i < 24; i++)
-    if (ctx->slab_ev[i]) cudaEventDestroy(ctx->slab_ev[i]);
   cudaFree(ctx->scratch);
   cudaFree(ctx->sob_dev);
   if (ctx->sob_graph) cudaGraphExecDestroy(ctx->sob_graph);

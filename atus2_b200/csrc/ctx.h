@@ -51,11 +51,6 @@ struct atus_ctx {
   int64_t fs_n1 = 0, fs_n2 = 0;
   double2 *fs_tw = nullptr;
   void *fs_tmp = nullptr;
-  // 3D real-space half step over x slabs on side streams (see capi.cu)
-  int slabs = 1, slab_streams = 2, zcap = 0, ycap = 0;
-  int cta_cap = 0;                      // CTAs per SM of the next pass launches (0: all that fit)
-  cudaStream_t slab_st[4] = {};
-  cudaEvent_t slab_ev[24] = {};
   // asynchronous output snapshots
   void *snap = nullptr;                 // ncomp x N complex128 staging copy
   cudaStream_t copy_stream = nullptr;   // its device->host copies

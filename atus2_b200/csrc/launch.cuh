@@ -49,7 +49,7 @@ static inline int launch_pass_t(atus_ctx *ctx, PassArgs &a, int axis) {
   a.ncomp_grid = ctx->ncomp;
   // persistent grid: every resident CTA walks work items with stride gridDim
   const int64_t work = a.per_comp ? ntiles * ctx->ncomp : ntiles;
-  const int64_t slots = (int64_t)nsm * ((ctx->cta_cap > 0 && ctx->cta_cap < resident) ? ctx->cta_cap : resident);
+  const int64_t slots = (int64_t)nsm * resident;
   const unsigned grid = (unsigned)(work < slots ? work : slots);
   pass_kernel<R, N, TC><<<grid, Cfg::NT, smem, ctx->stream>>>(a);
   LAUNCHED(ctx);
@@ -156,7 +156,7 @@ static inline int launch_pass2_t(atus_ctx *ctx, PassArgs &a, int axis) {
   a.ntiles = ntiles;
   a.ncomp_grid = ctx->ncomp;
   const int64_t work = a.per_comp ? ntiles * ctx->ncomp : ntiles;
-  const int64_t slots = (int64_t)nsm * ((ctx->cta_cap > 0 && ctx->cta_cap < resident) ? ctx->cta_cap : resident);
+  const int64_t slots = (int64_t)nsm * resident;
   unsigned grid = (unsigned)(work < slots ? work : slots);
   if (MODE == M2_KIN_RABI && grid > RED_BLOCKS) grid = RED_BLOCKS;  // one partial row per CTA
   pass2_kernel<R, N, TC, MODE, STRIDED><<<grid, Cfg::NT, smem, ctx->stream>>>(a);
