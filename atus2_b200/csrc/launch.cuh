@@ -4,6 +4,7 @@
 #pragma once
 #include "ctx.h"
 #include "pass2.cuh"
+#include "pass3.cuh"
 
 template <typename R, int N, int TC>
 static inline int launch_pass_t(atus_ctx *ctx, PassArgs &a, int axis) {
@@ -164,6 +165,56 @@ static inline int launch_pass2_t(atus_ctx *ctx, PassArgs &a, int axis) {
   return ATUS_OK;
 }
 
+// Launch of pass3_kernel (pencils of 512..2048 points); as launch_pass2_t.
+template <typename R, int N, int TC, int MODE, bool STRIDED>
+static inline int launch_pass3_t(atus_ctx *ctx, PassArgs &a, int axis) {
+  using Cfg = P3Cfg<R, N, TC, STRIDED>;
+  constexpr size_t smem = Cfg::smem;
+  static int resident = 0;
+  static int nsm = 0;
+  if (!resident) {
+    CK(cudaFuncSetAttribute(pass3_kernel<R, N, TC, MODE, STRIDED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)smem));
+    CK(cudaFuncSetAttribute(pass3_kernel<R, N, TC, MODE, STRIDED>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                            cudaSharedmemCarveoutMaxShared));
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, pass3_kernel<R, N, TC, MODE, STRIDED>, Cfg::NT, smem));
+    if (resident < 1) return fail(ctx, ATUS_E_UNSUPPORTED, "pass kernel does not fit on an SM");
+  }
+  int64_t sa = 1;
+  for (int b = axis + 1; b < 3; b++) sa *= ctx->n[b];
+  if ((sa > 1) != STRIDED) return ATUS_E_UNSUPPORTED;
+  a.sa = sa;
+  int64_t ntiles;
+  if (sa > 1) {
+    a.inner_tiles = (sa + Cfg::B - 1) / Cfg::B;
+    ntiles = (ctx->npts / (N * sa)) * a.inner_tiles;
+    a.npencils = 0;
+  } else {
+    a.inner_tiles = 1;
+    a.npencils = ctx->npts / N;
+    ntiles = (a.npencils + Cfg::B - 1) / Cfg::B;
+  }
+  a.x_along = (axis == 0);
+  a.axis = axis;
+  a.g = geo(ctx);
+  a.tw = (sizeof(R) == 8) ? ctx->tw64 : ctx->tw;
+  for (int ax = 0; ax < 3; ax++) {
+    a.dk[ax] = ctx->dk[ax];
+    a.n[ax] = (int)ctx->n[ax];
+  }
+  a.ntiles = ntiles;
+  a.ncomp_grid = ctx->ncomp;
+  const int64_t work = a.per_comp ? ntiles * ctx->ncomp : ntiles;
+  const int64_t slots = (int64_t)nsm * resident;
+  const unsigned grid = (unsigned)(work < slots ? work : slots);
+  pass3_kernel<R, N, TC, MODE, STRIDED><<<grid, Cfg::NT, smem, ctx->stream>>>(a);
+  LAUNCHED(ctx);
+  return ATUS_OK;
+}
+
 template <typename R, int TC, int MODE, bool STRIDED>
 static inline int launch_pass2_n(atus_ctx *ctx, PassArgs &a, int axis) {
   switch (ctx->n[axis]) {
@@ -171,7 +222,16 @@ static inline int launch_pass2_n(atus_ctx *ctx, PassArgs &a, int axis) {
     case 64: return launch_pass2_t<R, 64, TC, MODE, STRIDED>(ctx, a, axis);
     case 128: return launch_pass2_t<R, 128, TC, MODE, STRIDED>(ctx, a, axis);
     case 256: return launch_pass2_t<R, 256, TC, MODE, STRIDED>(ctx, a, axis);
-    default: return ATUS_E_UNSUPPORTED;
+    default: break;
   }
+  if constexpr (MODE != M2_KIN_RABI) {
+    switch (ctx->n[axis]) {
+      case 512: return launch_pass3_t<R, 512, TC, MODE, STRIDED>(ctx, a, axis);
+      case 1024: return launch_pass3_t<R, 1024, TC, MODE, STRIDED>(ctx, a, axis);
+      case 2048: return launch_pass3_t<R, 2048, TC, MODE, STRIDED>(ctx, a, axis);
+      default: break;
+    }
+  }
+  return ATUS_E_UNSUPPORTED;
 }
 

@@ -263,7 +263,7 @@ def test_field_transform_matches_oracle(dim, n):
 
 
 @pytest.mark.parametrize("n,prec,tol", [(16384, PREC_FP64, FP64_TOL), (131072, PREC_FP64, FP64_TOL),
-                                        (16384, PREC_MIXED, MIXED_TOL)])
+                                        (1048576, PREC_FP64, FP64_TOL), (16384, PREC_MIXED, MIXED_TOL)])
 def test_long_1d_matches_oracle(n, prec, tol):
     """1D grids longer than one pass (four-step transforms over an n1 x n2
     view with exact W_N twiddles): a two-state Bragg pulse then free steps
@@ -349,10 +349,17 @@ def _run_cfg(h, ncomp, prec, psis, kind, nsteps, V=None, laser=None, F=None):
     ([64, 32, 256], 3, KIND_NL),         # three components: potential pass on the tile kernel
     ([128, 64, 32], 3, KIND_DOUBLE_BRAGG_AD),
     ([64, 32, 128], 4, KIND_BRAGG_DS_AD),
+    ([512, 1024], 2, KIND_BRAGG_AD),     # three-stage passes: strided 512 kinetic, contiguous 1024 potential
+    ([2048, 64], 1, KIND_NL),            # strided 2048-point kinetic pass
+    ([64, 2048], 1, KIND_NL),            # contiguous 2048-point potential pass, one component
+    ([16, 512, 2048], 2, KIND_BRAGG_AD), # strided 512-point transforms, contiguous 2048 with two components
 ])
 def test_register_staged_passes_match_tile_kernel(prec, shape, ncomp, kind, monkeypatch):
-    """The register-staged pass kernel and the shared-memory tile kernel run
-    the same Stockham stages, so whole Strang blocks agree to rounding."""
+    """The register-staged pass kernels and the shared-memory tile kernel
+    agree to rounding over whole Strang blocks: to 1e-13 for pencils of up
+    to 256 points (the same Stockham stages in the same order), to 1e-12 for
+    512..2048 (three register stages 16 x 16 x R3 against the tile kernel's
+    radix sequence: other roundings)."""
     h = _grid(len(shape), shape, 16.0)
     xs = _coords(h)
     r2 = sum(x * x for x in xs)
@@ -368,7 +375,8 @@ def test_register_staged_passes_match_tile_kernel(prec, shape, ncomp, kind, monk
         res.append(_run_cfg(h, ncomp, prec, psis, kind, 12, V, laser, F))
     err = np.linalg.norm(np.stack(res[0]) - np.stack(res[1])) / np.linalg.norm(np.stack(res[1]))
     print(f"register-staged vs tile kernel: rel L2 {err:.3e}")
-    state_close(res[0], res[1], 1e-13 if prec == PREC_FP64 else 1e-5)
+    tol64 = 1e-13 if max(shape) <= 256 else 1e-12
+    state_close(res[0], res[1], tol64 if prec == PREC_FP64 else 1e-5)
 
 
 def test_register_staged_sobolev_matches_tile_kernel(monkeypatch):
