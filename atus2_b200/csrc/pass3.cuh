@@ -27,14 +27,18 @@ template <typename R> struct Tile3;
 template <> struct Tile3<double> { static constexpr int NT = 128; };
 template <> struct Tile3<float> { static constexpr int NT = 256; };
 
-// Strided tiles hold at least 4 adjacent pencils, so that a warp's loads
-// cover 64-byte (FP64) or 32-byte (complex64) runs of a row, not single values.
+// Strided tiles hold 8 adjacent pencils, so that a warp's loads cover
+// 64-byte (complex64) or 128-byte (FP64) runs of a row; FP64 2048-point
+// pencils take 4 (512 threads of 16 complex128 values fill the register
+// file).  Measured on the 2048^2 complex64 x pass: 4 -> 8 pencils 0.072 ->
+// 0.050 ms.
 template <typename R, int N, int TC, bool STRIDED>
 struct P3Cfg {
   static constexpr int M = N / 16;   // stage-1 butterflies: threads per pencil-component
   static constexpr int R3 = M / 16;  // radix of stage 3
   static constexpr int T3 = 16 / R3; // stage-3 butterflies per thread
-  static constexpr int NT_MIN = M * TC * (STRIDED ? 4 : 1);
+  static constexpr int BMIN = STRIDED ? ((sizeof(R) == 8 && M * TC * 8 > 512) ? 4 : 8) : 1;
+  static constexpr int NT_MIN = M * TC * BMIN;
   static constexpr int NT = (NT_MIN > Tile3<R>::NT) ? NT_MIN : Tile3<R>::NT;
   static constexpr int NPC = NT / M; // pencil-components per tile
   static constexpr int B = NPC / TC; // pencils per tile
