@@ -102,11 +102,22 @@ __global__ void __launch_bounds__(NT) batch1d_kernel(const BInst1 *__restrict__ 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *const s = reinterpret_cast<C *>(smem_raw);
   const typename TwTab<R>::type *tw = (const typename TwTab<R>::type *)twv;
+  // the instance's Bragg parameters live in shared memory (thread 0 sets the
+  // step's time and pulse amplitude): a per-thread copy of the ~0.5 KB block
+  // sat in local memory
+  __shared__ NLArgs s_nl;
+  const NLArgs &nl = s_nl;
   for (int k = blockIdx.x; k < ninst; k += gridDim.x) {
     const int id = order[k];
     const BInst1 &in = insts[id];
     C *fld[2] = {(C *)in.psi[0], (C *)in.psi[1]};
-    NLArgs nl = in.nl;
+    {
+      static_assert(sizeof(NLArgs) % 8 == 0, "NLArgs is copied in 8-byte words");
+      const unsigned long long *src = reinterpret_cast<const unsigned long long *>(&in.nl);
+      unsigned long long *dst = reinterpret_cast<unsigned long long *>(&s_nl);
+      for (int e = threadIdx.x; e < (int)(sizeof(NLArgs) / 8); e += NT) dst[e] = src[e];
+    }
+    __syncthreads();
     const double dt = nl.dt;
     double t = t0[id];
     if constexpr (RES == 2) {
@@ -117,8 +128,11 @@ __global__ void __launch_bounds__(NT) batch1d_kernel(const BInst1 *__restrict__ 
       b1_kinetic<R, N, NT>(s + NP, tw, in.kh, in.s_f, in.s_b);
       t += 0.5 * dt;
       for (int j = 0; j < nk; j++) {
-        nl.t1 = t + 0.5 * dt;
-        nl.F = pulse_at(in.pulse, nl.t1);
+        if (threadIdx.x == 0) {
+          s_nl.t1 = t + 0.5 * dt;
+          s_nl.F = pulse_at(in.pulse, s_nl.t1);
+        }
+        __syncthreads();
         for (int i = threadIdx.x; i < N; i += NT) {
           const double x0 = (double)(i - nl.shift0) * nl.dx0;
           double om, ec, es;
@@ -153,8 +167,11 @@ __global__ void __launch_bounds__(NT) batch1d_kernel(const BInst1 *__restrict__ 
       b1_kinetic<R, N, NT>(s, tw, in.kh, in.s_f, in.s_b);
       t += 0.5 * dt;
       for (int j = 0; j < nk; j++) {
-        nl.t1 = t + 0.5 * dt;
-        nl.F = pulse_at(in.pulse, nl.t1);
+        if (threadIdx.x == 0) {
+          s_nl.t1 = t + 0.5 * dt;
+          s_nl.F = pulse_at(in.pulse, s_nl.t1);
+        }
+        __syncthreads();
         C *other = fld[rc ^ 1];
         for (int i = threadIdx.x; i < N; i += NT) {
           const double x0 = (double)(i - nl.shift0) * nl.dx0;
