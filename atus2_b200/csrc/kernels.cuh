@@ -907,10 +907,17 @@ __global__ void __launch_bounds__(BLOCK1D_NT) block1d_kernel(Block1DArgs a) {
   kin_1d<R, N, TC>(s, kh, nc, a.s_f, a.s_b);
   fft_tile<R, N, TC, NT, +1, TWN>(s, tw);
   t += 0.5 * dt;
-  NLArgs nl = a.nl;
+  // the step parameters in shared memory (thread 0 sets the step's time and
+  // pulse amplitude): a per-thread copy of the ~0.5 KB block sat in local memory
+  __shared__ NLArgs s_nl;
+  const NLArgs &nl = s_nl;
+  if (threadIdx.x == 0) s_nl = a.nl;
   for (int j = 0; j < a.nk; j++) {
-    nl.t1 = t + 0.5 * dt;
-    nl.F = a.F ? a.F[j] : 1.0;
+    if (threadIdx.x == 0) {
+      s_nl.t1 = t + 0.5 * dt;
+      s_nl.F = a.F ? a.F[j] : 1.0;
+    }
+    __syncthreads();
     for (int i = threadIdx.x; i < N; i += NT) {
       const double x0 = (double)(i - nl.shift0) * nl.dx0;
       double om = 0, ec = 1, es = 0;
