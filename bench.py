@@ -1109,16 +1109,34 @@ def reference_arm(args, rank, ws, dist):
 
 
 def profile_block(which):
-    """One block of 2 Strang steps on the 256^3 two-component Bragg state, no
-    warm-up: pass2_kernel launches in order FFT_z, FFT_y, x kinetic (half),
-    IFFT_y, z potential, FFT_y, x kinetic, IFFT_y, z potential, FFT_y, x
-    kinetic (half), IFFT_y, IFFT_z."""
+    """fp64 / mixed: one block of 2 Strang steps on the 256^3 two-component
+    Bragg state, no warm-up: pass2_kernel launches in order FFT_z, FFT_y, x
+    kinetic (half), IFFT_y, z potential, FFT_y, x kinetic, IFFT_y, z
+    potential, FFT_y, x kinetic (half), IFFT_y, IFFT_z.  rt1d: one block of
+    1000 steps of the 1D rt_solver workload (one block1d_kernel launch)."""
     import torch
 
-    from atus2_b200 import PREC_FP64, PREC_MIXED
+    from atus2_b200 import PREC_FP64, PREC_MIXED, STEP_NL, Solver
 
     stream = torch.cuda.Stream()
-    s, ms, launches, _ = run_gpu(PREC_FP64 if which == "fp64" else PREC_MIXED, 2, 0, stream)
+    if which == "rt1d":
+        # one 1000-step block of the 1D rt_solver workload: one block1d_kernel launch
+        h, psi, V = config1_inputs()
+        s = Solver(h, 1, PREC_FP64)
+        s.set_stream(stream.cuda_stream)
+        s.set_psi(0, psi)
+        s.set_alpha(0, [0.5])
+        s.set_gs([10.0])
+        s.set_potential(0, V)
+        s.set_dt(DT)
+        torch.cuda.synchronize()
+        l0 = s.launches
+        t0 = time.perf_counter()
+        s.block(C1_NK, STEP_NL)
+        s.synchronize()
+        ms, launches = (time.perf_counter() - t0) * 1e3, s.launches - l0
+    else:
+        s, ms, launches, _ = run_gpu(PREC_FP64 if which == "fp64" else PREC_MIXED, 2, 0, stream)
     s.close()
     print(json.dumps({"profile_block": which, "ms": ms, "launches": launches}))
 
@@ -1138,9 +1156,10 @@ def main():
                     help="also time the drop-in bragg program with output every block (async vs sync files)")
     ap.add_argument("--phase-scans", action="store_true",
                     help="also time the drop-in bragg program's phase scans side by side against one by one")
-    ap.add_argument("--profile-block", choices=["fp64", "mixed"],
-                    help="run one 2-step block of the 256^3 Bragg workload and exit (for profiler captures; "
-                         "the fifth pass2_kernel launch is the z potential pass)")
+    ap.add_argument("--profile-block", choices=["fp64", "mixed", "rt1d"],
+                    help="run one 2-step block of the 256^3 Bragg workload (fp64, mixed; the fifth "
+                         "pass2_kernel launch is the z potential pass) or one 1000-step block of the 1D "
+                         "rt_solver workload (rt1d) and exit -- for profiler captures")
     args = ap.parse_args()
     if args.profile_block:
         profile_block(args.profile_block)
