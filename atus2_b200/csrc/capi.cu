@@ -569,6 +569,9 @@ int atus_create(const atus_grid *grid, int ncomp, int precision, atus_ctx **out)
     // ATUS_PASS2=0: tile kernel only (A/B comparisons of the two pass kernels)
     const char *p2 = getenv("ATUS_PASS2");
     ctx->use_pass2 = !(p2 && p2[0] == '0');
+    // ATUS_CLUSTER1D=0: 1D blocks on one CTA only (A/B comparisons)
+    const char *c1 = getenv("ATUS_CLUSTER1D");
+    ctx->use_cluster1d = !(c1 && c1[0] == '0');
   }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) { delete ctx; return ATUS_E_CUDA; }
@@ -768,6 +771,7 @@ int atus_clone(const atus_ctx *src, atus_ctx **out) {
   ctx->win_dur[1] = src->win_dur[1];
   ctx->bragg_stable = src->bragg_stable;
   ctx->use_pass2 = src->use_pass2;
+  ctx->use_cluster1d = src->use_cluster1d;
   int e = ATUS_OK;
   auto copy = [&](void *dst, const void *from, size_t bytes) {
     if (e == ATUS_OK && cudaMemcpyAsync(dst, from, bytes, cudaMemcpyDeviceToDevice, ctx->stream) != cudaSuccess)
@@ -1046,7 +1050,8 @@ static int strang_block(atus_ctx *ctx, int nk, int kind, const double *F, const 
   // shared memory of the resident 1D kernel (padded pencils, Pad<N>)
   const int64_t n0 = ctx->n[0];
   const int64_t np1d = ((n0 >= 16) ? (n0 + n0 / 16) : n0) | 1;
-  const bool fits1d = (int64_t)ctx->csize * tc_for(ctx->ncomp) * np1d <= 227 * 1024;
+  const bool on_cluster = ctx->use_cluster1d && n0 >= 2048 && n0 <= 8192;  // cluster1d.cuh
+  const bool fits1d = on_cluster || (int64_t)ctx->csize * tc_for(ctx->ncomp) * np1d <= 227 * 1024;
   if (ctx->dim == 1 && (ctx->ncomp > 2 || kind == K_NUM_BRAGG || ctx->fs_tw || !fits1d)) {
     // more components or points than the resident 1D kernel holds, or a step
     // that reads the header time itself: per step one kinetic pass (FFT,

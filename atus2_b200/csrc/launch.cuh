@@ -3,6 +3,7 @@
 // combination, so the kernels compile in parallel.
 #pragma once
 #include "ctx.h"
+#include "cluster1d.cuh"
 #include "pass2.cuh"
 #include "pass3.cuh"
 
@@ -91,8 +92,30 @@ static inline int launch_block1d_t(atus_ctx *ctx, Block1DArgs &a) {
   return ATUS_OK;
 }
 
+// A 1D block on one cluster of 8 CTAs (cluster1d.cuh).
+template <typename R, int N, int TC>
+static inline int launch_cluster1d_t(atus_ctx *ctx, Block1DArgs &a) {
+  using Cfg = C1Cfg<R, N, TC>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    CK(cudaFuncSetAttribute(cluster1d_kernel<R, N, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::smem));
+    attr_set = true;
+  }
+  cluster1d_kernel<R, N, TC><<<Cfg::C, Cfg::NT, Cfg::smem, ctx->stream>>>(a);
+  LAUNCHED(ctx);
+  return ATUS_OK;
+}
+
 template <typename R, int TC>
 static inline int launch_block1d_n(atus_ctx *ctx, Block1DArgs &a) {
+  if (ctx->use_cluster1d) {
+    switch (ctx->n[0]) {
+      case 2048: return launch_cluster1d_t<R, 2048, TC>(ctx, a);
+      case 4096: return launch_cluster1d_t<R, 4096, TC>(ctx, a);
+      case 8192: return launch_cluster1d_t<R, 8192, TC>(ctx, a);
+      default: break;
+    }
+  }
   switch (ctx->n[0]) {
     case 2: return launch_block1d_t<R, 2, TC>(ctx, a);
     case 4: return launch_block1d_t<R, 4, TC>(ctx, a);

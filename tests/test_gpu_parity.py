@@ -295,6 +295,38 @@ def test_long_1d_matches_oracle(n, prec, tol):
     np.testing.assert_allclose(s.rabi_integrals(k0, 1.0, 1), o.rabi_integrals(k0, 1.0, 1), rtol=q, atol=1e-14)
 
 
+@pytest.mark.parametrize("prec,tol", [(PREC_FP64, FP64_TOL), (PREC_MIXED, MIXED_TOL)])
+@pytest.mark.parametrize("n,ncomp,kind", [(2048, 1, KIND_NL), (4096, 2, KIND_BRAGG_AD), (8192, 2, KIND_BRAGG_AD),
+                                          (8192, 1, KIND_NL)])
+def test_cluster_1d_block_matches_oracle(n, ncomp, kind, prec, tol):
+    """1D Strang blocks of 2048..8192 points run on one cluster of 8 CTAs
+    that exchange through distributed shared memory: 3 blocks of 50 steps
+    (a Bragg pulse, or a harmonic potential with g = 20) against the oracle,
+    and the particle numbers."""
+    h = _grid(1, [n], n / 64.0)
+    (x,) = _coords(h)
+    psi0 = np.exp(-x * x / 16.0 + 0.5j * x).astype(np.complex128)
+    psi0 /= math.sqrt(float(h["dx"]) * np.sum(np.abs(psi0) ** 2))
+    psis = [psi0] + [np.zeros_like(psi0)] * (ncomp - 1)
+    gs = [20.0, 15.0, 15.0, 18.0][: ncomp * ncomp] if ncomp == 2 else [20.0]
+    V = 0.02 * x * x if kind == KIND_NL else None
+    o, s = _setup_pair(h, ncomp, psis, [0.5], gs, V, 1e-3, prec)
+    kw = dict(beta=[0.2, 0, 0], DeltaL=[0, 0.5, 0, 0], Amp=[3.0, 3.0], laser_k=[4.0, 0], laser_dk=[0.3, 0],
+              laser_domh=[4.0, 0], phase=[0, 0], chirp_rate=[0, 0], chirp=0.0)
+    Lo, Ls = (OLaser.make(**kw), Laser.make(**kw)) if kind == KIND_BRAGG_AD else (None, None)
+    F = np.full(50, 0.9) if kind == KIND_BRAGG_AD else None
+    for _ in range(3):
+        o.block(50, kind, Lo, F)
+        s.block(50, kind, Ls, F)
+    assert s.t == o.t
+    state_close([s.psi(c) for c in range(ncomp)], [o.psi(c) for c in range(ncomp)], tol)
+    if ncomp == 2:
+        assert o.particle_number(1) > 1e-3
+    q = 1e-11 if prec == PREC_FP64 else 1e-5
+    for c in range(ncomp):
+        np.testing.assert_allclose(s.particle_number(c), o.particle_number(c), rtol=q, atol=1e-14)
+
+
 def test_sobmin_mu_matches_oracle():
     h = _grid(3, [32, 32, 16], 12.0)
     x, y, z = _coords(h)
