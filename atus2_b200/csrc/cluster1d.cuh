@@ -27,9 +27,12 @@
 
 namespace atus {
 
+// CTAs of the cluster (8: the portable cluster size)
+#define ATUS_C1_CLUSTER 8
+
 template <typename R, int N, int TC>
 struct C1Cfg {
-  static constexpr int C = 8;          // CTAs of the cluster
+  static constexpr int C = ATUS_C1_CLUSTER;
   static constexpr int P = N / C;      // points of a bin pencil
   static constexpr int PC = P / C;     // columns of a CTA
   static constexpr int NT = 256;
@@ -108,7 +111,7 @@ __device__ __forceinline__ void c1_kinetic(cooperative_groups::cluster_group &cl
 }
 
 template <typename R, int N, int TC>
-__global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(256, 1) cluster1d_kernel(Block1DArgs a) {
+__global__ void __cluster_dims__(ATUS_C1_CLUSTER, 1, 1) __launch_bounds__(256, 1) cluster1d_kernel(Block1DArgs a) {
   using C_ = cplx<R>;
   using Cfg = C1Cfg<R, N, TC>;
   constexpr int C = Cfg::C, P = Cfg::P, PC = Cfg::PC, NT = Cfg::NT;

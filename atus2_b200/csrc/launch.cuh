@@ -99,6 +99,7 @@ static inline int launch_cluster1d_t(atus_ctx *ctx, Block1DArgs &a) {
   static bool attr_set = false;
   if (!attr_set) {
     CK(cudaFuncSetAttribute(cluster1d_kernel<R, N, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::smem));
+    if (Cfg::C > 8) CK(cudaFuncSetAttribute(cluster1d_kernel<R, N, TC>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     attr_set = true;
   }
   cluster1d_kernel<R, N, TC><<<Cfg::C, Cfg::NT, Cfg::smem, ctx->stream>>>(a);
