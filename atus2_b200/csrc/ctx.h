@@ -34,7 +34,7 @@ struct atus_ctx {
   cudaStream_t own_stream = nullptr, stream = nullptr;
   int64_t launches = 0;
   bool use_pass2 = true;        // register-staged passes for pencils of 32..256 points
-  bool use_cluster1d = true;    // 1D blocks of 2048..8192 points on an 8-CTA cluster
+  bool use_cluster1d = true;    // 1D blocks of 2048..8192 points on a 16-CTA cluster
   int bragg_stable = 0;         // FP64 Bragg step in the eigenvalue-free form
   std::string err;
   // Sobolev state

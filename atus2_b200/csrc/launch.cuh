@@ -92,7 +92,7 @@ static inline int launch_block1d_t(atus_ctx *ctx, Block1DArgs &a) {
   return ATUS_OK;
 }
 
-// A 1D block on one cluster of 8 CTAs (cluster1d.cuh).
+// A 1D block on one cluster of CTAs (cluster1d.cuh).
 template <typename R, int N, int TC>
 static inline int launch_cluster1d_t(atus_ctx *ctx, Block1DArgs &a) {
   using Cfg = C1Cfg<R, N, TC>;

@@ -299,7 +299,7 @@ def test_long_1d_matches_oracle(n, prec, tol):
 @pytest.mark.parametrize("n,ncomp,kind", [(2048, 1, KIND_NL), (4096, 2, KIND_BRAGG_AD), (8192, 2, KIND_BRAGG_AD),
                                           (8192, 1, KIND_NL)])
 def test_cluster_1d_block_matches_oracle(n, ncomp, kind, prec, tol):
-    """1D Strang blocks of 2048..8192 points run on one cluster of 8 CTAs
+    """1D Strang blocks of 2048..8192 points run on one cluster of 16 CTAs
     that exchange through distributed shared memory: 3 blocks of 50 steps
     (a Bragg pulse, or a harmonic potential with g = 20) against the oracle,
     and the particle numbers."""
