@@ -795,7 +795,7 @@ def run_output_overlap(blocks=4, nk=1000, reps=3):
     return out
 
 
-def run_phase_scans(reps=3):
+def run_phase_scans(reps=5):
     """ATUS-2's bragg program on the drop-in headers with a phase scan
     (no_of_chirps scans of a bragg_ad sequence, chirp_mode 1, Rabi sums every
     block): scans 1..n-1 side by side on cloned contexts (the default)
@@ -806,8 +806,8 @@ def run_phase_scans(reps=3):
         return {"unavailable": "host/bin/bragg is not built (needs the ATUS-2 source tree at build time)"}
     from atus2_b200 import binfmt
 
-    cases = [dict(name="1D-4096", dim=1, n=[4096], L=[128.0], scans=16, nk=100, blocks=4),
-             dict(name="2D-512", dim=2, n=[512, 512], L=[32.0, 32.0], scans=8, nk=100, blocks=2)]
+    cases = [dict(name="1D-4096", dim=1, n=[4096], L=[128.0], scans=16, nk=400, blocks=10),
+             dict(name="2D-512", dim=2, n=[512, 512], L=[32.0, 32.0], scans=8, nk=200, blocks=5)]
     out = {}
     for c in cases:
         dim = c["dim"]
@@ -844,6 +844,7 @@ def run_phase_scans(reps=3):
         out[c["name"]] = {"scans": c["scans"], "steps_per_scan": c["blocks"] * c["nk"],
                           "side_by_side_s": statistics.median(times["side_by_side"]),
                           "sequential_s": statistics.median(times["sequential"]), "all_s": times,
+                          "min_s": {k: min(v) for k, v in times.items()},
                           "speedup": statistics.median(times["sequential"]) / statistics.median(times["side_by_side"])}
     return out
 
@@ -1024,6 +1025,7 @@ def time_ref_sobmin(wy, wz, g, seconds=15.0):
         return None
     from atus2_b200 import guess
 
+    wy, wz, g = float(wy), float(wz), float(g)  # plain floats: numpy scalars repr as np.float64(...)
     cores = os.cpu_count() or 1
     h = guess.header(SOB_N)
     V = guess.potential(h, wy, wz)
