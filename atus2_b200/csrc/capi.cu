@@ -572,6 +572,9 @@ int atus_create(const atus_grid *grid, int ncomp, int precision, atus_ctx **out)
     // ATUS_CLUSTER1D=0: 1D blocks on one CTA only (A/B comparisons)
     const char *c1 = getenv("ATUS_CLUSTER1D");
     ctx->use_cluster1d = !(c1 && c1[0] == '0');
+    // ATUS_TMA=1: strided 256-point passes fed by TMA tile copies
+    const char *tm = getenv("ATUS_TMA");
+    ctx->use_tma = (tm && tm[0] == '1');
   }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) { delete ctx; return ATUS_E_CUDA; }
@@ -583,6 +586,7 @@ int atus_create(const atus_grid *grid, int ncomp, int precision, atus_ctx **out)
     if (ok) ok = cudaMemset(ctx->psi[c], 0, ctx->csize * ctx->npts) == cudaSuccess;
   }
   if (ok) ok = cudaMalloc(&ctx->scratch, 16 * ctx->npts) == cudaSuccess;
+  if (ok) ok = cudaMalloc(&ctx->err_dev, sizeof(int)) == cudaSuccess && cudaMemset(ctx->err_dev, 0, sizeof(int)) == cudaSuccess;
   if (ok) ok = cudaMalloc(&ctx->red_partial, sizeof(double) * RED_BLOCKS * RED_MAXQ) == cudaSuccess;
   if (ok) ok = cudaMalloc(&ctx->red_out, sizeof(double) * RED_MAXQ) == cudaSuccess;
   if (ok) ok = cudaMallocHost(&ctx->h_red, sizeof(double) * RED_MAXQ) == cudaSuccess;
@@ -663,6 +667,7 @@ void atus_destroy(atus_ctx *ctx) {
   if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
   cudaFree(ctx->fs_tw);
   cudaFree(ctx->fs_tmp);
+  cudaFree(ctx->err_dev);
   cudaFree(ctx->scratch);
   cudaFree(ctx->sob_dev);
   if (ctx->sob_graph) cudaGraphExecDestroy(ctx->sob_graph);
@@ -772,6 +777,7 @@ int atus_clone(const atus_ctx *src, atus_ctx **out) {
   ctx->bragg_stable = src->bragg_stable;
   ctx->use_pass2 = src->use_pass2;
   ctx->use_cluster1d = src->use_cluster1d;
+  ctx->use_tma = src->use_tma;
   int e = ATUS_OK;
   auto copy = [&](void *dst, const void *from, size_t bytes) {
     if (e == ATUS_OK && cudaMemcpyAsync(dst, from, bytes, cudaMemcpyDeviceToDevice, ctx->stream) != cudaSuccess)
@@ -971,13 +977,26 @@ int atus_embed(atus_ctx *src, int comp_s, atus_ctx *dst, int comp_d) {
   return ATUS_OK;
 }
 
+// The device error word after kernels with bounded waits (the TMA-fed
+// passes): read once they are done, reset, and reported as ATUS_E_CUDA.
+static int wait_check(atus_ctx *ctx) {
+  if (!ctx->err_armed) return ATUS_OK;
+  ctx->err_armed = false;
+  int e = 0;
+  CK(cudaMemcpyAsync(&e, ctx->err_dev, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (e == 0) return ATUS_OK;
+  CK(cudaMemsetAsync(ctx->err_dev, 0, sizeof(int), ctx->stream));
+  return fail(ctx, ATUS_E_CUDA, "a TMA tile copy did not complete within the wait limit");
+}
+
 int atus_ft_step(atus_ctx *ctx, int half) {
   if (!ctx) return ATUS_E_ARG;
   RUN(transform_inner(ctx, T_FWD));
   RUN(kinetic_pass(ctx, half));
   RUN(transform_inner(ctx, T_INV));
   ctx->t += half ? 0.5 * ctx->dt : ctx->dt;
-  return ATUS_OK;
+  return wait_check(ctx);
 }
 
 static int check_kind(atus_ctx *ctx, int kind) {
@@ -1013,7 +1032,8 @@ static int strang_block(atus_ctx *ctx, int nk, int kind, const double *F, const 
                         bool *fused);
 
 int atus_strang_block(atus_ctx *ctx, int nk, int kind, const double *F) {
-  return strang_block(ctx, nk, kind, F, nullptr, nullptr, nullptr);
+  RUN(strang_block(ctx, nk, kind, F, nullptr, nullptr, nullptr));
+  return wait_check(ctx);
 }
 
 int atus_strang_block_rabi(atus_ctx *ctx, int nk, int kind, const double *F, int ncomp_r, const int *comps,
@@ -1032,6 +1052,7 @@ int atus_strang_block_rabi(atus_ctx *ctx, int nk, int kind, const double *F, int
   double sums[RED_MAXQ];
   bool fused = false;
   RUN(strang_block(ctx, nk, kind, F, &rr, sums, &fused));
+  RUN(wait_check(ctx));
   if (!fused) {  // the separate transform and reduction of compute_rabi_integrals
     for (int c = 0; c < ncomp_r; c++)
       RUN(atus_rabi_integrals_comp(ctx, comps[c], k0 + (size_t)c * n * ctx->dim, n, thr, out + c * n));

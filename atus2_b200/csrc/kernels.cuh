@@ -113,6 +113,7 @@ struct PassArgs {
   double rabi_thr;
   double rabi_k0[8][3];
   double *rabi_partial;
+  int *err;  // device error word (bounded waits that ran out set bits)
 };
 
 __device__ __forceinline__ void idx3(const Geo &g, int64_t l, int &ix, int &iy, int &iz) {

@@ -2,9 +2,12 @@
 // (inst_*.cu) includes this and exports one precision / component-count
 // combination, so the kernels compile in parallel.
 #pragma once
+#include <cstring>
+
 #include "ctx.h"
 #include "cluster1d.cuh"
 #include "pass2.cuh"
+#include "pass2_tma.cuh"
 #include "pass3.cuh"
 
 template <typename R, int N, int TC>
@@ -139,8 +142,96 @@ static inline int launch_block1d_n(atus_ctx *ctx, Block1DArgs &a) {
 // ------------------------------------------------------------ register-staged passes
 // Launch of pass2_kernel (pencils of 32..256 points); ATUS_E_UNSUPPORTED,
 // without an error message, for lengths it has no instantiation for.
+// cuTensorMapEncodeTiled from the driver (no link against libcuda).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static inline EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// Strided 256-point pass with TMA tile copies (pass2_tma.cuh); the tile and
+// launch geometry of launch_pass2_t.  ATUS_E_UNSUPPORTED (nothing launched)
+// where a tensor map cannot describe the pass.
+template <typename R, int N, int MODE>
+static inline int launch_pass2_tma_t(atus_ctx *ctx, PassArgs &a, int axis) {
+  using T = P2TmaCfg<R, N>;
+  constexpr size_t smem = T::smem;
+  EncodeTiledFn enc = encode_tiled();
+  if (!enc) return ATUS_E_UNSUPPORTED;
+  int64_t sa = 1;
+  for (int b = axis + 1; b < 3; b++) sa *= ctx->n[b];
+  const int64_t outer = ctx->npts / (N * sa);
+  if (sa < 2 || T::VPC * sa > (int64_t(1) << 31) || outer > (int64_t(1) << 31)) return ATUS_E_UNSUPPORTED;
+  static int resident = 0;
+  static int nsm = 0;
+  if (!resident) {
+    CK(cudaFuncSetAttribute(pass2_tma_kernel<R, N, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CK(cudaFuncSetAttribute(pass2_tma_kernel<R, N, MODE>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                            cudaSharedmemCarveoutMaxShared));
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, pass2_tma_kernel<R, N, MODE>, T::Cfg::NT, smem));
+    if (resident < 1) return fail(ctx, ATUS_E_UNSUPPORTED, "TMA pass kernel does not fit on an SM");
+  }
+  const int nf = a.per_comp ? ctx->ncomp : 1;
+  TmaMaps maps;
+  memset(&maps, 0, sizeof(maps));
+  for (int c = 0; c < nf; c++) {
+    // 8-byte units: {VPC sa, N, outer}, box {VPC B, N, 1}, 128-byte swizzle
+    const cuuint64_t dims[3] = {(cuuint64_t)(T::VPC * sa), (cuuint64_t)N, (cuuint64_t)outer};
+    const cuuint64_t strides[2] = {(cuuint64_t)(T::VPC * sa * 8), (cuuint64_t)(T::VPC * sa * 8 * N)};
+    const cuuint32_t box[3] = {(cuuint32_t)(T::VPC * T::B), (cuuint32_t)N, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    if (enc(&maps.m[c], CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, a.psi[c], dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return ATUS_E_UNSUPPORTED;
+  }
+  a.sa = sa;
+  a.inner_tiles = (sa + T::B - 1) / T::B;
+  const int64_t ntiles = outer * a.inner_tiles;
+  a.npencils = 0;
+  a.x_along = (axis == 0);
+  a.axis = axis;
+  a.g = geo(ctx);
+  a.tw = (sizeof(R) == 8) ? ctx->tw64 : ctx->tw;
+  for (int ax = 0; ax < 3; ax++) {
+    a.dk[ax] = ctx->dk[ax];
+    a.n[ax] = (int)ctx->n[ax];
+  }
+  a.ntiles = ntiles;
+  a.ncomp_grid = ctx->ncomp;
+  a.err = ctx->err_dev;
+  const int64_t work = ntiles * ctx->ncomp;
+  const int64_t slots = (int64_t)nsm * resident;
+  const unsigned grid = (unsigned)(work < slots ? work : slots);
+  pass2_tma_kernel<R, N, MODE><<<grid, T::Cfg::NT, smem, ctx->stream>>>(a, maps);
+  LAUNCHED(ctx);
+  ctx->err_armed = true;
+  return ATUS_OK;
+}
+
 template <typename R, int N, int TC, int MODE, bool STRIDED>
 static inline int launch_pass2_t(atus_ctx *ctx, PassArgs &a, int axis) {
+  if constexpr (STRIDED && N == 256 && TC == 1 && (MODE == M2_FWD || MODE == M2_INV || MODE == M2_KIN)) {
+    if (ctx->use_tma && a.per_comp && ctx->err_dev && ctx->npts / ctx->n[axis] >= 2) {
+      const int r = launch_pass2_tma_t<R, N, MODE>(ctx, a, axis);
+      if (r != ATUS_E_UNSUPPORTED) return r;
+    }
+  }
   using Cfg = P2Cfg<R, N, TC>;
   constexpr size_t smem = ((MODE == M2_KIN || MODE == M2_KIN_RABI) && Cfg::kin_smem) ? Cfg::smem_kin : Cfg::smem;
   static int resident = 0;

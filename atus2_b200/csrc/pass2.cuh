@@ -162,9 +162,29 @@ __device__ __forceinline__ void p2_rabi(const PassArgs &a, int ci, const int *p0
   }
 }
 
-template <typename R, int N, int TC, int MODE, bool STRIDED>
+// After-load hook of p2_item (the TMA kernel refills the tile buffer there).
+struct P2NoHook {
+  __device__ __forceinline__ void operator()() const {}
+};
+
+// Swizzled tile of a strided pass as a 128-byte-swizzled TMA box writes it:
+// row i (point i of the B pencils) is 128 bytes, its 16-byte chunk c at
+// position c ^ (i & 7).  Value of pencil b at point i.
+template <typename R>
+__device__ __forceinline__ cplx<R> p2_tile_at(const unsigned char *tile, int i, int b) {
+  if constexpr (sizeof(R) == 8)
+    return *reinterpret_cast<const cplx<R> *>(tile + i * 128 + ((b ^ (i & 7)) << 4));
+  else
+    return *reinterpret_cast<const cplx<R> *>(tile + i * 128 + (((b >> 1) ^ (i & 7)) << 4) + ((b & 1) << 3));
+}
+
+// One work item.  SMEM_TILE: the tile's inputs come from `tile` (swizzled,
+// see p2_tile_at) instead of global memory, and hook() runs once every
+// thread has taken its values.
+template <typename R, int N, int TC, int MODE, bool STRIDED, bool SMEM_TILE = false, typename Hook = P2NoHook>
 __device__ __forceinline__ void p2_item(const PassArgs &a, const TileGeo &g, unsigned char *smem_raw, bool kt_shared,
-                                        double *s_om, double *s_ec, double *s_es, double *rq = nullptr) {
+                                        double *s_om, double *s_ec, double *s_es, double *rq = nullptr,
+                                        const unsigned char *tile = nullptr, Hook hook = Hook()) {
   using C = cplx<R>;
   using TW = typename TwTab<R>::type;
   using Cfg = P2Cfg<R, N, TC>;
@@ -202,8 +222,14 @@ __device__ __forceinline__ void p2_item(const PassArgs &a, const TileGeo &g, uns
   }
 
   C v[16];
-  #pragma unroll
-  for (int r = 0; r < 16; r++) v[r] = live ? src[r * step] : mk<R>(0, 0);
+  if constexpr (SMEM_TILE) {
+    #pragma unroll
+    for (int r = 0; r < 16; r++) v[r] = p2_tile_at<R>(tile, j + R2 * r, b);
+    hook();
+  } else {
+    #pragma unroll
+    for (int r = 0; r < 16; r++) v[r] = live ? src[r * step] : mk<R>(0, 0);
+  }
 
   if constexpr (MODE == M2_FWD) {
     p2_transform<R, N, -1, !STRIDED>(v, my, twS, j);
