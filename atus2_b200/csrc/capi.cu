@@ -572,9 +572,12 @@ int atus_create(const atus_grid *grid, int ncomp, int precision, atus_ctx **out)
     // ATUS_CLUSTER1D=0: 1D blocks on one CTA only (A/B comparisons)
     const char *c1 = getenv("ATUS_CLUSTER1D");
     ctx->use_cluster1d = !(c1 && c1[0] == '0');
-    // ATUS_TMA=1: strided 256-point passes fed by TMA tile copies
+    // ATUS_TMA=0: strided 256-point passes load their tiles themselves (no TMA)
     const char *tm = getenv("ATUS_TMA");
-    ctx->use_tma = (tm && tm[0] == '1');
+    ctx->use_tma = !(tm && tm[0] == '0');
+    // ATUS_BULK_NL=1: contiguous 256-point potential passes fed by bulk copies
+    const char *bn = getenv("ATUS_BULK_NL");
+    ctx->use_bulk_nl = (bn && bn[0] == '1');
   }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) { delete ctx; return ATUS_E_CUDA; }
@@ -778,6 +781,7 @@ int atus_clone(const atus_ctx *src, atus_ctx **out) {
   ctx->use_pass2 = src->use_pass2;
   ctx->use_cluster1d = src->use_cluster1d;
   ctx->use_tma = src->use_tma;
+  ctx->use_bulk_nl = src->use_bulk_nl;
   int e = ATUS_OK;
   auto copy = [&](void *dst, const void *from, size_t bytes) {
     if (e == ATUS_OK && cudaMemcpyAsync(dst, from, bytes, cudaMemcpyDeviceToDevice, ctx->stream) != cudaSuccess)

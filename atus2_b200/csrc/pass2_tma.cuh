@@ -52,6 +52,14 @@ __device__ __forceinline__ void tma_load_3d(unsigned dst, const CUtensorMap *map
       : "memory");
 }
 
+// Bulk copy of `bytes` contiguous bytes (16-byte aligned, a multiple of 16)
+// into shared memory at dst, completing on mbar.
+__device__ __forceinline__ void bulk_load(unsigned dst, const void *src, unsigned bytes, unsigned mbar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(reinterpret_cast<unsigned long long>(src)), "r"(bytes), "r"(mbar)
+               : "memory");
+}
+
 template <typename R, int N>
 struct P2TmaCfg {
   using Cfg = P2Cfg<R, N, 1>;
@@ -111,6 +119,72 @@ __global__ void __launch_bounds__(Tile2<R>::NT, 3) pass2_tma_kernel(PassArgs a, 
     };
     p2_item<R, N, 1, MODE, true, true>(a, tile_geo<B, N>(a, w), rest, false, s_om, s_ec, s_es, nullptr, tile,
                                        refill);
+  }
+}
+
+// Contiguous-axis potential pass (IFFT, potential step, FFT along the last
+// axis, TC components per tile) with each tile -- B whole pencils of every
+// component, contiguous in memory -- brought in by TC bulk copies on an
+// mbarrier; the next tile's copies are issued once the current one is in
+// registers.
+template <typename R, int N, int TC>
+struct P2BulkCfg {
+  using Cfg = P2Cfg<R, N, TC>;
+  static constexpr int B = Cfg::B;
+  static constexpr unsigned TILE_BYTES = (unsigned)(TC * B * N * sizeof(cplx<R>));
+  static constexpr size_t smem = 128 + TILE_BYTES + Cfg::smem;
+};
+
+template <typename R, int N, int TC>
+__global__ void __launch_bounds__(Tile2<R>::NT, 3) pass2_bulk_nl_kernel(PassArgs a) {
+  using T = P2BulkCfg<R, N, TC>;
+  using C = cplx<R>;
+  constexpr int B = T::B;
+  extern __shared__ __align__(16) unsigned char smem_all[];
+  const unsigned base = smem_u32(smem_all);
+  unsigned char *const tile = smem_all + ((128u - (base & 127u)) & 127u);
+  unsigned char *const rest = tile + T::TILE_BYTES;
+  __shared__ __align__(8) unsigned long long mbar;
+  __shared__ double s_om[B], s_ec[B], s_es[B];
+  const unsigned mb = smem_u32(&mbar);
+  const int tid = threadIdx.x;
+  p2_setup<R, N, TC, M2_NL>(a, rest);
+  if (tid == 0) {
+    mbar_init(mb, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  const int64_t W = a.ntiles;
+  const int nc = a.nc;
+  auto issue = [&](int64_t w) {
+    const int64_t p0 = w * B;
+    const int64_t nb = (a.npencils - p0) < B ? (a.npencils - p0) : B;
+    const unsigned bytes = (unsigned)(nb * N * sizeof(C));
+    mbar_expect_tx(mb, bytes * (unsigned)nc);
+    for (int c = 0; c < nc; c++)
+      bulk_load(smem_u32(tile + (size_t)c * B * N * sizeof(C)), (const C *)pick(a.psi, c) + p0 * N, bytes, mb);
+  };
+  int64_t w = blockIdx.x;
+  if (tid == 0 && w < W) issue(w);
+  unsigned parity = 0;
+  for (; w < W; w += gridDim.x) {
+    bool ok = false;
+    for (long it = 0; it < TMA_WAIT_LIMIT && !ok; it++) ok = mbar_try_wait(mb, parity);
+    if (!__syncthreads_and(ok)) {
+      if (tid == 0 && a.err) atomicOr(a.err, 1);
+      break;
+    }
+    parity ^= 1;
+    const int64_t wn = w + gridDim.x;
+    auto refill = [&]() {
+      __syncthreads();
+      if (tid == 0 && wn < W) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        issue(wn);
+      }
+    };
+    p2_item<R, N, TC, M2_NL, false, true>(a, tile_geo<B, N>(a, w), rest, false, s_om, s_ec, s_es, nullptr, tile,
+                                          refill);
   }
 }
 
