@@ -575,9 +575,6 @@ int atus_create(const atus_grid *grid, int ncomp, int precision, atus_ctx **out)
     // ATUS_TMA=0: strided 256-point passes load their tiles themselves (no TMA)
     const char *tm = getenv("ATUS_TMA");
     ctx->use_tma = !(tm && tm[0] == '0');
-    // ATUS_BULK_NL=1: contiguous 256-point potential passes fed by bulk copies
-    const char *bn = getenv("ATUS_BULK_NL");
-    ctx->use_bulk_nl = (bn && bn[0] == '1');
   }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) { delete ctx; return ATUS_E_CUDA; }
@@ -723,6 +720,13 @@ int atus_get_dt(const atus_ctx *ctx, double *dt) {
   return ATUS_OK;
 }
 
+int atus_set_wait_limits(atus_ctx *ctx, int64_t wait_rounds, int drop_copies) {
+  if (!ctx || wait_rounds < 1 || (drop_copies != 0 && drop_copies != 1)) return ATUS_E_ARG;
+  ctx->wait_limit = (long)wait_rounds;
+  ctx->drop_copies = drop_copies;
+  return ATUS_OK;
+}
+
 int atus_set_bragg_stable(atus_ctx *ctx, int on) {
   if (!ctx || (on != 0 && on != 1)) return ATUS_E_ARG;
   ctx->bragg_stable = on;
@@ -781,7 +785,6 @@ int atus_clone(const atus_ctx *src, atus_ctx **out) {
   ctx->use_pass2 = src->use_pass2;
   ctx->use_cluster1d = src->use_cluster1d;
   ctx->use_tma = src->use_tma;
-  ctx->use_bulk_nl = src->use_bulk_nl;
   int e = ATUS_OK;
   auto copy = [&](void *dst, const void *from, size_t bytes) {
     if (e == ATUS_OK && cudaMemcpyAsync(dst, from, bytes, cudaMemcpyDeviceToDevice, ctx->stream) != cudaSuccess)

@@ -36,9 +36,10 @@ struct atus_ctx {
   bool use_pass2 = true;        // register-staged passes for pencils of 32..256 points
   bool use_cluster1d = true;    // 1D blocks of 2048..8192 points on a 16-CTA cluster
   bool use_tma = false;         // strided 256-point passes fed by TMA tile copies
-  bool use_bulk_nl = false;     // and contiguous 256-point potential passes fed by bulk copies
   int *err_dev = nullptr;       // device error word of bounded waits (0: none)
   bool err_armed = false;       // a kernel that can set it ran since the last check
+  long wait_limit = 1L << 22;   // TMA tile waits: try_wait rounds (atus_set_wait_limits)
+  int drop_copies = 0;          // TMA passes issue no copies (error-path tests)
   int bragg_stable = 0;         // FP64 Bragg step in the eigenvalue-free form
   std::string err;
   // Sobolev state

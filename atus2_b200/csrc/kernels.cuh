@@ -114,6 +114,8 @@ struct PassArgs {
   double rabi_k0[8][3];
   double *rabi_partial;
   int *err;  // device error word (bounded waits that ran out set bits)
+  long wait_limit;       // try_wait rounds before a TMA tile counts as lost
+  int drop_copies;       // issue no tile copies, so every wait runs out (error-path tests; 0)
 };
 
 __device__ __forceinline__ void idx3(const Geo &g, int64_t l, int &ix, int &iy, int &iz) {

@@ -215,6 +215,8 @@ static inline int launch_pass2_tma_t(atus_ctx *ctx, PassArgs &a, int axis) {
   a.ntiles = ntiles;
   a.ncomp_grid = ctx->ncomp;
   a.err = ctx->err_dev;
+  a.wait_limit = ctx->wait_limit;
+  a.drop_copies = ctx->drop_copies;
   const int64_t work = ntiles * ctx->ncomp;
   const int64_t slots = (int64_t)nsm * resident;
   const unsigned grid = (unsigned)(work < slots ? work : slots);
@@ -224,53 +226,8 @@ static inline int launch_pass2_tma_t(atus_ctx *ctx, PassArgs &a, int axis) {
   return ATUS_OK;
 }
 
-// Contiguous 256-point potential pass with bulk-copied tiles (pass2_tma.cuh).
-template <typename R, int N, int TC>
-static inline int launch_pass2_bulk_nl_t(atus_ctx *ctx, PassArgs &a, int axis) {
-  using T = P2BulkCfg<R, N, TC>;
-  using Cfg = P2Cfg<R, N, TC>;
-  constexpr size_t smem = T::smem;
-  static int resident = 0;
-  static int nsm = 0;
-  if (!resident) {
-    CK(cudaFuncSetAttribute(pass2_bulk_nl_kernel<R, N, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    CK(cudaFuncSetAttribute(pass2_bulk_nl_kernel<R, N, TC>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                            cudaSharedmemCarveoutMaxShared));
-    int dev = 0;
-    CK(cudaGetDevice(&dev));
-    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, pass2_bulk_nl_kernel<R, N, TC>, Cfg::NT, smem));
-    if (resident < 1) return fail(ctx, ATUS_E_UNSUPPORTED, "bulk-copy pass kernel does not fit on an SM");
-  }
-  a.sa = 1;
-  a.inner_tiles = 1;
-  a.npencils = ctx->npts / N;
-  const int64_t ntiles = (a.npencils + Cfg::B - 1) / Cfg::B;
-  a.x_along = (axis == 0);
-  a.axis = axis;
-  a.g = geo(ctx);
-  a.tw = (sizeof(R) == 8) ? ctx->tw64 : ctx->tw;
-  for (int ax = 0; ax < 3; ax++) {
-    a.dk[ax] = ctx->dk[ax];
-    a.n[ax] = (int)ctx->n[ax];
-  }
-  a.ntiles = ntiles;
-  a.ncomp_grid = ctx->ncomp;
-  a.err = ctx->err_dev;
-  const int64_t slots = (int64_t)nsm * resident;
-  const unsigned grid = (unsigned)(ntiles < slots ? ntiles : slots);
-  pass2_bulk_nl_kernel<R, N, TC><<<grid, Cfg::NT, smem, ctx->stream>>>(a);
-  LAUNCHED(ctx);
-  ctx->err_armed = true;
-  return ATUS_OK;
-}
-
 template <typename R, int N, int TC, int MODE, bool STRIDED>
 static inline int launch_pass2_t(atus_ctx *ctx, PassArgs &a, int axis) {
-  if constexpr (!STRIDED && N == 256 && MODE == M2_NL) {
-    if (ctx->use_tma && ctx->use_bulk_nl && !a.per_comp && ctx->err_dev && axis == ctx->dim - 1)
-      return launch_pass2_bulk_nl_t<R, N, TC>(ctx, a, axis);
-  }
   if constexpr (STRIDED && N == 256 && TC == 1 && (MODE == M2_FWD || MODE == M2_INV || MODE == M2_KIN)) {
     if (ctx->use_tma && a.per_comp && ctx->err_dev && ctx->npts / ctx->n[axis] >= 2) {
       const int r = launch_pass2_tma_t<R, N, MODE>(ctx, a, axis);

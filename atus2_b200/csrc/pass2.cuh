@@ -178,10 +178,9 @@ __device__ __forceinline__ cplx<R> p2_tile_at(const unsigned char *tile, int i, 
     return *reinterpret_cast<const cplx<R> *>(tile + i * 128 + (((b >> 1) ^ (i & 7)) << 4) + ((b & 1) << 3));
 }
 
-// One work item.  SMEM_TILE: the tile's inputs come from `tile` instead of
-// global memory -- strided tiles swizzled (p2_tile_at), contiguous tiles as
-// the B pencils of each component one after another ([c][b][i]) -- and
-// hook() runs once every thread has taken its values.
+// One work item.  SMEM_TILE (strided passes): the tile's inputs come from
+// `tile` (swizzled, see p2_tile_at) instead of global memory, and hook()
+// runs once every thread has taken its values.
 template <typename R, int N, int TC, int MODE, bool STRIDED, bool SMEM_TILE = false, typename Hook = P2NoHook>
 __device__ __forceinline__ void p2_item(const PassArgs &a, const TileGeo &g, unsigned char *smem_raw, bool kt_shared,
                                         double *s_om, double *s_ec, double *s_es, double *rq = nullptr,
@@ -224,14 +223,9 @@ __device__ __forceinline__ void p2_item(const PassArgs &a, const TileGeo &g, uns
 
   C v[16];
   if constexpr (SMEM_TILE) {
-    if constexpr (STRIDED) {
-      #pragma unroll
-      for (int r = 0; r < 16; r++) v[r] = p2_tile_at<R>(tile, j + R2 * r, b);
-    } else {
-      const C *tv = reinterpret_cast<const C *>(tile) + (c * B + b) * N + j;
-      #pragma unroll
-      for (int r = 0; r < 16; r++) v[r] = tv[R2 * r];
-    }
+    static_assert(STRIDED, "shared-memory tiles of strided passes only");
+    #pragma unroll
+    for (int r = 0; r < 16; r++) v[r] = p2_tile_at<R>(tile, j + R2 * r, b);
     hook();
   } else {
     #pragma unroll

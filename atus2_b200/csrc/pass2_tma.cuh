@@ -8,8 +8,12 @@
 // (conflict-free: the swizzle spreads a row's pencils over all banks), one
 // thread issues the copy of the CTA's next tile into it, so that copy flies
 // while this tile is transformed and stored.  Waits on the mbarrier are
-// bounded: on time-out every thread leaves the loop and the error word is
-// set (read by the host after the block).
+// bounded (PassArgs::wait_limit rounds of try_wait): on time-out every thread
+// leaves the loop and the error word is set (read by the host after the
+// block).  A copy that never lands thus ends the pass with an error status
+// instead of a hang; PassArgs::drop_copies (no copy issued, no arrival on
+// the barrier) makes every wait run out with nothing in flight, for tests of
+// that path.
 #pragma once
 #include <cuda.h>
 
@@ -21,8 +25,6 @@ namespace atus {
 struct alignas(64) TmaMaps {
   CUtensorMap m[MAXC];
 };
-
-constexpr long TMA_WAIT_LIMIT = 1L << 22;  // try_wait rounds before a tile counts as lost
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -50,14 +52,6 @@ __device__ __forceinline__ void tma_load_3d(unsigned dst, const CUtensorMap *map
       "[%5];" ::"r"(dst),
       "l"(reinterpret_cast<unsigned long long>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(mbar)
       : "memory");
-}
-
-// Bulk copy of `bytes` contiguous bytes (16-byte aligned, a multiple of 16)
-// into shared memory at dst, completing on mbar.
-__device__ __forceinline__ void bulk_load(unsigned dst, const void *src, unsigned bytes, unsigned mbar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-               "l"(reinterpret_cast<unsigned long long>(src)), "r"(bytes), "r"(mbar)
-               : "memory");
 }
 
 template <typename R, int N>
@@ -95,6 +89,7 @@ __global__ void __launch_bounds__(Tile2<R>::NT, 3) pass2_tma_kernel(PassArgs a, 
     const int64_t t = w % a.ntiles;
     const int o = (int)(t / a.inner_tiles);
     const int r0 = (int)((t % a.inner_tiles) * B);
+    if (a.drop_copies) return;  // the barrier phase then never completes
     mbar_expect_tx(mb, T::TILE_BYTES);
     tma_load_3d(smem_u32(tile), &maps.m[comp], T::VPC * r0, 0, o, mb);
   };
@@ -103,7 +98,7 @@ __global__ void __launch_bounds__(Tile2<R>::NT, 3) pass2_tma_kernel(PassArgs a, 
   unsigned parity = 0;
   for (; w < W; w += gridDim.x) {
     bool ok = false;
-    for (long it = 0; it < TMA_WAIT_LIMIT && !ok; it++) ok = mbar_try_wait(mb, parity);
+    for (long it = 0; it < a.wait_limit && !ok; it++) ok = mbar_try_wait(mb, parity);
     if (!__syncthreads_and(ok)) {
       if (tid == 0 && a.err) atomicOr(a.err, 1);
       break;
@@ -119,72 +114,6 @@ __global__ void __launch_bounds__(Tile2<R>::NT, 3) pass2_tma_kernel(PassArgs a, 
     };
     p2_item<R, N, 1, MODE, true, true>(a, tile_geo<B, N>(a, w), rest, false, s_om, s_ec, s_es, nullptr, tile,
                                        refill);
-  }
-}
-
-// Contiguous-axis potential pass (IFFT, potential step, FFT along the last
-// axis, TC components per tile) with each tile -- B whole pencils of every
-// component, contiguous in memory -- brought in by TC bulk copies on an
-// mbarrier; the next tile's copies are issued once the current one is in
-// registers.
-template <typename R, int N, int TC>
-struct P2BulkCfg {
-  using Cfg = P2Cfg<R, N, TC>;
-  static constexpr int B = Cfg::B;
-  static constexpr unsigned TILE_BYTES = (unsigned)(TC * B * N * sizeof(cplx<R>));
-  static constexpr size_t smem = 128 + TILE_BYTES + Cfg::smem;
-};
-
-template <typename R, int N, int TC>
-__global__ void __launch_bounds__(Tile2<R>::NT, 3) pass2_bulk_nl_kernel(PassArgs a) {
-  using T = P2BulkCfg<R, N, TC>;
-  using C = cplx<R>;
-  constexpr int B = T::B;
-  extern __shared__ __align__(16) unsigned char smem_all[];
-  const unsigned base = smem_u32(smem_all);
-  unsigned char *const tile = smem_all + ((128u - (base & 127u)) & 127u);
-  unsigned char *const rest = tile + T::TILE_BYTES;
-  __shared__ __align__(8) unsigned long long mbar;
-  __shared__ double s_om[B], s_ec[B], s_es[B];
-  const unsigned mb = smem_u32(&mbar);
-  const int tid = threadIdx.x;
-  p2_setup<R, N, TC, M2_NL>(a, rest);
-  if (tid == 0) {
-    mbar_init(mb, 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  __syncthreads();
-  const int64_t W = a.ntiles;
-  const int nc = a.nc;
-  auto issue = [&](int64_t w) {
-    const int64_t p0 = w * B;
-    const int64_t nb = (a.npencils - p0) < B ? (a.npencils - p0) : B;
-    const unsigned bytes = (unsigned)(nb * N * sizeof(C));
-    mbar_expect_tx(mb, bytes * (unsigned)nc);
-    for (int c = 0; c < nc; c++)
-      bulk_load(smem_u32(tile + (size_t)c * B * N * sizeof(C)), (const C *)pick(a.psi, c) + p0 * N, bytes, mb);
-  };
-  int64_t w = blockIdx.x;
-  if (tid == 0 && w < W) issue(w);
-  unsigned parity = 0;
-  for (; w < W; w += gridDim.x) {
-    bool ok = false;
-    for (long it = 0; it < TMA_WAIT_LIMIT && !ok; it++) ok = mbar_try_wait(mb, parity);
-    if (!__syncthreads_and(ok)) {
-      if (tid == 0 && a.err) atomicOr(a.err, 1);
-      break;
-    }
-    parity ^= 1;
-    const int64_t wn = w + gridDim.x;
-    auto refill = [&]() {
-      __syncthreads();
-      if (tid == 0 && wn < W) {
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        issue(wn);
-      }
-    };
-    p2_item<R, N, TC, M2_NL, false, true>(a, tile_geo<B, N>(a, w), rest, false, s_om, s_ec, s_es, nullptr, tile,
-                                          refill);
   }
 }
 

@@ -118,6 +118,7 @@ SIGNATURES = {
     "atus_profile_passes": (_i, [_vp, _i, _i, _dp, _dp, _dp, C.POINTER(C.c_int)]),
     "atus_particle_number": (_i, [_vp, _i, _dp]),
     "atus_set_bragg_stable": (_i, [_vp, _i]),
+    "atus_set_wait_limits": (_i, [_vp, C.c_int64, _i]),
     "atus_particle_number_noalloc": (_i, [_vp, C.c_int64, _i, C.c_double, _vp, _vp]),
     "atus_guess_init": (_i, [C.c_uint64, _dp]),
     "atus_guess_grad": (_i, [_dp, _dp, _dp, _i, _dp, _dp]),
@@ -282,6 +283,11 @@ class Solver:
     def set_bragg_stable(self, on: bool = True) -> None:
         """FP64 bragg_ad in the eigenvalue-free form instead of the reference's eigen-form."""
         self._ok(self._L.atus_set_bragg_stable(self._c, int(bool(on))), "set_bragg_stable")
+
+    def set_wait_limits(self, wait_rounds: int = 1 << 22, drop_copies: bool = False) -> None:
+        """Bounded waits of the TMA-fed passes (atus_set_wait_limits);
+        drop_copies makes every wait run out (tests of the error path)."""
+        self._ok(self._L.atus_set_wait_limits(self._c, int(wait_rounds), int(bool(drop_copies))), "set_wait_limits")
 
     def set_laser(self, laser: Laser) -> None:
         self._ok(self._L.atus_set_laser(self._c, C.byref(laser)), "set_laser")

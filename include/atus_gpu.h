@@ -183,6 +183,16 @@ ATUS_API int atus_set_pulse_windows(atus_ctx *ctx, double t_start, const double 
  * Gaussian pulse reach both.  Default 0: the reference's form, bit for bit. */
 ATUS_API int atus_set_bragg_stable(atus_ctx *ctx, int on);
 
+/* No counterpart in the reference.  Bounded waits of the TMA-fed strided
+ * passes: a tile copy not complete after wait_rounds rounds of
+ * mbarrier.try_wait (default 2^22) ends the pass, and the block or step
+ * call returns ATUS_E_CUDA ("a TMA tile copy did not complete ...") instead
+ * of hanging; the context stays usable (its fields are then undefined).
+ * drop_copies = 1 issues no tile copies, so every wait runs out with nothing
+ * in flight: a test hook for that error path, 0 in normal use.  ATUS_E_ARG
+ * for wait_rounds < 1 or drop_copies not 0 or 1. */
+ATUS_API int atus_set_wait_limits(atus_ctx *ctx, int64_t wait_rounds, int drop_copies);
+
 /* ------------------------------------------------------------ fields */
 /* Interleaved complex128, N values, grid order (the .bin payload). */
 ATUS_API int atus_upload_psi(atus_ctx *ctx, int comp, const double *psi);
