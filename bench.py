@@ -626,7 +626,7 @@ def run_cpu_baseline(n_short=1, n_long=5, repeats=3):
 # FP64 256^3 x 2 kernels, each from one ncu capture of that kernel on this
 # workload on a B200 (a profiler cannot run inside the timed bench, so the
 # capture's figure is carried here).
-NCU_TRAFFIC_FP64 = {"pass2_kernel M2_NL (z)": 1.0941e9, "pass2_kernel M2_KIN": 1.0433e9}
+NCU_TRAFFIC_FP64 = {"pass2_kernel M2_NL (z)": 1.0941e9, "pass2_kernel M2_KIN": 1.0155e9}
 
 
 def roofline(s, kind, peak, peak_kind, fp64=True):
