@@ -626,14 +626,16 @@ def run_cpu_baseline(n_short=1, n_long=5, repeats=3):
 # FP64 256^3 x 2 kernels, each from one ncu capture of that kernel on this
 # workload on a B200 (a profiler cannot run inside the timed bench, so the
 # capture's figure is carried here).
-NCU_TRAFFIC_FP64 = {"pass2_kernel M2_NL (z)": 1.0941e9, "pass2_kernel M2_KIN": 1.0155e9}
+NCU_TRAFFIC_FP64 = {"pass2_kernel M2_NL (z)": 1.0941e9, "pass2_tma_kernel M2_KIN (x)": 1.0155e9}
 
 
 def roofline(s, kind, peak, peak_kind, fp64=True):
     prof = s.profile_passes(kind, reps=5)
     # pass names in atus_profile_passes order: x kinetic pass, then the
-    # three axis passes of the real-space half step
-    names = ["pass2_kernel M2_KIN", "pass2_kernel M2_INV (y)", "pass2_kernel M2_NL (z)", "pass2_kernel M2_FWD (y)"]
+    # three axis passes of the real-space half step (strided passes take
+    # their tiles by TMA unless ATUS_TMA=0)
+    sk = "pass2_kernel" if os.environ.get("ATUS_TMA") == "0" else "pass2_tma_kernel"
+    names = [f"{sk} M2_KIN (x)", f"{sk} M2_INV (y)", "pass2_kernel M2_NL (z)", f"{sk} M2_FWD (y)"]
     # dominant pass: largest device time per Strang step
     bi = max(range(len(prof)), key=lambda q: prof[q][0] * prof[q][1])
     ms, lps, by = prof[bi]
