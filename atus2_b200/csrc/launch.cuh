@@ -173,7 +173,9 @@ static inline int launch_pass2_tma_t(atus_ctx *ctx, PassArgs &a, int axis) {
   int64_t sa = 1;
   for (int b = axis + 1; b < 3; b++) sa *= ctx->n[b];
   const int64_t outer = ctx->npts / (N * sa);
-  if (sa < 2 || T::VPC * sa > (int64_t(1) << 31) || outer > (int64_t(1) << 31)) return ATUS_E_UNSUPPORTED;
+  // whole tiles only (the box never reaches past the row), coordinates in int32
+  if (sa < T::B || sa % T::B != 0 || T::VPC * sa > (int64_t(1) << 31) || outer > (int64_t(1) << 31))
+    return ATUS_E_UNSUPPORTED;
   static int resident = 0;
   static int nsm = 0;
   if (!resident) {
