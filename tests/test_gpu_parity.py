@@ -118,6 +118,7 @@ def test_config1_1d_full_length_fp64():
         errs_np.append(rel_l2(ref_np[b], o.psi(0)))
     msg = ("GPU vs oracle: " + " ".join(f"{e:.2e}" for e in errs) + " | numpy-FFT vs oracle: " +
            " ".join(f"{e:.2e}" for e in errs_np))
+    print(msg)
     # 1e-11 for the first 5000 steps; beyond, no worse than swapping in another
     # exact FP64 FFT (the FFT rounding of any implementation accumulates on
     # this 20000-step nonlinear run)
