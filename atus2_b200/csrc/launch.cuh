@@ -161,7 +161,7 @@ static inline EncodeTiledFn encode_tiled() {
   return fn;
 }
 
-// Strided 256-point pass with TMA tile copies (pass2_tma.cuh); the tile and
+// Strided pass (64..256-point pencils) with TMA tile copies (pass2_tma.cuh); the tile and
 // launch geometry of launch_pass2_t.  ATUS_E_UNSUPPORTED (nothing launched)
 // where a tensor map cannot describe the pass.
 template <typename R, int N, int MODE>
@@ -192,14 +192,14 @@ static inline int launch_pass2_tma_t(atus_ctx *ctx, PassArgs &a, int axis) {
   TmaMaps maps;
   memset(&maps, 0, sizeof(maps));
   for (int c = 0; c < nf; c++) {
-    // 8-byte units: {VPC sa, N, outer}, box {VPC B, N, 1}, 128-byte swizzle
+    // 8-byte units: {VPC sa, N, outer}, box {VPC B, N, 1}, 128-byte swizzle for 128-byte rows
     const cuuint64_t dims[3] = {(cuuint64_t)(T::VPC * sa), (cuuint64_t)N, (cuuint64_t)outer};
     const cuuint64_t strides[2] = {(cuuint64_t)(T::VPC * sa * 8), (cuuint64_t)(T::VPC * sa * 8 * N)};
     const cuuint32_t box[3] = {(cuuint32_t)(T::VPC * T::B), (cuuint32_t)N, 1};
     const cuuint32_t estr[3] = {1, 1, 1};
     if (enc(&maps.m[c], CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, a.psi[c], dims, strides, box, estr,
-            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            CU_TENSOR_MAP_INTERLEAVE_NONE, T::SWZ ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
       return ATUS_E_UNSUPPORTED;
   }
   a.sa = sa;
@@ -230,7 +230,7 @@ static inline int launch_pass2_tma_t(atus_ctx *ctx, PassArgs &a, int axis) {
 
 template <typename R, int N, int TC, int MODE, bool STRIDED>
 static inline int launch_pass2_t(atus_ctx *ctx, PassArgs &a, int axis) {
-  if constexpr (STRIDED && N == 256 && TC == 1 && (MODE == M2_FWD || MODE == M2_INV || MODE == M2_KIN)) {
+  if constexpr (STRIDED && N >= 64 && TC == 1 && (MODE == M2_FWD || MODE == M2_INV || MODE == M2_KIN)) {
     if (ctx->use_tma && a.per_comp && ctx->err_dev && ctx->npts / ctx->n[axis] >= 2) {
       const int r = launch_pass2_tma_t<R, N, MODE>(ctx, a, axis);
       if (r != ATUS_E_UNSUPPORTED) return r;

@@ -167,12 +167,17 @@ struct P2NoHook {
   __device__ __forceinline__ void operator()() const {}
 };
 
-// Swizzled tile of a strided pass as a 128-byte-swizzled TMA box writes it:
-// row i (point i of the B pencils) is 128 bytes, its 16-byte chunk c at
-// position c ^ (i & 7).  Value of pencil b at point i.
-template <typename R>
+// Tile of a strided pass as a TMA box writes it: row i (point i of the B
+// pencils) is B values.  Rows of 128 bytes come with the 128-byte swizzle
+// (16-byte chunk c at position c ^ (i & 7)); longer rows unswizzled (the
+// threads of a quarter warp read consecutive pencils of one row).  Value of
+// pencil b at point i.
+template <typename R, int B>
 __device__ __forceinline__ cplx<R> p2_tile_at(const unsigned char *tile, int i, int b) {
-  if constexpr (sizeof(R) == 8)
+  constexpr int ROW = B * (int)sizeof(cplx<R>);
+  if constexpr (ROW != 128)
+    return *reinterpret_cast<const cplx<R> *>(tile + i * ROW + b * (int)sizeof(cplx<R>));
+  else if constexpr (sizeof(R) == 8)
     return *reinterpret_cast<const cplx<R> *>(tile + i * 128 + ((b ^ (i & 7)) << 4));
   else
     return *reinterpret_cast<const cplx<R> *>(tile + i * 128 + (((b >> 1) ^ (i & 7)) << 4) + ((b & 1) << 3));
@@ -225,7 +230,7 @@ __device__ __forceinline__ void p2_item(const PassArgs &a, const TileGeo &g, uns
   if constexpr (SMEM_TILE) {
     static_assert(STRIDED, "shared-memory tiles of strided passes only");
     #pragma unroll
-    for (int r = 0; r < 16; r++) v[r] = p2_tile_at<R>(tile, j + R2 * r, b);
+    for (int r = 0; r < 16; r++) v[r] = p2_tile_at<R, B>(tile, j + R2 * r, b);
     hook();
   } else {
     #pragma unroll

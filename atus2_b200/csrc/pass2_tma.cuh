@@ -1,11 +1,12 @@
 // pass2_tma.cuh -- strided register-staged passes whose tiles arrive by TMA.
 //
-// The same work items as pass2_kernel (B adjacent 256-point pencils of one
-// component along a strided axis, B x 16 bytes = one 128-byte row per point),
-// but each tile is copied by one cp.async.bulk.tensor (a 3D box {B pencils,
-// 256 points, 1}) into a shared-memory buffer with 128-byte swizzle, complete
-// on an mbarrier.  Once every thread has taken its 16 values from the buffer
-// (conflict-free: the swizzle spreads a row's pencils over all banks), one
+// The same work items as pass2_kernel (B adjacent pencils of 64..256 points
+// of one component along a strided axis, one row of B values per point), but
+// each tile is copied by one cp.async.bulk.tensor (a 3D box {B pencils, N
+// points, 1}) into a shared-memory buffer -- 128-byte rows with 128-byte
+// swizzle, longer rows plain -- complete on an mbarrier.  Once every thread
+// has taken its 16 values from the buffer (conflict-free: a quarter warp
+// reads consecutive pencils of one row, spread over the banks), one
 // thread issues the copy of the CTA's next tile into it, so that copy flies
 // while this tile is transformed and stored.  Waits on the mbarrier are
 // bounded (PassArgs::wait_limit rounds of try_wait): on time-out every thread
@@ -59,8 +60,10 @@ struct P2TmaCfg {
   using Cfg = P2Cfg<R, N, 1>;
   static constexpr int B = Cfg::B;
   static constexpr int VPC = (int)sizeof(cplx<R>) / 8;  // 8-byte units per value
-  static constexpr unsigned TILE_BYTES = (unsigned)N * 128;
-  static_assert(B * sizeof(cplx<R>) == 128, "one 128-byte row per point");
+  static constexpr int ROW = B * (int)sizeof(cplx<R>);  // bytes per point of the tile
+  static constexpr unsigned TILE_BYTES = (unsigned)N * ROW;
+  static constexpr bool SWZ = (ROW == 128);               // 128-byte swizzle (else none)
+  static_assert(ROW >= 128 && VPC * B <= 256, "rows of 128 bytes or more, at most 256 units a box row");
   // tile (1024-byte aligned inside the allocation) + exchange rows + twiddles
   static constexpr size_t smem = 1024 + TILE_BYTES + Cfg::smem;
 };
