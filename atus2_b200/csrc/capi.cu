@@ -572,7 +572,7 @@ int atus_create(const atus_grid *grid, int ncomp, int precision, atus_ctx **out)
     // ATUS_CLUSTER1D=0: 1D blocks on one CTA only (A/B comparisons)
     const char *c1 = getenv("ATUS_CLUSTER1D");
     ctx->use_cluster1d = !(c1 && c1[0] == '0');
-    // ATUS_TMA=0: strided 64..256-point passes load their tiles themselves (no TMA)
+    // ATUS_TMA=0: strided 256-point passes load their tiles themselves (no TMA)
     const char *tm = getenv("ATUS_TMA");
     ctx->use_tma = !(tm && tm[0] == '0');
   }

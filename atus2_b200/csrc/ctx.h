@@ -35,7 +35,7 @@ struct atus_ctx {
   int64_t launches = 0;
   bool use_pass2 = true;        // register-staged passes for pencils of 32..256 points
   bool use_cluster1d = true;    // 1D blocks of 2048..8192 points on a 16-CTA cluster
-  bool use_tma = false;         // strided 64..256-point passes fed by TMA tile copies
+  bool use_tma = false;         // strided 256-point passes fed by TMA tile copies
   int *err_dev = nullptr;       // device error word of bounded waits (0: none)
   bool err_armed = false;       // a kernel that can set it ran since the last check
   long wait_limit = 1L << 22;   // TMA tile waits: try_wait rounds (atus_set_wait_limits)

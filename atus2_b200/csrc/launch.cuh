@@ -161,7 +161,7 @@ static inline EncodeTiledFn encode_tiled() {
   return fn;
 }
 
-// Strided pass (64..256-point pencils) with TMA tile copies (pass2_tma.cuh); the tile and
+// Strided pass with TMA tile copies (pass2_tma.cuh); the tile and
 // launch geometry of launch_pass2_t.  ATUS_E_UNSUPPORTED (nothing launched)
 // where a tensor map cannot describe the pass.
 template <typename R, int N, int MODE>
@@ -230,7 +230,10 @@ static inline int launch_pass2_tma_t(atus_ctx *ctx, PassArgs &a, int axis) {
 
 template <typename R, int N, int TC, int MODE, bool STRIDED>
 static inline int launch_pass2_t(atus_ctx *ctx, PassArgs &a, int axis) {
-  if constexpr (STRIDED && N >= 64 && TC == 1 && (MODE == M2_FWD || MODE == M2_INV || MODE == M2_KIN)) {
+  // 256-point pencils only: on 128-point pencils (the 128^3 Sobolev
+  // iteration) the TMA-fed passes measured no faster (0.253 vs 0.252 ms per
+  // iteration)
+  if constexpr (STRIDED && N == 256 && TC == 1 && (MODE == M2_FWD || MODE == M2_INV || MODE == M2_KIN)) {
     if (ctx->use_tma && a.per_comp && ctx->err_dev && ctx->npts / ctx->n[axis] >= 2) {
       const int r = launch_pass2_tma_t<R, N, MODE>(ctx, a, axis);
       if (r != ATUS_E_UNSUPPORTED) return r;
