@@ -565,7 +565,15 @@ __device__ __forceinline__ void nl_point(const NLArgs &a, cplx<R> *v, int64_t l,
   }
   if constexpr (TC >= 2) {
     if (a.kind == K_NUM_BRAGG || a.kind == K_RAMAN) {
-      num_point<R, TC>(a, v, l, x0);
+      // the out-of-line step gets a copy: were the caller's array handed to
+      // it, its address would escape and the array would live in local
+      // memory on every path
+      cplx<R> w[TC];
+      #pragma unroll
+      for (int c = 0; c < TC; c++) w[c] = v[c];
+      num_point<R, TC>(a, w, l, x0);
+      #pragma unroll
+      for (int c = 0; c < TC; c++) v[c] = w[c];
       return;
     }
   }
