@@ -74,18 +74,22 @@ __device__ __forceinline__ void c1_kinetic(cooperative_groups::cluster_group &cl
   }
   __syncthreads();
   fft_tile<R, P, TC, NT, -1, TWN>(K, tw);
-  // psi^ <- ((psi^ s_f) K) s_b in FP64 at wavenumber index q + C k2
-  for (int e = threadIdx.x; e < TC * P; e += NT) {
-    const int c = e / P, k2 = e % P;
+  // psi^ <- ((psi^ s_f) K) s_b in FP64 at wavenumber index q + C k2 (the
+  // component loop unrolled: a run-time index into tab would put the
+  // pointer array in local memory)
+  #pragma unroll
+  for (int c = 0; c < TC; c++) {
     if (c < nc) {
-      const int si = c * NP + Pad<P>::idx(0, k2);
-      double2 v = to_d<R>(K[si]);
-      v.x *= s_f;
-      v.y *= s_f;
-      v = cmul(v, __ldg(&tab[c][q + C * k2]));
-      v.x *= s_b;
-      v.y *= s_b;
-      K[si] = from_d<R>(v);
+      for (int k2 = threadIdx.x; k2 < P; k2 += NT) {
+        const int si = c * NP + Pad<P>::idx(0, k2);
+        double2 v = to_d<R>(K[si]);
+        v.x *= s_f;
+        v.y *= s_f;
+        v = cmul(v, __ldg(&tab[c][q + C * k2]));
+        v.x *= s_b;
+        v.y *= s_b;
+        K[si] = from_d<R>(v);
+      }
     }
   }
   __syncthreads();
@@ -134,10 +138,12 @@ __global__ void __cluster_dims__(ATUS_C1_CLUSTER, 1, 1) __launch_bounds__(256, 1
     kf[c] = a.kf[c];
   }
   // the CTA's columns: points q PC + pl + P r
-  for (int e = threadIdx.x; e < Cfg::HN; e += NT) {
-    const int c = e / (C * PC), r = (e / PC) % C, pl = e % PC;
-    H[e] = (c < nc) ? fld[c][q * PC + pl + P * r] : mk<R>(0, 0);
-  }
+  #pragma unroll
+  for (int c = 0; c < TC; c++)
+    for (int e = threadIdx.x; e < C * PC; e += NT) {
+      const int r = e / PC, pl = e % PC;
+      H[c * C * PC + e] = (c < nc) ? fld[c][q * PC + pl + P * r] : mk<R>(0, 0);
+    }
   __shared__ NLArgs s_nl;
   const NLArgs &nl = s_nl;
   if (threadIdx.x == 0) s_nl = a.nl;
@@ -173,10 +179,13 @@ __global__ void __cluster_dims__(ATUS_C1_CLUSTER, 1, 1) __launch_bounds__(256, 1
     c1_kinetic<R, N, TC>(cl, H, K, tw, tab, nc, a.s_f, a.s_b);
     t += last ? 0.5 * dt : dt;
   }
-  for (int e = threadIdx.x; e < Cfg::HN; e += NT) {
-    const int c = e / (C * PC), r = (e / PC) % C, pl = e % PC;
-    if (c < nc) fld[c][q * PC + pl + P * r] = H[e];
-  }
+  #pragma unroll
+  for (int c = 0; c < TC; c++)
+    if (c < nc)
+      for (int e = threadIdx.x; e < C * PC; e += NT) {
+        const int r = e / PC, pl = e % PC;
+        fld[c][q * PC + pl + P * r] = H[c * C * PC + e];
+      }
   cl.sync();  // no CTA leaves while another may still read its shared memory
 }
 
