@@ -683,6 +683,19 @@ void atus_destroy(atus_ctx *ctx) {
 
 const char *atus_last_error(const atus_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
+// The device error word after kernels with bounded waits (the TMA-fed
+// passes): read once they are done, reset, and reported as ATUS_E_CUDA.
+static int wait_check(atus_ctx *ctx) {
+  if (!ctx->err_armed) return ATUS_OK;
+  ctx->err_armed = false;
+  int e = 0;
+  CK(cudaMemcpyAsync(&e, ctx->err_dev, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (e == 0) return ATUS_OK;
+  CK(cudaMemsetAsync(ctx->err_dev, 0, sizeof(int), ctx->stream));
+  return fail(ctx, ATUS_E_CUDA, "a TMA tile copy did not complete within the wait limit");
+}
+
 int atus_set_stream(atus_ctx *ctx, void *stream) {
   if (!ctx) return ATUS_E_ARG;
   CK(cudaStreamSynchronize(ctx->stream));
@@ -693,7 +706,7 @@ int atus_set_stream(atus_ctx *ctx, void *stream) {
 int atus_synchronize(atus_ctx *ctx) {
   if (!ctx) return ATUS_E_ARG;
   CK(cudaStreamSynchronize(ctx->stream));
-  return ATUS_OK;
+  return wait_check(ctx);
 }
 
 int atus_launch_count(const atus_ctx *ctx, int64_t *out) {
@@ -949,7 +962,7 @@ int atus_ft(atus_ctx *ctx, int comp, int isign) {
   else
     ft_scale_kernel<float><<<grid_blocks(ctx->npts, 256), 256, 0, ctx->stream>>>(ctx->psi[comp], fak, ctx->npts);
   LAUNCHED(ctx);
-  return ATUS_OK;
+  return wait_check(ctx);
 }
 
 int atus_embed(atus_ctx *src, int comp_s, atus_ctx *dst, int comp_d) {
@@ -982,19 +995,6 @@ int atus_embed(atus_ctx *src, int comp_s, atus_ctx *dst, int comp_d) {
   LAUNCHED(dst);
   CK(cudaStreamSynchronize(dst->stream));
   return ATUS_OK;
-}
-
-// The device error word after kernels with bounded waits (the TMA-fed
-// passes): read once they are done, reset, and reported as ATUS_E_CUDA.
-static int wait_check(atus_ctx *ctx) {
-  if (!ctx->err_armed) return ATUS_OK;
-  ctx->err_armed = false;
-  int e = 0;
-  CK(cudaMemcpyAsync(&e, ctx->err_dev, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
-  if (e == 0) return ATUS_OK;
-  CK(cudaMemsetAsync(ctx->err_dev, 0, sizeof(int), ctx->stream));
-  return fail(ctx, ATUS_E_CUDA, "a TMA tile copy did not complete within the wait limit");
 }
 
 int atus_ft_step(atus_ctx *ctx, int half) {
@@ -1256,7 +1256,7 @@ int atus_expval_momentum(atus_ctx *ctx, int comp, double *out) {
   RUN(reduce(ctx, a, s));
   const double f = scale_fak(ctx->dim, ctx->d);
   for (int i = 0; i < ctx->dim; i++) out[i] = ctx->ar_k * (f * f * s[i]);
-  return ATUS_OK;
+  return wait_check(ctx);
 }
 
 int atus_setup_momentum(atus_ctx *ctx, int comp, const double *p) {
@@ -1299,7 +1299,7 @@ int atus_rabi_integrals_comp(atus_ctx *ctx, int comp, const double *k0, int n, d
   RUN(reduce(ctx, a, s));
   const double f = scale_fak(ctx->dim, ctx->d);
   for (int m = 0; m < n; m++) out[m] = ctx->ar_k * (f * f * s[m]);
-  return ATUS_OK;
+  return wait_check(ctx);
 }
 
 // ------------------------------------------------------------------ Sobolev gradient
@@ -1512,7 +1512,7 @@ int atus_sob_renormalize(atus_ctx *ctx) {
 int atus_sob_iterate(atus_ctx *ctx, int n_iter, double *res, double *N) {
   if (!ctx || !ctx->sob_ready) return ctx ? fail(ctx, ATUS_E_STATE, "atus_sob_init first") : ATUS_E_ARG;
   for (int k = 0; k < n_iter; k++) RUN(sob_iterate_once(ctx, res, N));
-  return ATUS_OK;
+  return wait_check(ctx);
 }
 
 // Iterations until the residual is <= epsilon (the reference's run loop, the
@@ -1560,7 +1560,7 @@ int atus_sob_run(atus_ctx *ctx, double epsilon, int max_iter, int *iters, double
   }
   if (iters) *iters = hd->iters;
   if (res) *res = hd->res;
-  return ATUS_OK;
+  return wait_check(ctx);
 }
 
 int atus_sob_mu(atus_ctx *ctx, double *mu) {
