@@ -185,9 +185,11 @@ ATUS_API int atus_set_bragg_stable(atus_ctx *ctx, int on);
 
 /* No counterpart in the reference.  Bounded waits of the TMA-fed strided
  * passes: a tile copy not complete after wait_rounds rounds of
- * mbarrier.try_wait (default 2^22) ends the pass, and the block or step
- * call returns ATUS_E_CUDA ("a TMA tile copy did not complete ...") instead
- * of hanging; the context stays usable (its fields are then undefined).
+ * mbarrier.try_wait (default 2^22) ends the pass, and the call that ran it
+ * (a block, step, transform, spectral reduction or descent; else the next
+ * atus_synchronize) returns ATUS_E_CUDA ("a TMA tile copy did not complete
+ * ...") instead of hanging; the context stays usable (its fields are then
+ * undefined).
  * drop_copies = 1 issues no tile copies, so every wait runs out with nothing
  * in flight: a test hook for that error path, 0 in normal use.  ATUS_E_ARG
  * for wait_rounds < 1 or drop_copies not 0 or 1. */
