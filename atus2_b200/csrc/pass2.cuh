@@ -25,7 +25,7 @@ namespace atus {
 
 // Tile budget (complex values) and threads; one thread owns 16 values.
 template <typename R> struct Tile2;
-template <> struct Tile2<double> { static constexpr int E = 2048, NT = 128, MINB = 4; };
+template <> struct Tile2<double> { static constexpr int E = 2048, NT = 128, MINB = 5; };
 template <> struct Tile2<float> { static constexpr int E = 4096, NT = 256, MINB = 3; };
 
 template <typename R, int N, int TC>
