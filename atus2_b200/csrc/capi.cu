@@ -1080,30 +1080,7 @@ static int strang_block(atus_ctx *ctx, int nk, int kind, const double *F, const 
   const int64_t np1d = ((n0 >= 16) ? (n0 + n0 / 16) : n0) | 1;
   const bool on_cluster = ctx->use_cluster1d && n0 >= 2048 && n0 <= 8192;  // cluster1d.cuh
   const bool fits1d = on_cluster || (int64_t)ctx->csize * tc_for(ctx->ncomp) * np1d <= 227 * 1024;
-  if (ctx->dim == 1 && (ctx->ncomp > 2 || kind == K_NUM_BRAGG || ctx->fs_tw || !fits1d)) {
-    // more components or points than the resident 1D kernel holds, or a step
-    // that reads the header time itself: per step one kinetic pass (FFT,
-    // phase, IFFT per component) and one point-wise potential step
-    RUN(kinetic_pass(ctx, 1));
-    ctx->t += 0.5 * dt;
-    for (int j = 0; j < nk; j++) {
-      NLKArgs a;
-      memset(&a, 0, sizeof(a));
-      for (int c = 0; c < MAXC; c++) a.psi[c] = ctx->psi[c];
-      a.nl = nl_args(ctx, kind, ctx->t + 0.5 * dt, F ? F[j] : 1.0);
-      a.g = geo(ctx);
-      if (ctx->prec == ATUS_PREC_FP64)
-        nl_kernel<double><<<grid_blocks(ctx->npts, 256), 256, 0, ctx->stream>>>(a);
-      else
-        nl_kernel<float><<<grid_blocks(ctx->npts, 256), 256, 0, ctx->stream>>>(a);
-      LAUNCHED(ctx);
-      const bool last = (j == nk - 1);
-      RUN(kinetic_pass(ctx, last ? 1 : 0));
-      ctx->t += last ? 0.5 * dt : dt;
-    }
-    return ATUS_OK;
-  }
-  if (ctx->dim == 1) {
+  if (ctx->dim == 1 && ctx->ncomp <= 2 && kind != K_NUM_BRAGG && !ctx->fs_tw && fits1d) {
     Block1DArgs a;
     memset(&a, 0, sizeof(a));
     for (int c = 0; c < MAXC; c++) {
@@ -1134,11 +1111,39 @@ static int strang_block(atus_ctx *ctx, int nk, int kind, const double *F, const 
       cudaStreamSynchronize(ctx->stream);
       cudaFree(dF);
     }
-    if (r != ATUS_OK) return r;
-    // replay the header-time additions of the reference
-    double t = ctx->t + 0.5 * dt;
-    for (int j = 0; j < nk; j++) t += (j == nk - 1) ? 0.5 * dt : dt;
-    ctx->t = t;
+    if (r == ATUS_OK) {
+      // replay the header-time additions of the reference
+      double t = ctx->t + 0.5 * dt;
+      for (int j = 0; j < nk; j++) t += (j == nk - 1) ? 0.5 * dt : dt;
+      ctx->t = t;
+      return ATUS_OK;
+    }
+    // ATUS_E_UNSUPPORTED: nothing was launched (no cluster placeable, the
+    // field too long for one CTA); the per-step passes below run the block
+    if (r != ATUS_E_UNSUPPORTED) return r;
+    ctx->err.clear();
+  }
+  if (ctx->dim == 1) {
+    // more components or points than the resident 1D kernel holds, or a step
+    // that reads the header time itself: per step one kinetic pass (FFT,
+    // phase, IFFT per component) and one point-wise potential step
+    RUN(kinetic_pass(ctx, 1));
+    ctx->t += 0.5 * dt;
+    for (int j = 0; j < nk; j++) {
+      NLKArgs a;
+      memset(&a, 0, sizeof(a));
+      for (int c = 0; c < MAXC; c++) a.psi[c] = ctx->psi[c];
+      a.nl = nl_args(ctx, kind, ctx->t + 0.5 * dt, F ? F[j] : 1.0);
+      a.g = geo(ctx);
+      if (ctx->prec == ATUS_PREC_FP64)
+        nl_kernel<double><<<grid_blocks(ctx->npts, 256), 256, 0, ctx->stream>>>(a);
+      else
+        nl_kernel<float><<<grid_blocks(ctx->npts, 256), 256, 0, ctx->stream>>>(a);
+      LAUNCHED(ctx);
+      const bool last = (j == nk - 1);
+      RUN(kinetic_pass(ctx, last ? 1 : 0));
+      ctx->t += last ? 0.5 * dt : dt;
+    }
     return ATUS_OK;
   }
   // 2D / 3D: [inner forward] kinetic(half) { potential, kinetic } ... [inner inverse]

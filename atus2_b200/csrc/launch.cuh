@@ -96,15 +96,31 @@ static inline int launch_block1d_t(atus_ctx *ctx, Block1DArgs &a) {
 }
 
 // A 1D block on one cluster of CTAs (cluster1d.cuh).
+// ATUS_E_UNSUPPORTED (nothing launched) where the device cannot place such a
+// cluster (then the caller takes the one-CTA kernel or the per-step passes).
 template <typename R, int N, int TC>
 static inline int launch_cluster1d_t(atus_ctx *ctx, Block1DArgs &a) {
   using Cfg = C1Cfg<R, N, TC>;
-  static bool attr_set = false;
-  if (!attr_set) {
+  static int placeable = -1;  // clusters of this kernel the device can hold at once
+  if (placeable < 0) {
     CK(cudaFuncSetAttribute(cluster1d_kernel<R, N, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::smem));
     if (Cfg::C > 8) CK(cudaFuncSetAttribute(cluster1d_kernel<R, N, TC>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-    attr_set = true;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(Cfg::C);
+    cfg.blockDim = dim3(Cfg::NT);
+    cfg.dynamicSmemBytes = Cfg::smem;
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeClusterDimension;
+    attr.val.clusterDim.x = Cfg::C;
+    attr.val.clusterDim.y = 1;
+    attr.val.clusterDim.z = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    placeable = (cudaOccupancyMaxActiveClusters(&n, cluster1d_kernel<R, N, TC>, &cfg) == cudaSuccess) ? n : 0;
+    cudaGetLastError();  // a refused query leaves no sticky error
   }
+  if (placeable < 1) return ATUS_E_UNSUPPORTED;
   cluster1d_kernel<R, N, TC><<<Cfg::C, Cfg::NT, Cfg::smem, ctx->stream>>>(a);
   LAUNCHED(ctx);
   return ATUS_OK;
@@ -113,12 +129,14 @@ static inline int launch_cluster1d_t(atus_ctx *ctx, Block1DArgs &a) {
 template <typename R, int TC>
 static inline int launch_block1d_n(atus_ctx *ctx, Block1DArgs &a) {
   if (ctx->use_cluster1d) {
+    int r = ATUS_E_UNSUPPORTED;
     switch (ctx->n[0]) {
-      case 2048: return launch_cluster1d_t<R, 2048, TC>(ctx, a);
-      case 4096: return launch_cluster1d_t<R, 4096, TC>(ctx, a);
-      case 8192: return launch_cluster1d_t<R, 8192, TC>(ctx, a);
+      case 2048: r = launch_cluster1d_t<R, 2048, TC>(ctx, a); break;
+      case 4096: r = launch_cluster1d_t<R, 4096, TC>(ctx, a); break;
+      case 8192: r = launch_cluster1d_t<R, 8192, TC>(ctx, a); break;
       default: break;
     }
+    if (r != ATUS_E_UNSUPPORTED) return r;
   }
   switch (ctx->n[0]) {
     case 2: return launch_block1d_t<R, 2, TC>(ctx, a);
