@@ -547,10 +547,12 @@ __device__ __noinline__ void num_point(const NLArgs &a, cplx<R> *v, int64_t l, d
 // CRT_Base_IF.h:392-418, bragg.cpp:210-302).  Mixed: FP64 phase arguments,
 // FP32 field arithmetic, and the eigenvalue-free form of the 2x2 exponential.
 // TC: the number of components the calling kernel holds (ncomp <= TC); step
-// kinds that need more components are compiled out.
-template <typename R, int TC = MAXC>
+// kinds that need more components are compiled out.  PREV (one component):
+// the caller has loaded the potential at l into vpre (0 without a potential).
+template <typename R, int TC = MAXC, bool PREV = false>
 __device__ __forceinline__ void nl_point(const NLArgs &a, cplx<R> *v, int64_t l, double x0, double Omega,
-                                         double eta_c, double eta_s) {
+                                         double eta_c, double eta_s, double vpre = 0.0) {
+  static_assert(!PREV || TC == 1, "a pre-loaded potential serves one component");
   if constexpr (TC >= 3) {
     if (a.kind == K_DBRAGG) {
       dbragg_point<R>(a, v, l, x0);
@@ -588,7 +590,8 @@ __device__ __forceinline__ void nl_point(const NLArgs &a, cplx<R> *v, int64_t l,
       if (i >= n) break;
       double phi;
       if (a.kind == K_NL) {
-        phi = a.V[i] ? a.V[i][l] : 0.0;
+        if constexpr (PREV) phi = vpre;
+        else phi = a.V[i] ? a.V[i][l] : 0.0;
         #pragma unroll
         for (int j = 0; j < TC; j++)
           if (j < n) phi += a.gs[i * MAXC + j] * rho[j];

@@ -42,7 +42,13 @@ struct P3Cfg {
   static constexpr int NT = (NT_MIN > Tile3<R>::NT) ? NT_MIN : Tile3<R>::NT;
   static constexpr int NPC = NT / M; // pencil-components per tile
   static constexpr int B = NPC / TC; // pencils per tile
-  static constexpr int PB = 17 * M + 1;
+  // Pencil pitch of the exchange rows.  A bank group (the threads whose
+  // 128-byte wavefront is served at once: G = 8 complex128 or 16 complex64
+  // values) holds, in strided tiles, B pencils x G / B consecutive t; pitch
+  // PB = G / B (mod G) puts them on G distinct banks (the rows' own offsets
+  // are t mod G, 17 M = 0 mod G).  Contiguous tiles: a group is one pencil.
+  static constexpr int G = 128 / (int)sizeof(cplx<R>);
+  static constexpr int PB = 17 * M + ((STRIDED && B < G) ? G / B : 1);
   static constexpr size_t smem_ex = sizeof(cplx<R>) * NPC * PB;
   // W_N^{t q} (row q, column t) and W_M^{j2 q2} (row q2, column j2)
   static constexpr int TWN_N = 16 * M, TWN_M = 16 * R3;
@@ -153,6 +159,18 @@ __device__ __forceinline__ void p3_item(const PassArgs &a, const TileGeo &g, uns
   #pragma unroll
   for (int r = 0; r < 16; r++) v[r] = live ? src[r * step] : mk<R>(0, 0);
 
+  // one-component potential step: the potential of the thread's 16 points
+  // is requested into L2 now and loaded eight points ahead of its use after
+  // the inverse transform (behind the per-point branches each load would
+  // wait on its own)
+  const double *const Vp = a.nl.V[0];
+  const bool preV = MODE == M2_NL && TC == 1 && a.nl.kind == K_NL && Vp != nullptr && live;
+  if (preV) {
+    #pragma unroll
+    for (int m = 0; m < 16; m++)
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(Vp + lb + (int64_t)(t + M * m) * a.sa));
+  }
+
   if constexpr (MODE == M2_FWD) {
     p3_transform<R, N, -1>(v, my, twN, twM, t);
   } else if constexpr (MODE == M2_INV) {
@@ -215,8 +233,14 @@ __device__ __forceinline__ void p3_item(const PassArgs &a, const TileGeo &g, uns
     if constexpr (TC == 1) {
       int p0[3];
       idx3(a.g, lb, p0[0], p0[1], p0[2]);
+      constexpr int AHEAD = 8;  // potential loads in flight
+      double vpre[16];
+      auto load_v = [&](int m) { vpre[m] = preV ? __ldg(&Vp[lb + (int64_t)(t + M * m) * a.sa]) : 0.0; };
+      #pragma unroll
+      for (int m = 0; m < AHEAD; m++) load_v(m);
       #pragma unroll
       for (int m = 0; m < 16; m++) {
+        if (m + AHEAD < 16) load_v(m + AHEAD);
         const int i = t + M * m;
         const int64_t l = lb + (int64_t)i * a.sa;
         const int ix = (a.axis == 0) ? i : p0[0];
@@ -225,7 +249,7 @@ __device__ __forceinline__ void p3_item(const PassArgs &a, const TileGeo &g, uns
         if (a.nl.kind == K_BRAGG) bragg_coupling(a.nl, x0, om, ec, es);
         C u[MAXC];
         u[0] = v[m];
-        if (live) nl_point<R, TC>(a.nl, u, l, x0, om, ec, es);
+        if (live) nl_point<R, TC, true>(a.nl, u, l, x0, om, ec, es, vpre[m]);
         v[m] = u[0];
       }
     } else {
