@@ -307,8 +307,18 @@ __device__ __forceinline__ void p2_item(const PassArgs &a, const TileGeo &g, uns
     if constexpr (TC == 1) {
       int p0[3];
       idx3(a.g, lb, p0[0], p0[1], p0[2]);
+      // the potential, loaded four points ahead of its use (behind the
+      // per-point branches each load would wait on its own)
+      const double *const Vp = a.nl.V[0];
+      const bool preV = a.nl.kind == K_NL && Vp != nullptr && live;
+      constexpr int AHEAD = 4;
+      double vpre[16];
+      auto load_v = [&](int m) { vpre[m] = preV ? __ldg(&Vp[lb + (int64_t)(j + R2 * m) * a.sa]) : 0.0; };
+      #pragma unroll
+      for (int m = 0; m < AHEAD; m++) load_v(m);
       #pragma unroll
       for (int m = 0; m < 16; m++) {
+        if (m + AHEAD < 16) load_v(m + AHEAD);
         const int i = j + R2 * m;
         const int64_t l = lb + (int64_t)i * a.sa;
         const int ix = (a.axis == 0) ? i : p0[0];
@@ -317,7 +327,7 @@ __device__ __forceinline__ void p2_item(const PassArgs &a, const TileGeo &g, uns
         if (a.nl.kind == K_BRAGG) bragg_coupling(a.nl, x0, om, ec, es);
         C u[MAXC];
         u[0] = v[m];
-        if (live) nl_point<R, TC>(a.nl, u, l, x0, om, ec, es);
+        if (live) nl_point<R, TC, true>(a.nl, u, l, x0, om, ec, es, vpre[m]);
         v[m] = u[0];
       }
     } else {

@@ -1117,7 +1117,10 @@ def profile_block(which):
     Bragg state, no warm-up: pass2_kernel launches in order FFT_z, FFT_y, x
     kinetic (half), IFFT_y, z potential, FFT_y, x kinetic, IFFT_y, z
     potential, FFT_y, x kinetic (half), IFFT_y, IFFT_z.  rt1d: one block of
-    1000 steps of the 1D rt_solver workload (one block1d_kernel launch)."""
+    1000 steps of the 1D rt_solver workload (one block1d_kernel launch).
+    slit / slit-mixed: one block of 2 steps of the 2048^2 double slit:
+    pass3_kernel launches FFT_y, x kinetic (half), y potential, x kinetic,
+    y potential, x kinetic (half), IFFT_y."""
     import torch
 
     from atus2_b200 import PREC_FP64, PREC_MIXED, STEP_NL, Solver
@@ -1137,6 +1140,15 @@ def profile_block(which):
         l0 = s.launches
         t0 = time.perf_counter()
         s.block(C1_NK, STEP_NL)
+        s.synchronize()
+        ms, launches = (time.perf_counter() - t0) * 1e3, s.launches - l0
+    elif which.startswith("slit"):
+        h, psi, V = config2_inputs()
+        s = _c2_solver(PREC_MIXED if which == "slit-mixed" else PREC_FP64, stream, h, psi, V)
+        torch.cuda.synchronize()
+        l0 = s.launches
+        t0 = time.perf_counter()
+        s.block(2, STEP_NL)
         s.synchronize()
         ms, launches = (time.perf_counter() - t0) * 1e3, s.launches - l0
     else:
@@ -1160,10 +1172,11 @@ def main():
                     help="also time the drop-in bragg program with output every block (async vs sync files)")
     ap.add_argument("--phase-scans", action="store_true",
                     help="also time the drop-in bragg program's phase scans side by side against one by one")
-    ap.add_argument("--profile-block", choices=["fp64", "mixed", "rt1d"],
+    ap.add_argument("--profile-block", choices=["fp64", "mixed", "rt1d", "slit", "slit-mixed"],
                     help="run one 2-step block of the 256^3 Bragg workload (fp64, mixed; the fifth "
-                         "pass2_kernel launch is the z potential pass) or one 1000-step block of the 1D "
-                         "rt_solver workload (rt1d) and exit -- for profiler captures")
+                         "pass2_kernel launch is the z potential pass), one 1000-step block of the 1D "
+                         "rt_solver workload (rt1d) or one 2-step block of the 2048^2 double slit "
+                         "(slit, slit-mixed) and exit -- for profiler captures")
     args = ap.parse_args()
     if args.profile_block:
         profile_block(args.profile_block)
