@@ -143,13 +143,13 @@ __device__ __forceinline__ double reduce_2pi(double a) {
 // Horner form on x^2; larger arguments call sincos().
 __device__ __forceinline__ void sincos_step(double x, double *s, double *c) {
   if (fabs(x) <= 0.03125) {
+    // Taylor series to x^7 (sin) and x^8 (cos): the first omitted terms,
+    // x^9/9! and x^10/10!, are below 2.5e-18 x and 2.5e-22 for |x| <= 1/32
     const double x2 = x * x;
-    double ps = fma(x2, 1.0 / 362880.0, -1.0 / 5040.0);
-    ps = fma(ps, x2, 1.0 / 120.0);
+    double ps = fma(x2, -1.0 / 5040.0, 1.0 / 120.0);
     ps = fma(ps, x2, -1.0 / 6.0);
     *s = fma(ps * x2, x, x);
-    double pc = fma(x2, -1.0 / 3628800.0, 1.0 / 40320.0);
-    pc = fma(pc, x2, -1.0 / 720.0);
+    double pc = fma(x2, 1.0 / 40320.0, -1.0 / 720.0);
     pc = fma(pc, x2, 1.0 / 24.0);
     pc = fma(pc, x2, -0.5);
     *c = fma(pc, x2, 1.0);
@@ -303,11 +303,16 @@ __device__ __forceinline__ void bragg_pair(int stable, double dt, double V11, do
       const double Ep = 0.5 * (V11 + V22 + tmp1);
       const double Em = 0.5 * (V11 + V22 - tmp1);
       double2 gp, gm;
+      // the reference's 1 / |(V11 - E+-)^2 + Omega^2| (sums of squares, so
+      // |.| is the identity) from one division: 1/A = B/(AB), 1/B = A/(AB)
+      const double Ap = (V11 - Ep) * (V11 - Ep) + Omega * Omega;
+      const double Am = (V11 - Em) * (V11 - Em) + Omega * Omega;
+      const double inv = 1.0 / (Ap * Am);
       sincos_step(-dt * Ep, &im1, &re1);
-      tmp1 = 1.0 / fabs((V11 - Ep) * (V11 - Ep) + Omega * Omega);
+      tmp1 = Am * inv;
       gp = make_double2(tmp1 * re1, tmp1 * im1);
       sincos_step(-dt * Em, &im1, &re1);
-      tmp1 = 1.0 / fabs((V11 - Em) * (V11 - Em) + Omega * Omega);
+      tmp1 = Ap * inv;
       gm = make_double2(tmp1 * re1, tmp1 * im1);
       const double O2 = Omega * Omega;
       const double2 O11 = make_double2(O2 * (gp.x + gm.x), O2 * (gp.y + gm.y));
