@@ -1169,9 +1169,25 @@ static int strang_block(atus_ctx *ctx, int nk, int kind, const double *F, const 
 int atus_profile_passes(atus_ctx *ctx, int kind, int reps, double *ms, double *lps, double *bytes, int *npass) {
   if (!ctx || !ms || !lps || !bytes || !npass || reps < 1) return ATUS_E_ARG;
   RUN(check_kind(ctx, kind));
-  cudaEvent_t e0, e1;
-  CK(cudaEventCreate(&e0));
-  CK(cudaEventCreate(&e1));
+  // The passes run out of the Strang schedule (a kinetic pass alone carries
+  // the whole transform scale, so repeated launches can drive complex64
+  // fields to zero): the fields and the time are saved here and put back.
+  const size_t fbytes = (size_t)ctx->csize * (size_t)ctx->npts;
+  char *saved = nullptr;
+  CK(cudaMalloc(&saved, fbytes * ctx->ncomp));
+  cudaError_t ce = cudaSuccess;
+  for (int c = 0; c < ctx->ncomp && ce == cudaSuccess; c++)
+    ce = cudaMemcpyAsync(saved + c * fbytes, ctx->psi[c], fbytes, cudaMemcpyDeviceToDevice, ctx->stream);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (ce == cudaSuccess) ce = cudaEventCreate(&e0);
+  if (ce == cudaSuccess) ce = cudaEventCreate(&e1);
+  if (ce != cudaSuccess) {
+    if (e0) cudaEventDestroy(e0);
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(saved);
+    return cuda_check(ctx, ce, "profile_passes: saving the fields");
+  }
+  const double t_saved = ctx->t;
   const NLArgs nl = nl_args(ctx, kind, ctx->t + 0.5 * ctx->dt, 1.0);
   const double fb = 2.0 * (double)ctx->csize * (double)ctx->ncomp * (double)ctx->npts;  // read + write all fields
   const double vb = (kind == K_NL) ? 8.0 * ctx->npts * [&] {
@@ -1218,7 +1234,13 @@ int atus_profile_passes(atus_ctx *ctx, int kind, int reps, double *ms, double *l
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  for (int c = 0; c < ctx->ncomp && ce == cudaSuccess; c++)
+    ce = cudaMemcpyAsync(ctx->psi[c], saved + c * fbytes, fbytes, cudaMemcpyDeviceToDevice, ctx->stream);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(ctx->stream);
+  cudaFree(saved);
+  ctx->t = t_saved;
   *npass = np;
+  if (ce != cudaSuccess) return cuda_check(ctx, ce, "profile_passes: restoring the fields");
   return r;
 }
 

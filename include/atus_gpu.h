@@ -247,8 +247,10 @@ ATUS_API int atus_strang_block_rabi(atus_ctx *ctx, int nk, int kind, const doubl
  * with CUDA events there.  ms[i] receives the average duration of one launch
  * of pass i, launches_per_step[i] how often one Strang step launches it, and
  * bytes[i] the field bytes one launch reads and writes (the algorithmic
- * traffic).  *npass receives the number of pass kinds (<= 8).  The fields are
- * advanced by the passes; restore them before using the results. */
+ * traffic).  *npass receives the number of pass kinds (<= 8).  The passes
+ * run out of the Strang schedule on the context's fields; the fields and the
+ * time are saved before (a temporary device copy of the fields) and restored
+ * after, so the context's state is unchanged. */
 ATUS_API int atus_profile_passes(atus_ctx *ctx, int kind, int reps, double *ms, double *launches_per_step,
                                  double *bytes, int *npass);
 

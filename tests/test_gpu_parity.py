@@ -638,3 +638,30 @@ def test_sob_run_on_device_matches_host_loop():
     # residual, a squared norm of a small gradient, amplifies them
     assert abs(runs[0][1] - runs[1][1]) <= 1e-12 * runs[0][1]
     assert rel_l2(runs[1][2], runs[0][2]) < 1e-13
+
+
+@pytest.mark.parametrize("prec", [PREC_FP64, PREC_MIXED])
+@pytest.mark.parametrize("shape", [[512, 256], [64, 32, 128]])
+def test_profile_passes_keeps_state(prec, shape):
+    """atus_profile_passes runs the passes out of the Strang schedule (a
+    kinetic pass alone carries the whole transform scale: twenty of them in a
+    row drive complex64 fields to zero) and must put the fields and the time
+    back exactly."""
+    h = _grid(len(shape), shape, 16.0)
+    xs = _coords(h)
+    r2 = sum(x * x for x in xs)
+    s = Solver(h, 1, prec)
+    s.set_psi(0, np.exp(-0.5 * r2) * np.exp(1j * xs[0]))
+    s.set_alpha(0, [0.5] * len(shape))
+    s.set_gs([1.0])
+    s.set_potential(0, 0.5 * r2)
+    s.set_dt(1e-3)
+    s.block(5, KIND_NL)
+    before, t0 = s.psi(0), s.t
+    prof = s.profile_passes(KIND_NL, reps=20)
+    assert len(prof) >= 2 and all(p[0] > 0 for p in prof)
+    assert s.t == t0
+    assert np.array_equal(s.psi(0), before)
+    s.block(5, KIND_NL)
+    assert np.linalg.norm(s.psi(0)) > 0.5 * np.linalg.norm(before)
+    s.close()
